@@ -1,0 +1,249 @@
+/*
+ * iw_b200.h -- C ABI of the B200 time-step library for the stratified
+ * Boussinesq solver "Dubwise" (Fourier x,y / Legendre multidomain penalty z).
+ *
+ * Two groups of entry points:
+ *
+ *  1. The handle API (iw_*): a Fortran driver binds these with
+ *     ISO_C_BINDING (every argument is a plain pointer or a value, every
+ *     function returns an int status, 0 = ok).  Fields live on the device
+ *     across steps; the host uploads the state once and downloads it for
+ *     output or restart.
+ *
+ *  2. Drop-in replacements for the reference subroutines, with the
+ *     reference's names, argument lists (all by reference, Fortran style,
+ *     trailing underscore) and in-place semantics.  They act on the handle
+ *     made current by iw_bind().  Routines that the reference calls on
+ *     COMMON-block state (convec_, calcuvwt_) act on the bound handle's
+ *     device state; routines that take an array argument (horfft_, dpdz_,
+ *     interface_avg3d_, filter_3dlegenfourier_, ...) take host arrays and
+ *     copy them in and out, as the reference's diagnostics need.
+ *
+ * Array layout (identical to the reference COMMON blocks): a field is
+ * (nxpp, ny, nz) doubles, x fastest, with nxpp = nx+2.  In spectral space the
+ * x index holds interleaved (Re, Im) pairs for kx = 0..nx/2, y holds FFT-
+ * ordered ky, and z holds the physical GLL points of nsubd subdomains of nzloc
+ * points each (interface points duplicated).  A column is the nz values of one
+ * (kx, ky) mode.
+ *
+ * Threading: one host thread per handle; work is ordered on the handle's
+ * CUDA stream.  Errors are reported by the return code and iw_last_error().
+ */
+#ifndef IW_B200_H
+#define IW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IW_MAX_SUBD 64
+#define IW_MAX_NZLOC 64
+
+/* status codes */
+#define IW_OK 0
+#define IW_ERR_CONFIG 1    /* invalid dims / radices / subdomain table    */
+#define IW_ERR_CUDA 2      /* a CUDA runtime call failed                  */
+#define IW_ERR_NONFINITE 3 /* NaN/Inf detected in the state               */
+#define IW_ERR_PIVOT 4     /* exactly zero pivot in a band factorisation  */
+#define IW_ERR_STATE 5     /* call out of order (no handle bound, ...)    */
+#define IW_ERR_NOMEM 6     /* device allocation failed                    */
+#define IW_ERR_TIMEOUT 7   /* a bounded device wait gave up               */
+
+/* boundary-condition variants of calcuvwt (reference files in brackets) */
+#define IW_BC_FREESLIP 0 /* calcuvwt.f / calcuvwt_freeslip.f: u,v Neumann at both ends */
+#define IW_BC_NOSLIP 1   /* calcuvwt_noslip.f: u,v Dirichlet bottom, Neumann top      */
+
+/* storage precision of the bulk fields */
+#define IW_PREC_FP64 0  /* everything FP64 (parity path)                         */
+#define IW_PREC_MIXED 1 /* FP32 fields/FFTs/products/filters, FP64 solves        */
+
+/* dim.h PARAMETERs, made runtime values (dim.h:12-28). */
+typedef struct iw_dims {
+  int32_t nx;    /* points in x (even; radices 2,3,5)            */
+  int32_t ny;    /* points in y (1 => 2-D run, ndims=2)          */
+  int32_t nzloc; /* GLL points per subdomain                     */
+  int32_t nsubd; /* subdomains in z; nz = nzloc*nsubd            */
+} iw_dims;
+
+/* input.dat namelists &inputs &params &mflags (main.f:185-194) plus the
+ * subd.dat table (setup.f:316-325) and the switches that the reference
+ * hard-codes in source. */
+typedef struct iw_params {
+  /* &inputs */
+  double dt;          /* dtin                                        */
+  /* &params */
+  double xlen, ylen, zlen;
+  double brunt;       /* buoyancy frequency N                        */
+  double xnu, xkappa; /* viscosity, diffusivity                      */
+  double grav, rho0;
+  double umax;        /* forcing velocity scale                      */
+  double xacrit;      /* paddle forcing amplitude (0 = off)          */
+  double xbcrit, zcen;/* mean-u damping window fzgaus                */
+  double fwave;       /* forcing duration in wave periods            */
+  /* &mflags */
+  double amp, p, pf;  /* filter amplitude, Legendre/Fourier orders   */
+  double fackc;
+  double facdir, facneumn, facrobin;
+  int32_t ispecfilternl, ispecfilterexp, nspecfilterexp, navgintrfc;
+  /* switches hard-coded in the reference */
+  int32_t bc_variant;    /* IW_BC_*                                  */
+  int32_t meanu_damping; /* (1,1)-mode u *= 1-fzgaus (calcuvwt.f:343) */
+  int32_t forcing;       /* virtual paddle in rhsfm (solver.f:942)   */
+  int32_t precision;     /* IW_PREC_*                                */
+  /* subd.dat */
+  double z0[IW_MAX_SUBD];
+  double zh[IW_MAX_SUBD];
+} iw_params;
+
+/* multistep coefficients (COMMON /ab/ /bdf/, comtimeadvance.h) */
+typedef struct iw_coefs {
+  double fac1, fac2, fac3;       /* SS extrapolation of the NL term */
+  double bdf1, bdf2, bdf3, bdfv; /* BDF of the time derivative      */
+  double dt;
+} iw_coefs;
+
+/* per-step diagnostics (maxcalc various.f:665-987, energycalc_postp
+ * postp.f:415-732) */
+typedef struct iw_diag_out {
+  double ke;       /* 0.5 * sum_{k>=2} (u^2+v^2+w^2) over physical points */
+  double eps;      /* xnu * sum_{k>=2} |grad u|^2                           */
+  double umin, umax, vmin, vmax, wmin, wmax, tmin, tmax;
+  double cflx, cfly, cflz;
+  double wrms_bottom; /* rms of w over z < 0.2 zlen (noise growth)      */
+  double t;
+  int32_t istep;
+  int32_t interface_avg_count[4];
+} iw_diag_out;
+
+typedef struct iw_handle iw_handle;
+
+/* ---------------------------------------------------------------------- */
+/* Handle API                                                               */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces main.f:210-218 (fftfax/cftfax), setup.f:6-267 (setup) and the
+ * allocation of every COMMON block; validates dims and the subdomain table.
+ * device < 0 selects the current device. */
+int iw_init(const iw_dims *dims, const iw_params *prm, int device,
+            iw_handle **out);
+int iw_destroy(iw_handle *h);
+const char *iw_last_error(void);
+
+/* Upload / download the complete multistep state in the reference layout.
+ * Each pointer addresses 4 fields (u,v,w,temp) back to back, i.e.
+ * 4*nxpp*ny*nz doubles; NULL skips that level.  Levels: n, n-1, n-2 for the
+ * prognostic fields (comflow.h) and n-1, n-2 for the NL terms (commatrix.h). */
+int iw_upload_state(iw_handle *h, const double *uvwt, const double *uvwt_n,
+                    const double *uvwt_nm, const double *s_n,
+                    const double *s_nm, double t, int istep_done);
+int iw_download_state(iw_handle *h, double *uvwt, double *uvwt_n,
+                      double *uvwt_nm, double *s_n, double *s_nm);
+
+/* Mode-1 internal wave initial condition plus seeded uniform noise in the
+ * bottom 20% of the depth, transformed to spectral space (a new init: the
+ * reference init.f sets zeros).  Deterministic for a given seed. */
+int iw_init_mode1(iw_handle *h, double amplitude, double noise_amp,
+                  uint64_t seed);
+
+/* One complete time step of main.f:653-1066: maxcalc round trip, convec,
+ * coefficient schedule, calcuvwt, t += dt, interface averaging.  The
+ * coefficient schedule of main.f:700-856 is applied internally (fixed dt). */
+int iw_step(iw_handle *h);
+/* nsteps steps; with use_graph != 0 the steady-state step is captured once
+ * into a CUDA graph and replayed. */
+int iw_run(iw_handle *h, int nsteps, int use_graph);
+/* As iw_step but with caller-supplied coefficients (variable-dt restarts). */
+int iw_step_coefs(iw_handle *h, const iw_coefs *c);
+
+int iw_diag(iw_handle *h, iw_diag_out *out);
+int iw_sync(iw_handle *h);
+/* raw device pointer of field f (0..3 = u,v,w,temp at level n) */
+int iw_field_ptr(iw_handle *h, int f, void **dptr);
+/* CUDA stream the handle works on (cudaStream_t) */
+int iw_stream(iw_handle *h, void **stream);
+/* bytes of device memory held by the handle */
+int iw_device_bytes(iw_handle *h, size_t *bytes);
+
+/* Batched vertical penalty solves (one Helmholtz system per (kx,ky)
+ * column), the isolated-solve workload: lambda = kx^2+ky^2 + c, BCs by the
+ * bc flags.  rhs/sol are complex columns [ncol][nz] as (re,im) pairs on the
+ * device.  mode 0: FP64 factor + FP64 solve; 1: FP32 solve + one FP64
+ * residual refinement.  The factors are built on the first call for a given
+ * (c, ifbcbot, ifbctop) and kept. */
+int iw_helm_solve_batched(iw_handle *h, const double *lam_dev, int ncol,
+                          int ifbcbot, int ifbctop, const double *rhs_dev,
+                          double *sol_dev, int mode);
+
+/* Make h the handle the Fortran-style entry points below act on. */
+int iw_bind(iw_handle *h);
+
+/* ---------------------------------------------------------------------- */
+/* Drop-in replacements of the reference subroutines (Fortran calling      */
+/* convention: every argument by reference; REAL = double).                 */
+/* ---------------------------------------------------------------------- */
+
+/* horfft.f:2-69.  In place on nk z-planes of (nxpp, ny) doubles.  is=-1:
+ * physical -> spectral (x real-to-half-complex scaled 1/nx, then y complex
+ * unscaled over the first nx/2 kx columns, everything scaled 1/ny).
+ * is=+1: the inverse, unscaled.  Host array. */
+void horfft_(double *b, const int *is, const int *nk);
+
+/* derv.f:212-275: b = (2/zh(ks)) D a, per subdomain, whole field. Host. */
+void dpdz_(const double *a, double *b);
+
+/* filtering.f:811-983: Fourier (radial exponential) then Legendre modal
+ * exponential filter of a spectral field, in place.  Host array. */
+void filter_3dlegenfourier_(double *f, const int *ifourier, const int *ilegen,
+                            const int *iout);
+
+/* filtering.f:729-808: Legendre modal filter of one subdomain column. */
+void filter_legenpen_(const double *fin, double *fout, const double *ybar,
+                      const int *iprt, const int *ks);
+
+/* penalty.f:714-775: adaptive interface averaging in physical space of a
+ * spectral field, in place; ic returns the number of averaged points. */
+void interface_avg3d_(double *f, int *ic);
+
+/* penalty.f:162-251 (+ helmv_penalty 255-397, matrix_elmsetup 403-634,
+ * band_lu.f:15-54): assemble the penalty system for epsilon and the BCs,
+ * band-LU factor it and solve for the real and imaginary RHS.  rhsinr/rhsini
+ * are multiplied by -epsilon in place, as in the reference. */
+void penalty_main_(const double *epsilon, const int *ifuncreal,
+                   const double *bcrbot, const double *bcibot,
+                   const double *bcrtop, const double *bcitop,
+                   const int *ifbcbot, const int *ifbctop, double *rhsinr,
+                   double *rhsini, double *fr, double *fi);
+
+/* band_lu.f:15-54: dense (nz x nz, column major) -> band storage, SGBTRF
+ * (unblocked SGBTF2 path) and SGBTRS for xr and xi.  Solutions overwrite
+ * xr/xi. */
+void bandlu_solve_(const double *ain, double *xr, double *xi,
+                   const int *ifuncreal);
+
+/* penalty.f:9-53: interior-subdomain Robin parameters for epsilon (kept in
+ * the bound handle, used by the next penalty_main_). */
+void penalty_setup_(const double *epsilon);
+
+/* solver.f:6-514 on the bound handle's device state. */
+void convec_(const int *istep, const int *istart, const int *ispecfilternl);
+/* calcuvwt*.f on the bound handle's device state; cpenspecfilter is a
+ * Fortran LOGICAL (4-byte int, nonzero = .true.). */
+void calcuvwt_(const int *izmode, const int *ispecfilter, const int *irelax,
+               const int *cpenspecfilter);
+
+/* multistep.f:7-89: variable-step AB3 / BDF3 coefficients. */
+double abvar1_(const double *dt1, const double *dt2, const double *dt3);
+double abvar2_(const double *dt1, const double *dt2, const double *dt3);
+double abvar3_(const double *dt1, const double *dt2, const double *dt3);
+double bdfvarv_(const double *dt1, const double *dt2, const double *dt3);
+double bdfvar1_(const double *dt1, const double *dt2, const double *dt3);
+double bdfvar2_(const double *dt1, const double *dt2, const double *dt3);
+double bdfvar3_(const double *dt1, const double *dt2, const double *dt3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IW_B200_H */

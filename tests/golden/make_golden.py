@@ -1,0 +1,56 @@
+"""Extract the reference's own numeric artefacts into small fixtures.
+
+Run here (where the reference tree is mounted) with
+    python tests/golden/make_golden.py /root/reference/mode1_bbl
+It reads text files that the reference's runs wrote and stores them as JSON
+under tests/golden/.  The GPU box never reads the reference tree.
+
+* testout.dat     -- testhelm (testhelm.f:1-134): penalty solve of
+                     f - eps f'' = eps, f = 0 at both ends, eps = 1e-2,
+                     10 subdomains x 25 points of runfolder/subd.dat, zlen=5.
+* z_grid.dat      -- GLL grid of the shipped 12-subdomain run (setup.f:151-166)
+* x_grid.dat      -- x grid (setup.f:136-142)
+* uveltest.dat    -- rows 1041-1049: u(32,1,10), u(32,1,50) at t=0..0.8 of the
+                     shipped 2-D forced run (various.f:743-745)
+* minmaxtest.dat, cfl.dat, avgint.dat -- per-step traces of the same run
+* runfolder/subd.dat, subd.dat -- subdomain tables used above
+"""
+import json
+import os
+import sys
+
+
+def rows(path, skip=0):
+    out = []
+    for line in open(path).read().splitlines()[skip:]:
+        parts = line.split()
+        if not parts:
+            continue
+        try:
+            out.append([float(x.replace("D", "E")) for x in parts])
+        except ValueError:
+            continue
+    return out
+
+
+def main(ref):
+    here = os.path.dirname(os.path.abspath(__file__))
+    g = {}
+    g["testout"] = [r[:2] for r in rows(os.path.join(ref, "testout.dat"), 1)]
+    g["z_grid"] = rows(os.path.join(ref, "z_grid.dat"))
+    g["x_grid"] = rows(os.path.join(ref, "x_grid.dat"))
+    lines = open(os.path.join(ref, "uveltest.dat")).read().splitlines()
+    g["uveltest"] = [[float(x) for x in l.split()] for l in lines[1040:1049]]
+    g["minmaxtest"] = rows(os.path.join(ref, "minmaxtest.dat"))
+    g["cfl"] = rows(os.path.join(ref, "cfl.dat"), 1)
+    g["avgint"] = rows(os.path.join(ref, "avgint.dat"), 1)
+    g["subd_runfolder"] = rows(os.path.join(ref, "runfolder", "subd.dat"))
+    g["subd_shipped"] = rows(os.path.join(ref, "subd.dat"))
+    g["_source"] = "jmsegret/IWrepo mode1_bbl run artefacts; see make_golden.py"
+    with open(os.path.join(here, "reference_runs.json"), "w") as f:
+        json.dump(g, f, indent=0)
+    print("wrote", os.path.join(here, "reference_runs.json"))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/mode1_bbl")

@@ -1,0 +1,188 @@
+"""Pin the CPU oracle to the reference's own numeric artefacts.
+
+The reference has no test suite; its runs left text files that the oracle
+must reproduce (tests/golden/reference_runs.json, made by make_golden.py):
+
+* testout.dat (testhelm.f): penalty solve, 8 significant digits  -> exact pin
+* z_grid.dat / x_grid.dat: GLL / uniform grids, 7 decimals        -> exact pin
+* run log `output`: wave frequency of the 128x250 run, 15 digits  -> exact pin
+* uveltest.dat / cfl.dat / minmaxtest.dat: 9 steps of the shipped 2-D forced
+  run (calcuvwt_noslip.f).  The input.dat of that run is not recorded (it
+  stopped after 9 of the 400 steps the shipped file asks for); the oracle
+  follows it to 4-5 significant digits, the free-slip variant does not.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from iwrepo_b200 import config as cf
+from oracle import Oracle, multistep
+
+
+def runfolder_cfg(golden):
+    sub = golden["subd_runfolder"]
+    n = int(sub[0][0])
+    z0 = [r[0] for r in sub[1:n + 1]]
+    zh = [r[1] for r in sub[1:n + 1]]
+    return cf.Config(nx=8, ny=1, nzloc=25, nsubd=n, dt=0.1, xlen=10.0, ylen=1.0, zlen=5.0,
+                     z0=z0, zh=zh).validate()
+
+
+def test_testhelm_testout(golden):
+    """testhelm.f:59-99: eps=1e-2, rhs=-1, homogeneous Dirichlet both ends."""
+    cfg = runfolder_cfg(golden)
+    o = Oracle(cfg)
+    eps = 1e-2
+    o.penalty_setup(eps)
+    nz = cfg.nz
+    fr, fi, rr, _ = o.penalty_main(eps, 0, 0, (0.0, 0.0, 0.0, 0.0), -np.ones(nz), -np.ones(nz))
+    ref = np.array(golden["testout"])
+    z = o.tables()["z"]
+    assert np.allclose(z, ref[:, 0], atol=6e-8, rtol=0)
+    big = np.abs(ref[:, 1]) > 1e-6
+    assert np.max(np.abs(fr[big] - ref[big, 1]) / np.abs(ref[big, 1])) < 1e-7
+    assert np.max(np.abs(fr - ref[:, 1])) < 1e-10
+    assert np.array_equal(fr, fi)
+    # penalty_main scales the caller's RHS by -eps in place (penalty.f:188-191)
+    assert np.allclose(rr, eps)
+    # analytic solution of f - eps f'' = eps, f(0)=f(5)=0
+    s = math.sqrt(eps)
+    exact = eps * (1 - np.cosh((z - 2.5) / s) / math.cosh(2.5 / s))
+    assert np.max(np.abs(fr - exact)) < 1e-9
+
+
+def test_shipped_grids(golden):
+    o = Oracle(cf.shipped_2d())
+    z = o.tables()["z"]
+    zr = np.array(golden["z_grid"])
+    assert np.allclose(z, zr[:, 1], atol=6e-8, rtol=0)
+    xr = np.array(golden["x_grid"])[:, 1]
+    assert np.allclose(np.arange(256) * 20.0 / 256, xr, atol=6e-8)
+
+
+def test_gll_tables_katp():
+    cfg = cf.baseline("C0")
+    t = Oracle(cfg).tables()
+    zp, wg, d = t["zpts"], t["wg"], t["d"]
+    assert abs(wg.sum() - 2.0) < 1e-14
+    assert zp[0] == -1.0 and zp[-1] == 1.0
+    # D is exact on polynomials of degree <= N
+    for p in range(cfg.nzloc):
+        assert np.allclose(d @ zp ** p, p * zp ** max(p - 1, 0) if p else 0 * zp, atol=1e-9)
+    # GLL quadrature exact to degree 2N-1
+    assert abs(wg @ zp ** 30 - 2.0 / 31) < 1e-13
+
+
+def test_wave_parameters_run_log():
+    """output:53-67 of the 128x250 run: omega = 4.850712500726660E-002."""
+    pi2 = 8 * math.atan(1.0)
+    xk, xm = pi2 / 40.0, pi2 / (2 * 5.0)
+    omega = (0.2 * xk) / math.sqrt(xk * xk + xm * xm)
+    assert abs(omega - 4.850712500726660e-02) < 1e-16
+
+
+def test_multistep_coefficients():
+    dt = 0.37
+    assert abs(multistep("abvar1", dt, dt, dt) - 23 / 12) < 1e-15
+    assert abs(multistep("abvar2", dt, dt, dt) + 16 / 12) < 1e-15
+    assert abs(multistep("abvar3", dt, dt, dt) - 5 / 12) < 1e-15
+    assert abs(multistep("bdfvarv", dt, dt, dt) - 11 / 6) < 1e-15
+    assert abs(multistep("bdfvar1", dt, dt, dt) - 3) < 1e-14
+    assert abs(multistep("bdfvar2", dt, dt, dt) + 1.5) < 1e-14
+    assert abs(multistep("bdfvar3", dt, dt, dt) - 1 / 3) < 1e-15
+
+
+def test_horfft_semantics():
+    """FFT991/CFFT99 conventions incl. the x-Nyquist column quirk."""
+    cfg = cf.Config(nx=16, ny=8, nzloc=5, nsubd=2, dt=1e-3).validate()
+    o = Oracle(cfg)
+    rng = np.random.default_rng(1)
+    phys = np.zeros((cfg.nz, cfg.ny, cfg.nxpp))
+    phys[:, :, :cfg.nx] = rng.standard_normal((cfg.nz, cfg.ny, cfg.nx))
+    spec = o.horfft(phys.copy(), -1)
+    ref = np.fft.rfft2(phys[:, :, :cfg.nx], axes=(1, 2)) / (cfg.nx * cfg.ny)
+    c = spec[:, :, 0::2] + 1j * spec[:, :, 1::2]
+    assert np.allclose(c[:, :, :cfg.nx // 2], ref[:, :, :cfg.nx // 2], atol=1e-14)
+    # Nyquist column: x-transformed only, then scaled by 1/ny
+    nyq = np.fft.rfft(phys[:, :, :cfg.nx], axis=2)[:, :, cfg.nx // 2].real / cfg.nx / cfg.ny
+    assert np.allclose(c[:, :, cfg.nx // 2].real, nyq, atol=1e-14)
+    back = o.horfft(spec.copy(), 1)
+    R = np.fft.rfft(phys[:, :, :cfg.nx], axis=2)
+    R[:, :, cfg.nx // 2] /= cfg.ny  # a round trip scales the x-Nyquist column by 1/ny
+    assert np.allclose(back[:, :, :cfg.nx], np.fft.irfft(R, cfg.nx, axis=2), atol=1e-13)
+    assert np.all(back[:, :, cfg.nx:] == 0)
+
+
+def test_dpdz_exact_on_polynomials():
+    cfg = cf.Config(nx=8, ny=2, nzloc=9, nsubd=3, dt=1e-3, zlen=1.5,
+                    z0=[0.0, 0.3, 0.9], zh=[0.3, 0.6, 0.6]).validate()
+    o = Oracle(cfg)
+    z = o.tables()["z"]
+    f = np.zeros((cfg.nz, cfg.ny, cfg.nxpp))
+    f[:] = (z ** 5)[:, None, None]
+    df = o.dpdz(f)
+    assert np.allclose(df, (5 * z ** 4)[:, None, None], atol=1e-10)
+
+
+def test_filter_identity_for_low_modes():
+    cfg = cf.Config(nx=8, ny=2, nzloc=9, nsubd=2, dt=1e-3, amp=36.0, p=4.0, pf=4.0).validate()
+    o = Oracle(cfg)
+    t = o.tables()
+    assert t["sigma"][0] == 1.0 and abs(t["sigma"][-1] - math.exp(-36.0)) < 1e-30
+    f = np.zeros((cfg.nz, cfg.ny, cfg.nxpp))
+    f[:, 0, 0] = 1.0  # mean mode, constant in z
+    g = o.filter3d(f)
+    assert np.allclose(g, f, atol=1e-14)
+
+
+@pytest.mark.parametrize("variant,tol", [(cf.IW_BC_NOSLIP, 5e-4)])
+def test_shipped_2d_trajectory(golden, variant, tol):
+    ref = np.array(golden["uveltest"])
+    cflr = np.array(golden["cfl"])
+    o = Oracle(cf.shipped_2d(bc_variant=variant))
+    for s in range(9):
+        o.step(1)
+        lm = o.last_maxcalc()
+        assert abs(lm["probe"] - ref[s, 1:]).max() <= tol * max(1e-30, abs(ref[s, 1:]).max())
+        # CFL in z (w) to 4 digits, located at the same (i,j,k)
+        if s > 0:
+            assert abs(lm["cfl"][2] - cflr[s, 9]) <= 3e-4 * cflr[s, 9]
+            assert lm["cfl_idx"][8] == int(cflr[s, 12])
+
+
+def test_freeslip_variant_differs(golden):
+    """The shipped trajectory was made with calcuvwt_noslip.f."""
+    ref = np.array(golden["uveltest"])
+    errs = {}
+    for v in (cf.IW_BC_FREESLIP, cf.IW_BC_NOSLIP):
+        o = Oracle(cf.shipped_2d(bc_variant=v))
+        for s in range(9):
+            o.step(1)
+        errs[v] = abs(o.last_maxcalc()["probe"][0] - ref[8, 1]) / abs(ref[8, 1])
+    assert errs[cf.IW_BC_NOSLIP] < 0.05 * errs[cf.IW_BC_FREESLIP]
+
+
+def test_oracle_deterministic_across_threads():
+    import oracle as om
+    cfg = cf.Config(nx=16, ny=16, nzloc=9, nsubd=3, dt=1e-3).validate()
+    outs = []
+    for th in (1, 4):
+        om.set_threads(th)
+        o = Oracle(cfg)
+        o.init_mode1(0.05, 1e-4, 7)
+        o.step(3)
+        outs.append(o.state())
+    om.set_threads(om.max_threads())
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_factor_cache_is_bit_identical():
+    cfg = cf.Config(nx=16, ny=8, nzloc=9, nsubd=3, dt=1e-3).validate()
+    st = []
+    for cache in (False, True):
+        o = Oracle(cfg, cache=cache)
+        o.init_mode1(0.05, 1e-4, 11)
+        o.step(4)
+        st.append(o.state())
+    assert np.array_equal(st[0], st[1])
