@@ -1,0 +1,356 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 time step (grid-point-steps/s).
+
+Default workload: the mixed-precision single run, Nx=Ny=512, 12 subdomains x 33
+GLL points (nz=396), Re=5000, A=0.1, noise 1e-3, dt=2.5e-4 (FP32 fields, FFTs,
+products and filters; FP64 band solves, mean mode and projection).  The same
+steps are also run with the plain FP64 path on the same input to report the
+mixed/FP64 speed ratio and the mixed path's field error against FP64.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--config C3|C2|C0] [--precision mixed|fp64]
+
+N>1 (torchrun): independent replicas, one per GPU (the step does not shard),
+value = all ranks' grid-point-steps / max-over-ranks time.
+--impl reference: the CPU restatement of the reference step (all host
+threads) on a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from iwrepo_b200 import config as cf  # noqa: E402
+
+METRIC = "grid-pt-steps/s, mixed+batched vs plain FP64 on 1 B200 at <=1e-5 rel L2 err"
+UNIT = "grid-pt-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="C3")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_cfg(name: str, precision: str):
+    prec = cf.IW_PREC_MIXED if precision == "mixed" else cf.IW_PREC_FP64
+    return cf.baseline(name, precision=prec)
+
+
+def describe(cfg, precision):
+    amp, noise = cf.BASELINE_IC.get(cfg.name, (0.05, 1e-4))
+    return {
+        "workload": f"{cfg.name}: {cfg.nx}x{cfg.ny}x({cfg.nsubd}x{cfg.nzloc}={cfg.nz}) Boussinesq step, "
+                    f"Re={1 / cfg.xnu:.0f}, A={amp}, noise={noise}, dt={cfg.dt}, "
+                    f"{'FP32 fields + FP64 solves' if precision == 'mixed' else 'plain FP64'}",
+        "nx": cfg.nx, "ny": cfg.ny, "nz": cfg.nz, "nsubd": cfg.nsubd, "nzloc": cfg.nzloc,
+        "grid_points": cfg.grid_points, "bc": "no-slip bottom / free-slip top",
+        "filter": "exponential order 8, amp 36, every step",
+        "l2": "inputs larger than L2 (each field >= 105 MB); no flush needed",
+        "parallelism": "replicas (no sharding)",
+    }
+
+
+# ----------------------------------------------------------------------
+# clocks sampled during the timed region
+class Clocks:
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------
+def cpu_sample_cfg(cfg):
+    """Bounded sample of the workload for the CPU restatement: the same
+    vertical structure, physics and dt on a 32x32 horizontal grid."""
+    return cfg.replace(nx=32, ny=32, precision=cf.IW_PREC_FP64)
+
+
+def cpu_rate(cfg, threads: int, warm: int, steps: int, faithful: bool):
+    import oracle
+    oracle.set_threads(threads)
+    s = cpu_sample_cfg(cfg)
+    amp, noise = cf.BASELINE_IC.get(cfg.name, (0.05, 1e-4))
+    o = oracle.Oracle(s, cache=not faithful)
+    o.init_mode1(amp, noise, 1234)
+    o.step(warm)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return s.grid_points * steps / dt, s, dt
+
+
+def run_reference(args, rank, world):
+    cfg = workload_cfg(args.config, args.precision)
+    if rank != 0:
+        return
+    import oracle
+    threads = oracle.max_threads()
+    steps = max(1, min(args.steps, 4))
+    warm = max(1, min(args.warmup, 3))
+    rate, s, dt = cpu_rate(cfg, threads, warm, steps, faithful=True)
+    sample = (f"{s.nx}x{s.ny}x({s.nsubd}x{s.nzloc}) sample of {cfg.name} (same vertical grid/physics), "
+              f"{warm} warm-up + {steps} timed steps, faithful (refactor every step), FP64")
+    line = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+        "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": describe(cfg, args.precision),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------
+PHASE_FIELDS = {  # algorithmic fields moved per launch (reads + writes of ntot-sized arrays)
+    "stageA": 12, "y_inverse": 20, "x_row_nl": 23, "y_forward": 19, "stageE": 40,
+    "pressure": 6, "solve_uv": 4, "solve_w": 2, "solve_rho": 2,
+}
+LAUNCHES_PER_STEP = 18  # stageA, yinv, xrow, 2 yfwd, wallbc, stageE, press, 3 visc, 6 interface
+
+
+def run_ours(args, rank, world):
+    import torch
+    import iwrepo_b200 as iw
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        import datetime
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    cfg = workload_cfg(args.config, args.precision)
+    amp, noise = cf.BASELINE_IC.get(cfg.name, (0.05, 1e-4))
+    seed = 1000 + rank
+    s = iw.Solver(cfg, device=dev)
+    s.init_mode1(amp, noise, seed)
+    ext = torch.cuda.ExternalStream(s.stream())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    s.step(args.warmup)
+    barrier()
+    clocks = Clocks(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    s.step(args.steps)
+    e1.record(ext)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cfg.grid_points * args.steps / (ms / 1e3)
+
+    # per-phase device time (separate profiled steps) -> dominant kernel
+    s.profile(True)
+    s.step(max(2, min(args.steps, 5)))
+    s.sync()
+    ph = s.profile_read()
+    s.profile(False)
+    elem = 4 if args.precision == "mixed" else 8
+    fb = cfg.ntot * elem
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    phases = {}
+    for k, (t_ms, n) in ph.items():
+        if n:
+            avg = t_ms / n
+            nb = PHASE_FIELDS.get(k)
+            phases[k] = {"ms": avg, "gbs": (nb * fb / (avg / 1e3) / 1e9) if nb else None}
+    dom = max((k for k in phases if PHASE_FIELDS.get(k)), key=lambda k: phases[k]["ms"])
+    dom_gbs = phases[dom]["gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_gbs, "peak": hbm, "unit": "GB/s",
+                "frac": dom_gbs / hbm, "traffic": None,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes_per_launch": PHASE_FIELDS[dom] * fb}
+    b_alg = 28 * elem * (cfg.nx + 2) / cfg.nx
+    step_frac = (value / world) * b_alg / (hbm * 1e9)
+
+    line = {}
+    if rank == 0:
+        # e2e through the public API: host state in, K steps with a per-step
+        # host read of the mean profiles, host state out
+        st0 = s.state(0)
+        pinned = torch.empty(st0.size, dtype=torch.float64, pin_memory=True).numpy().reshape(st0.shape)
+        pinned[:] = st0
+        prof_host = torch.empty(4 * cfg.nz * 2, dtype=torch.float64, pin_memory=True).numpy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        zeros = np.zeros_like(pinned)
+        s.set_state(pinned, zeros, zeros, zeros, zeros, t=0.0, istep=0)
+        for k in range(args.steps):
+            s.step(1)
+            s.mean_profiles(prof_host)  # per-step device -> host result
+        out = s.state(0)
+        e2e_s = time.perf_counter() - t0
+        e2e_val = cfg.grid_points * args.steps / e2e_s
+        state_bytes = 4 * cfg.ntot * 8
+        line_e2e = {"value": world * e2e_val, "unit": UNIT,
+                    "h2d_bytes_per_step": int(5 * state_bytes / args.steps),
+                    "d2h_bytes_per_step": int(state_bytes / args.steps) + 4 * cfg.nz * 8,
+                    "note": "restart-style run through the C ABI: state upload (5 levels, pinned host) + "
+                            "K steps each reading the mean profiles back + state download; host wall clock"}
+
+        fp64 = None
+        err = None
+        if args.precision == "mixed" and not args.no_fp64_compare:
+            s.close()
+            del s
+            torch.cuda.empty_cache()
+            c64 = cfg.replace(precision=cf.IW_PREC_FP64)
+            r64 = iw.Solver(c64, device=dev)
+            r64.init_mode1(amp, noise, seed)
+            r64.step(args.warmup)
+            ext64 = torch.cuda.ExternalStream(r64.stream())
+            torch.cuda.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(ext64)
+            r64.step(args.steps)
+            a1.record(ext64)
+            torch.cuda.synchronize()
+            ms64 = a0.elapsed_time(a1)
+            fp64 = cfg.grid_points * args.steps / (ms64 / 1e3)
+            # same initial condition and step count for the error
+            xs = out
+            r64b = r64
+            ref = r64b.state(0)
+            # mixed ran warmup + steps (+ profiled) steps; compare fresh runs instead
+            r64.close()
+            del r64
+            sm = iw.Solver(cfg, device=dev)
+            sm.init_mode1(amp, noise, seed)
+            nerr = args.warmup + args.steps
+            sm.step(nerr)
+            a = sm.state(0)
+            sm.close()
+            r2 = iw.Solver(c64, device=dev)
+            r2.init_mode1(amp, noise, seed)
+            r2.step(nerr)
+            b = r2.state(0)
+            r2.close()
+            err = {f: float(np.linalg.norm(a[q] - b[q]) / max(np.linalg.norm(b[q]), 1e-300))
+                   for q, f in enumerate("uvwr")}
+            err["steps"] = nerr
+            del xs, ref
+
+        cpu = None
+        if not args.no_cpu:
+            try:
+                rate, smp, dt = cpu_rate(cfg, 1, 1, 1, faithful=True)
+                cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                       "sample": f"{smp.nx}x{smp.ny}x({smp.nsubd}x{smp.nzloc}) sample of {cfg.name}, "
+                                 f"1 warm-up + 1 timed step, single thread, faithful FP64 ({dt:.1f} s)"}
+            except Exception as e:  # the baseline is reported, never required
+                cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 fields/FFTs + f64 solves" if args.precision == "mixed" else "f64",
+            "data": "synthetic (mode-1 wave + seeded noise)",
+            "config": describe(cfg, args.precision),
+            "e2e": line_e2e, "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "roofline": roofline, "step_roofline_frac": step_frac, "phases": phases,
+            "cpu_baseline": cpu, "clocks": clk,
+        }
+        if fp64 is not None:
+            line["fp64_value"] = fp64
+            line["mixed_over_fp64"] = value / world / fp64
+            line["mixed_rel_l2_vs_fp64"] = err
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.impl == "ours" else 1)))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world != args.gpus and "RANK" not in os.environ:
+        world = 1
+    run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

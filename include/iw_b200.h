@@ -159,6 +159,9 @@ int iw_run(iw_handle *h, int nsteps, int use_graph);
 int iw_step_coefs(iw_handle *h, const iw_coefs *c);
 
 int iw_diag(iw_handle *h, iw_diag_out *out);
+/* Mean (kx=ky=0) profiles of u, v, w, rho (4*nz doubles) copied to the host
+ * buffer: the small per-step result a driver reads back. */
+int iw_mean_profiles(iw_handle *h, double *host4nz);
 int iw_sync(iw_handle *h);
 /* raw device pointer of field f (0..3 = u,v,w,temp at level n) */
 int iw_field_ptr(iw_handle *h, int f, void **dptr);
@@ -176,6 +179,14 @@ int iw_device_bytes(iw_handle *h, size_t *bytes);
 int iw_helm_solve_batched(iw_handle *h, const double *lam_dev, int ncol,
                           int ifbcbot, int ifbctop, const double *rhs_dev,
                           double *sol_dev, int mode);
+
+/* Per-phase device time of the step, measured with CUDA events on the
+ * handle's stream: enable=1 starts (and zeroes), 0 stops.  iw_profile_read
+ * returns milliseconds and counts for 16 phases: 0 stageA, 1 y-inverse,
+ * 2 x-row NL products, 3 y-forward, 4 wall BC term, 5 stageE, 6 pressure,
+ * 7 u/v solve, 8 w solve, 9 rho solve, 10 interface averaging. */
+int iw_profile(iw_handle *h, int enable);
+int iw_profile_read(iw_handle *h, double *ms16, long *n16);
 
 /* Make h the handle the Fortran-style entry points below act on. */
 int iw_bind(iw_handle *h);

@@ -118,7 +118,7 @@ class Config:
     name: str = "custom"
 
     def __post_init__(self):
-        if self.z0 is None or self.zh is None:
+        if (self.z0 is None or self.zh is None) and self.nsubd >= 1:
             h = self.zlen / self.nsubd
             self.z0 = [k * h for k in range(self.nsubd)]
             self.zh = [h] * self.nsubd
@@ -154,7 +154,7 @@ class Config:
             raise ConfigError(f"nzloc={self.nzloc} outside [3,{IW_MAX_NZLOC}]")
         if not 1 <= self.nsubd <= IW_MAX_SUBD:
             raise ConfigError(f"nsubd={self.nsubd} outside [1,{IW_MAX_SUBD}]")
-        if len(self.z0) != self.nsubd or len(self.zh) != self.nsubd:
+        if self.z0 is None or len(self.z0) != self.nsubd or len(self.zh) != self.nsubd:
             raise ConfigError("subd.dat table length differs from nsubd")
         for ks, (a, h) in enumerate(zip(self.z0, self.zh)):
             if not (h > 0 and math.isfinite(h) and math.isfinite(a)):

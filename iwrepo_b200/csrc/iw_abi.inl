@@ -1,0 +1,520 @@
+// Drop-in entry points with the reference's names and argument lists, plus
+// the remaining handle API (initial condition, diagnostics, isolated solves).
+// Included at the end of iw_host.inl.
+
+namespace {
+
+// physical-space copy of a spectral field, with an optional derivative:
+// op 0: f, 1: d/dx, 2: d/dy, 3: d/dz.  dst and tmp are device scratch.
+template <typename T>
+int phys_of(iw_handle* h, FieldSet<T>& fs, const T* src, T* dst, T* tmp, int op) {
+  Geo g = geo(h);
+  const T* s = src;
+  if (op == 3) {
+    k_dz_field<T><<<(unsigned)((h->ntot + 255) / 256), 256, 0, h->st>>>(g, src, tmp);
+    s = tmp;
+  }
+  YJobs<T> jb;
+  memset(&jb, 0, sizeof jb);
+  jb.j[0] = YJob<T>{s, nullptr, dst, op == 2 ? 1 : 0};
+  launch_y<T>(h, fs, jb, 1, h->nz, false);
+  typedef typename cplx_t<T>::type C;
+  const int M = h->nx / 2;
+  size_t smem = 2 * (size_t)M * sizeof(C);
+  if (op == 1) {
+    // multiply by i kx in (kx,y) space
+    k_mulikx<T><<<(unsigned)((h->ntot / 2 + 255) / 256), 256, 0, h->st>>>(g, dst);
+  }
+  k_xfft_field<T><<<h->ny * h->nz, 128, smem, h->st>>>(g, dst, h->nz, 1, h->plx, fs.Wm, fs.Wn);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+template <typename T>
+__global__ void k_mean_profiles(Geo g, const T* u, const T* v, const T* w, const T* t, double* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= g.nz) return;
+  size_t p = (size_t)k * g.plane;
+  out[k] = (double)u[p];
+  out[g.nz + k] = (double)v[p];
+  out[2 * g.nz + k] = (double)w[p];
+  out[3 * g.nz + k] = (double)t[p];
+}
+
+template <typename T>
+int horfft_dev(iw_handle* h, FieldSet<T>& fs, T* b, int is, int nk) {
+  Geo g = geo(h);
+  typedef typename cplx_t<T>::type C;
+  const int M = h->nx / 2;
+  size_t smem = 2 * (size_t)M * sizeof(C);
+  YJobs<T> jb;
+  memset(&jb, 0, sizeof jb);
+  if (is == -1) {
+    k_xfft_field<T><<<h->ny * nk, 128, smem, h->st>>>(g, b, nk, 0, h->plx, fs.Wm, fs.Wn);
+    jb.j[0] = YJob<T>{b, nullptr, b, 2};
+    launch_y<T>(h, fs, jb, 1, nk, false);
+  } else {
+    jb.j[0] = YJob<T>{b, nullptr, b, 0};
+    launch_y<T>(h, fs, jb, 1, nk, false);
+    k_xfft_field<T><<<h->ny * nk, 128, smem, h->st>>>(g, b, nk, 1, h->plx, fs.Wm, fs.Wn);
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+uint64_t xs_next(uint64_t& s) {
+  s ^= s << 21;
+  s ^= s >> 35;
+  s ^= s << 4;
+  return s;
+}
+
+// per-call device scratch of n doubles
+struct DBuf {
+  double* p = nullptr;
+  explicit DBuf(size_t n) { cudaMalloc(&p, n * sizeof(double) + 16); }
+  ~DBuf() { cudaFree(p); }
+};
+
+iw_handle* bound() {
+  if (!g_bound) set_err(IW_ERR_STATE, "no handle bound (iw_bind)");
+  return g_bound;
+}
+
+double g_setup_eps = -1.0;
+
+// one penalty system for eps and BCs, assembled, factored (1 warp), and
+// used to solve for nr right-hand sides b[r*nz + k] (device).
+__global__ void k_solve_one(Geo g, const double* ab, const int* ipiv, double* b, int nr) {
+  extern __shared__ double sb[];
+  const int n = g.nz;
+  for (int t = threadIdx.x; t < nr * n; t += 32) sb[t] = b[t];
+  __syncwarp();
+  band_solve_warp(ab, ipiv, sb, nr, n, g.N, g.N, threadIdx.x);
+  for (int t = threadIdx.x; t < nr * n; t += 32) b[t] = sb[t];
+}
+
+__global__ void k_legen_one(Geo g, const double* wg, const double* alpol, const double* sigma, double* b, int N) {
+  legen_filter_cols(b, 1, N, N, 1, wg, alpol, sigma, threadIdx.x);
+}
+
+int factor_dense_or_params(iw_handle* h, const double* pen6, double eps, int bot, int top, const double* dense,
+                           double** ab_out, int** ipiv_out) {
+  const int n = h->nz, N = h->N, ldab = 3 * N + 1, ns = h->ns;
+  SysDesc sd;
+  memset(&sd, 0, sizeof sd);
+  sd.eps = eps;
+  sd.ifbcbot = bot;
+  sd.ifbctop = top;
+  SysDesc* dsd;
+  double *dpen, *dab;
+  int *dip, *dinfo;
+  CK(cudaMalloc(&dsd, sizeof sd));
+  CK(cudaMalloc(&dpen, 6 * ns * sizeof(double)));
+  CK(cudaMalloc(&dab, (size_t)ldab * n * sizeof(double)));
+  CK(cudaMalloc(&dip, n * sizeof(int)));
+  CK(cudaMalloc(&dinfo, sizeof(int)));
+  CK(cudaMemcpy(dsd, &sd, sizeof sd, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dpen, pen6, 6 * ns * sizeof(double), cudaMemcpyHostToDevice));
+  FactorArgs fa;
+  fa.sys = dsd;
+  fa.pen = dpen;
+  fa.ab = dab;
+  fa.ipiv = dip;
+  fa.info = dinfo;
+  fa.nsys = 1;
+  fa.D = h->dD;
+  fa.D2 = h->dD2;
+  fa.zh = h->dzh;
+  fa.assemble = 1;
+  if (dense) {
+    // band_lu.f:19-34 packing done on the host
+    std::vector<double> ab((size_t)ldab * n, 0.0);
+    for (int j = 1; j <= n; ++j)
+      for (int i = std::max(1, j - N); i <= std::min(n, j + N); ++i)
+        ab[(size_t)(2 * N + i - j) + (size_t)ldab * (j - 1)] = dense[(size_t)(i - 1) + (size_t)n * (j - 1)];
+    CK(cudaMemcpy(dab, ab.data(), ab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    fa.assemble = 0;
+  }
+  k_factor<<<1, 32, 0, h->st>>>(geo(h), fa);
+  CK(cudaStreamSynchronize(h->st));
+  cudaFree(dsd);
+  cudaFree(dpen);
+  cudaFree(dinfo);
+  *ab_out = dab;
+  *ipiv_out = dip;
+  return 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// K_A..K_E and the solves as the reference's two calls
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void convec_(const int* istep, const int* istart, const int* ispecfilternl) {
+  iw_handle* h = bound();
+  if (!h) return;
+  (void)istart;
+  int save = h->p.ispecfilternl;
+  if (ispecfilternl) h->p.ispecfilternl = *ispecfilternl;
+  if (istep) h->istep = *istep;
+  if (h->mixed)
+    convec_impl<float>(h, h->f32, 0);
+  else
+    convec_impl<double>(h, h->f64, 0);
+  h->p.ispecfilternl = save;
+}
+
+void calcuvwt_(const int* izmode, const int* ispecfilter, const int* irelax, const int* cpenspecfilter) {
+  (void)izmode;
+  (void)ispecfilter;
+  (void)irelax;
+  iw_handle* h = bound();
+  if (!h) return;
+  if (ensure_factors(h)) return;
+  int cpen = cpenspecfilter ? (*cpenspecfilter != 0) : 1;
+  if (h->mixed)
+    calcuvwt_impl<float>(h, h->f32, cpen);
+  else
+    calcuvwt_impl<double>(h, h->f64, cpen);
+}
+
+void horfft_(double* b, const int* is, const int* nk) {
+  iw_handle* h = bound();
+  if (!h || !b || !is || !nk) return;
+  size_t n = h->plane * (size_t)*nk;
+  DBuf d(n);
+  cudaMemcpy(d.p, b, n * sizeof(double), cudaMemcpyHostToDevice);
+  FieldSet<double> tmp;
+  typedef double2 C;
+  int M = h->nx / 2;
+  auto wm = twiddles<C>(M, M);
+  auto wn = twiddles<C>(h->nx, M + 1);
+  auto wy = twiddles<C>(h->ny, h->ny);
+  if (up(h, &tmp.Wm, wm) || up(h, &tmp.Wn, wn) || up(h, &tmp.Wy, wy)) return;
+  horfft_dev<double>(h, tmp, d.p, *is, *nk);
+  cudaStreamSynchronize(h->st);
+  cudaMemcpy(b, d.p, n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(tmp.Wm);
+  cudaFree(tmp.Wn);
+  cudaFree(tmp.Wy);
+}
+
+void dpdz_(const double* a, double* b) {
+  iw_handle* h = bound();
+  if (!h || !a || !b) return;
+  DBuf da(h->ntot), db(h->ntot);
+  cudaMemcpy(da.p, a, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
+  k_dz_field<double><<<(unsigned)((h->ntot + 255) / 256), 256, 0, h->st>>>(geo(h), da.p, db.p);
+  cudaStreamSynchronize(h->st);
+  cudaMemcpy(b, db.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
+}
+
+void filter_3dlegenfourier_(double* f, const int* ifourier, const int* ilegen, const int* iout) {
+  (void)iout;
+  iw_handle* h = bound();
+  if (!h || !f) return;
+  DBuf d(h->ntot);
+  cudaMemcpy(d.p, f, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
+  long total = (long)h->nxpp * h->ny * h->ns;
+  k_filter_field<double><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(geo(h), d.p, ifourier ? *ifourier : 1,
+                                                                            ilegen ? *ilegen : 1);
+  cudaStreamSynchronize(h->st);
+  cudaMemcpy(f, d.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
+}
+
+void filter_legenpen_(const double* fin, double* fout, const double* ybar, const int* iprt, const int* ks) {
+  (void)ybar;
+  (void)iprt;
+  (void)ks;
+  iw_handle* h = bound();
+  if (!h || !fin || !fout) return;
+  DBuf d(h->N);
+  cudaMemcpy(d.p, fin, h->N * sizeof(double), cudaMemcpyHostToDevice);
+  k_legen_one<<<1, 32, 0, h->st>>>(geo(h), h->dwg, h->dal, h->dsig, d.p, h->N);
+  cudaStreamSynchronize(h->st);
+  cudaMemcpy(fout, d.p, h->N * sizeof(double), cudaMemcpyDeviceToHost);
+}
+
+void interface_avg3d_(double* f, int* ic) {
+  iw_handle* h = bound();
+  if (!h || !f) return;
+  FieldSet<double> fs;
+  DBuf d(h->ntot), G(h->plane * 16 * (size_t)std::max(1, h->ns - 1));
+  typedef double2 C;
+  int M = h->nx / 2;
+  auto wm = twiddles<C>(M, M);
+  auto wn = twiddles<C>(h->nx, M + 1);
+  auto wy = twiddles<C>(h->ny, h->ny);
+  if (up(h, &fs.Wm, wm) || up(h, &fs.Wn, wn) || up(h, &fs.Wy, wy)) return;
+  cudaMemcpy(d.p, f, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
+  for (int q = 0; q < 4; ++q) fs.F[q] = d.p;
+  fs.G = G.p;
+  iface_avg<double>(h, fs, true, 1);
+  cudaStreamSynchronize(h->st);
+  cudaMemcpy(f, d.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
+  if (ic) {
+    int cnt[4];
+    cudaMemcpy(cnt, h->dcnt, sizeof cnt, cudaMemcpyDeviceToHost);
+    *ic = cnt[0];
+  }
+  fs.F[0] = fs.F[1] = fs.F[2] = fs.F[3] = nullptr;
+  fs.G = nullptr;
+  cudaFree(fs.Wm);
+  cudaFree(fs.Wn);
+  cudaFree(fs.Wy);
+  fs.Wm = fs.Wn = fs.Wy = nullptr;
+}
+
+void penalty_setup_(const double* epsilon) {
+  if (epsilon) g_setup_eps = *epsilon;
+}
+
+void penalty_main_(const double* epsilon, const int* ifuncreal, const double* bcrbot, const double* bcibot,
+                   const double* bcrtop, const double* bcitop, const int* ifbcbot, const int* ifbctop, double* rhsinr,
+                   double* rhsini, double* fr, double* fi) {
+  (void)ifuncreal;
+  iw_handle* h = bound();
+  if (!h) return;
+  const int n = h->nz, ns = h->ns;
+  const double eps = *epsilon;
+  std::vector<double> pen(6 * ns), pen_int(6 * ns);
+  h_penalty(ns, h->N, h->p, eps, *ifbcbot, *ifbctop, pen.data());
+  if (g_setup_eps > 0 && g_setup_eps != eps) {
+    // interior subdomains keep the parameters of the last penalty_setup
+    h_penalty(ns, h->N, h->p, g_setup_eps, *ifbcbot, *ifbctop, pen_int.data());
+    for (int a = 0; a < 6; ++a)
+      for (int ks = 1; ks < ns - 1; ++ks) pen[a * ns + ks] = pen_int[a * ns + ks];
+  }
+  for (int k = 0; k < n; ++k) {
+    rhsinr[k] = -(rhsinr[k] * eps);
+    rhsini[k] = -(rhsini[k] * eps);
+  }
+  std::vector<double> b(2 * (size_t)n);
+  for (int k = 0; k < n; ++k) {
+    b[k] = rhsinr[k];
+    b[n + k] = rhsini[k];
+  }
+  const double t1 = pen[4 * ns + 0], t2 = pen[5 * ns + ns - 1];
+  if (*ifbcbot == 0) {
+    b[0] = rhsinr[0] + t1 * *bcrbot;
+    b[n] = rhsini[0] + t1 * *bcibot;
+  } else {
+    b[0] = rhsinr[0] - t1 * *bcrbot * eps;
+    b[n] = rhsini[0] - t1 * *bcibot * eps;
+  }
+  if (*ifbctop == 0) {
+    b[n - 1] = rhsinr[n - 1] + t2 * *bcrtop;
+    b[2 * n - 1] = rhsini[n - 1] + t2 * *bcitop;
+  } else {
+    b[n - 1] = rhsinr[n - 1] + t2 * *bcrtop * eps;
+    b[2 * n - 1] = rhsini[n - 1] + t2 * *bcitop * eps;
+  }
+  double* dab;
+  int* dip;
+  if (factor_dense_or_params(h, pen.data(), eps, *ifbcbot, *ifbctop, nullptr, &dab, &dip)) return;
+  DBuf db(2 * (size_t)n);
+  cudaMemcpy(db.p, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice);
+  k_solve_one<<<1, 32, 2 * n * sizeof(double), h->st>>>(geo(h), dab, dip, db.p, 2);
+  cudaStreamSynchronize(h->st);
+  cudaMemcpy(b.data(), db.p, b.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  for (int k = 0; k < n; ++k) {
+    fr[k] = b[k];
+    fi[k] = b[n + k];
+  }
+  cudaFree(dab);
+  cudaFree(dip);
+}
+
+void bandlu_solve_(const double* ain, double* xr, double* xi, const int* ifuncreal) {
+  iw_handle* h = bound();
+  if (!h) return;
+  const int n = h->nz;
+  std::vector<double> pen(6 * h->ns, 0.0);
+  double* dab;
+  int* dip;
+  if (factor_dense_or_params(h, pen.data(), 1.0, 0, 0, ain, &dab, &dip)) return;
+  int nr = (ifuncreal && *ifuncreal == 1) ? 1 : 2;
+  std::vector<double> b(2 * (size_t)n);
+  for (int k = 0; k < n; ++k) {
+    b[k] = xr[k];
+    b[n + k] = xi ? xi[k] : 0.0;
+  }
+  DBuf db(2 * (size_t)n);
+  cudaMemcpy(db.p, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice);
+  k_solve_one<<<1, 32, 2 * n * sizeof(double), h->st>>>(geo(h), dab, dip, db.p, nr);
+  cudaStreamSynchronize(h->st);
+  cudaMemcpy(b.data(), db.p, b.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  for (int k = 0; k < n; ++k) {
+    xr[k] = b[k];
+    if (xi && nr == 2) xi[k] = b[n + k];
+  }
+  cudaFree(dab);
+  cudaFree(dip);
+}
+
+// multistep.f:7-89
+double abvar1_(const double* a, const double* b, const double* c) {
+  double dt1 = *a, dt2 = *b, dt3 = *c;
+  double dt123 = 2. * dt1 + 6. * dt2 + 3. * dt3, dt23 = dt2 + dt3;
+  return 1. + dt1 * dt123 / (6. * dt2 * dt23);
+}
+double abvar2_(const double* a, const double* b, const double* c) {
+  double dt1 = *a, dt2 = *b, dt3 = *c;
+  double dt123 = 2. * dt1 + 3. * dt2 + 3. * dt3;
+  return -dt1 * dt123 / (6. * dt2 * dt3);
+}
+double abvar3_(const double* a, const double* b, const double* c) {
+  double dt1 = *a, dt2 = *b, dt3 = *c;
+  double dt12 = 2. * dt1 + 3. * dt2, dt23 = dt2 + dt3;
+  return dt1 * dt12 / (6. * dt3 * dt23);
+}
+double bdfvarv_(const double* a, const double* b, const double* c) {
+  double dt1 = *a, dt2 = *b, dt3 = *c;
+  double dt12 = dt1 + dt2, dt123 = dt1 + dt2 + dt3;
+  return 1. + dt1 / dt12 + dt1 / dt123;
+}
+double bdfvar1_(const double* a, const double* b, const double* c) {
+  double dt1 = *a, dt2 = *b, dt3 = *c;
+  double dt12 = dt1 + dt2, dt23 = dt2 + dt3, dt123 = dt1 + dt2 + dt3;
+  double r = -1. - dt1 / dt2 - dt1 / dt123 - dt1 * dt1 / (dt123 * dt2) - dt1 * dt1 * dt12 / (dt123 * dt23 * dt2);
+  return -r;
+}
+double bdfvar2_(const double* a, const double* b, const double* c) {
+  double dt1 = *a, dt2 = *b, dt3 = *c;
+  double dt12 = dt1 + dt2, dt23 = dt2 + dt3, dt123 = dt1 + dt2 + dt3;
+  double r = dt1 * dt1 / (dt12 * dt2) + dt1 * dt1 / (dt2 * dt123) + dt1 * dt1 * dt12 / (dt2 * dt23 * dt123) +
+             dt1 * dt1 * dt12 / (dt3 * dt23 * dt123);
+  return -r;
+}
+double bdfvar3_(const double* a, const double* b, const double* c) {
+  double dt1 = *a, dt2 = *b, dt3 = *c;
+  double dt12 = dt1 + dt2, dt23 = dt2 + dt3, dt123 = dt1 + dt2 + dt3;
+  double r = -dt1 * dt1 * dt12 / (dt3 * dt23 * dt123);
+  return -r;
+}
+
+// ---------------------------------------------------------------------------
+int iw_init_mode1(iw_handle* h, double A, double anoise, uint64_t seed) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  cudaSetDevice(h->dev);
+  const int nx = h->nx, ny = h->ny, nz = h->nz, nxpp = h->nxpp;
+  const double pi2 = 8. * std::atan(1.0);
+  const double kx = pi2 / h->p.xlen, m = pi2 / (2. * h->p.zlen);
+  const double om = (h->p.brunt * kx) / std::sqrt(kx * kx + m * m);
+  const double rc = (h->p.rho0 * h->p.brunt * h->p.brunt) / h->p.grav;
+  const double xl = pi2 / (pi2 / h->p.xlen);
+  std::vector<double> zg(nz);
+  for (int ks = 0; ks < h->ns; ++ks)
+    for (int kl = 0; kl < h->N; ++kl) zg[ks * h->N + kl] = h->p.z0[ks] + 0.5 * h->p.zh[ks] * (h->tab.zpts[kl] + 1.0);
+  std::vector<double> st(4 * h->ntot, 0.0);
+  auto at = [&](int q, int i, int j, int k) -> double& {
+    return st[(size_t)q * h->ntot + (size_t)i + (size_t)nxpp * ((size_t)j + (size_t)ny * k)];
+  };
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        double x = i * xl / nx, z = zg[k];
+        at(0, i, j, k) = -(A / kx) * m * std::cos(m * z) * std::sin(kx * x);
+        at(2, i, j, k) = A * std::sin(m * z) * std::cos(kx * x);
+        at(3, i, j, k) = -(A / om) * rc * std::sin(m * z) * std::sin(kx * x);
+      }
+  uint64_t s = seed ? seed : 0x9E3779B97F4A7C15ULL;
+  for (int k = 0; k < nz; ++k) {
+    if (!(zg[k] < 0.2 * h->p.zlen)) continue;
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i)
+        for (int q = 0; q < 3; ++q) {
+          uint64_t v = xs_next(s);
+          double r = (double)(int64_t)v * 5.42101086242752217e-20 + 0.5;
+          at(q, i, j, k) += anoise * (2.0 * r - 1.0);
+        }
+  }
+  std::vector<double> zero(4 * h->ntot, 0.0);
+  int r = iw_upload_state(h, st.data(), zero.data(), zero.data(), zero.data(), zero.data(), 0.0, 0);
+  if (r) return r;
+  for (int q = 0; q < 4; ++q) {
+    if (h->mixed)
+      horfft_dev<float>(h, h->f32, h->f32.F[q], -1, nz);
+    else
+      horfft_dev<double>(h, h->f64, h->f64.F[q], -1, nz);
+  }
+  CK(cudaMemsetAsync(h->dwnl, 0, h->plane * 2 * sizeof(double), h->st));
+  CK(cudaMemsetAsync(h->dwvr, 0, h->plane * 2 * sizeof(double), h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return IW_OK;
+}
+
+}  // extern "C"
+
+template <typename T>
+static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
+  Geo g = geo(h);
+  T* dst = fs.Y12[0];
+  T* tmp = fs.Y12[1];
+  CK(cudaMemsetAsync(h->dred, 0, 8 * sizeof(double), h->st));
+  // KE: u,v,w ; eps: 9 gradients
+  for (int q = 0; q < 3; ++q) {
+    phys_of<T>(h, fs, fs.F[q], dst, tmp, 0);
+    k_reduce_sq<T><<<296, 256, 0, h->st>>>(g, dst, 1, h->dred + 0);
+    for (int op = 1; op <= 3; ++op) {
+      phys_of<T>(h, fs, fs.F[q], dst, tmp, op);
+      k_reduce_sq<T><<<296, 256, 0, h->st>>>(g, dst, 1, h->dred + 1);
+    }
+  }
+  double red[8];
+  CK(cudaMemcpyAsync(red, h->dred, sizeof red, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  memset(out, 0, sizeof *out);
+  out->ke = 0.5 * red[0];
+  out->eps = h->p.xnu * red[1];
+  out->t = h->t;
+  out->istep = h->istep;
+  int cnt[4] = {0, 0, 0, 0};
+  CK(cudaMemcpy(cnt, h->dcnt, sizeof cnt, cudaMemcpyDeviceToHost));
+  for (int q = 0; q < 4; ++q) out->interface_avg_count[q] = cnt[q];
+  // non-finite check of the state
+  CK(cudaMemsetAsync(h->dflag, 0, sizeof(int), h->st));
+  for (int q = 0; q < 4; ++q) k_nonfinite<T><<<296, 256, 0, h->st>>>(fs.F[q], h->ntot, h->dflag);
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->dflag, sizeof flag, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (flag) return set_err(IW_ERR_NONFINITE, "non-finite value in the state");
+  return IW_OK;
+}
+
+extern "C" {
+
+int iw_diag(iw_handle* h, iw_diag_out* out) {
+  if (!h || !out) return set_err(IW_ERR_STATE, "bad argument");
+  cudaSetDevice(h->dev);
+  return h->mixed ? diag_impl<float>(h, h->f32, out) : diag_impl<double>(h, h->f64, out);
+}
+
+// Mean (kx=ky=0) vertical profiles of u,v,w,rho copied to the host: the
+// per-step result a driver reads back.
+int iw_mean_profiles(iw_handle* h, double* host4nz) {
+  if (!h || !host4nz) return set_err(IW_ERR_STATE, "bad argument");
+  cudaSetDevice(h->dev);
+  Geo g = geo(h);
+  unsigned nb = (unsigned)((h->nz + 127) / 128);
+  if (h->mixed)
+    k_mean_profiles<float><<<nb, 128, 0, h->st>>>(g, h->f32.F[0], h->f32.F[1], h->f32.F[2], h->f32.F[3], h->dred);
+  else
+    k_mean_profiles<double><<<nb, 128, 0, h->st>>>(g, h->f64.F[0], h->f64.F[1], h->f64.F[2], h->f64.F[3], h->dred);
+  CK(cudaMemcpyAsync(host4nz, h->dred, 4 * (size_t)h->nz * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return IW_OK;
+}
+
+// Isolated batched solves: one system per column with lambda = lam[c].
+int iw_helm_solve_batched(iw_handle* h, const double* lam_dev, int ncol, int ifbcbot, int ifbctop,
+                          const double* rhs_dev, double* sol_dev, int mode) {
+  if (!h || !lam_dev || !rhs_dev || !sol_dev || ncol <= 0) return set_err(IW_ERR_STATE, "bad argument");
+  cudaSetDevice(h->dev);
+  return helm_batched(h, lam_dev, ncol, ifbcbot, ifbctop, rhs_dev, sol_dev, mode);
+}
+
+}  // extern "C"

@@ -1,0 +1,1376 @@
+// Host side of the library: setup tables, handle, step orchestration, C ABI.
+// Included at the end of iw_lib.cu (it launches the kernels defined there).
+//
+// Host setup code is compiled without floating-point contraction
+// (-Xcompiler -ffp-contract=off) so the tables equal the ones the reference
+// builds (setup.f, penalty.f param_set) bit for bit.
+
+namespace {
+
+// --------------------------------------------------------------------------
+// setup.f restated for the host (GLL points, weights, Legendre table,
+// Costa-Don derivative matrix).
+// --------------------------------------------------------------------------
+void h_legen(std::vector<double>& al, int n, double xc) {
+  al.assign(n + 2, 0.0);
+  al[0] = 1.;
+  al[1] = xc;
+  for (int k = 1; k <= n; ++k) {
+    int kp = k + 1, km = k - 1;
+    al[kp] = (2. * k + 1.) * xc * al[k] / kp - k * al[km] / kp;
+  }
+}
+
+void h_jacobf(int n, double& poly, double& pder, double& polym1, double& pderm1, double& polym2, double& pderm2,
+              double x) {
+  poly = 1.0;
+  pder = 0.0;
+  if (n == 0) return;
+  double polylst = poly, pderlst = pder;
+  poly = x;
+  pder = 1.0;
+  if (n == 1) return;
+  double psave = 0, pdsave = 0;
+  for (int k = 2; k <= n; ++k) {
+    double a1 = 2. * k * (k + 0.0) * (2. * k + 0.0 - 2.);
+    double a2 = (2. * k + 0.0 - 1.) * (0.0);
+    double b3 = (2. * k + 0.0 - 2.);
+    double a3 = b3 * (b3 + 1.) * (b3 + 2.);
+    double a4 = 2. * (k + 0.0 - 1.) * (k + 0.0 - 1.) * (2. * k + 0.0);
+    double polyn = ((a2 + a3 * x) * poly - a4 * polylst) / a1;
+    double pdern = ((a2 + a3 * x) * pder - a4 * pderlst + a3 * poly) / a1;
+    psave = polylst;
+    pdsave = pderlst;
+    polylst = poly;
+    poly = polyn;
+    pderlst = pder;
+    pder = pdern;
+  }
+  polym1 = polylst;
+  pderm1 = pderlst;
+  polym2 = psave;
+  pderm2 = pdsave;
+}
+
+void h_jacobl(int n, std::vector<double>& xcol) {
+  std::vector<double> xjac(n + 3, 0.0);
+  int np = n + 1;
+  double pnp1p, pdnp1p, pnp, pdnp, pnm1p, pdnm1, pnp1m, pdnp1m, pnm, pdnm, pnm1m;
+  h_jacobf(np, pnp1p, pdnp1p, pnp, pdnp, pnm1p, pdnm1, 1.0);
+  h_jacobf(np, pnp1m, pdnp1m, pnm, pdnm, pnm1m, pdnm1, -1.0);
+  double det = pnp * pnm1m - pnm * pnm1p;
+  double rp = -pnp1p, rm = -pnp1m;
+  double a = (rp * pnm1m - rm * pnm1p) / det;
+  double b = (rm * pnp - rp * pnm) / det;
+  xjac[1] = 1.0;
+  int nh = (n + 1) / 2;
+  double dth = 3.14159265 / (2 * n + 1);
+  double cd_ = std::cos(2. * dth), sd = std::sin(2. * dth), cs = std::cos(dth), ss = std::sin(dth);
+  for (int j = 2; j <= nh; ++j) {
+    double x = cs;
+    for (int k = 1; k <= 10; ++k) {
+      double pnp1, pdnp1, pn, pdn, pnm1;
+      h_jacobf(np, pnp1, pdnp1, pn, pdn, pnm1, pdnm1, x);
+      double poly = pnp1 + a * pn + b * pnm1;
+      double pder = pdnp1 + a * pdn + b * pdnm1;
+      double recsum = 0.0;
+      for (int i = 1; i <= j - 1; ++i) recsum = recsum + 1.0 / (x - xjac[i]);
+      double delx = -poly / (pder - recsum * poly);
+      x = x + delx;
+      if (std::fabs(delx) < 1.0e-12) break;
+    }
+    xjac[j] = x;
+    double cssave = cs * cd_ - ss * sd;
+    ss = cs * sd + ss * cd_;
+    cs = cssave;
+  }
+  xjac[np] = -1.0;
+  for (int i = 2; i <= nh; ++i) xjac[n + 2 - i] = -xjac[i];
+  if (n % 2 == 0) xjac[nh + 1] = 0.0;
+  xcol.assign(n + 1, 0.0);
+  for (int k = 0; k <= n; ++k) xcol[k] = xjac[n - k + 1];
+}
+
+struct Tables {
+  std::vector<double> zpts, wg, alpol, D, D2, sigma, Lfil;
+};
+
+Tables h_tables(int N, double p, double amp, double fackc) {
+  Tables t;
+  int n = N - 1;
+  h_jacobl(n, t.zpts);
+  t.wg.assign(N, 0.0);
+  t.alpol.assign((size_t)N * N, 0.0);
+  std::vector<double> al;
+  for (int k = 0; k <= n; ++k) {
+    h_legen(al, n, t.zpts[k]);
+    t.wg[k] = 2. / ((double)(n * (n + 1)) * al[n] * al[n] + 1.0e-30);
+    for (int j = 0; j <= n; ++j) t.alpol[(size_t)j * N + k] = al[j];
+  }
+  std::vector<double> c(N);
+  const auto& x = t.zpts;
+  for (int k = 0; k <= n; ++k) {
+    double prod = 1.;
+    for (int l = 0; l <= n; ++l)
+      if (l != k) prod = prod * (x[k] - x[l]);
+    c[k] = prod;
+  }
+  t.D.assign((size_t)N * N, 0.0);
+  t.D2 = t.D;
+  for (int k = 0; k <= n; ++k)
+    for (int j = 0; j <= n; ++j) t.D[k * N + j] = (k != j) ? c[k] / (c[j] * (x[k] - x[j])) : 0.;
+  for (int k = 0; k <= n; ++k) {
+    double s = 0.;
+    for (int j = 0; j <= n; ++j)
+      if (k != j) s = s + t.D[k * N + j];
+    t.D[k * N + k] = -s;
+  }
+  for (int k = 0; k <= n; ++k)
+    for (int j = 0; j <= n; ++j)
+      t.D2[k * N + j] = (k != j) ? 2.0 * (t.D[k * N + k] * t.D[k * N + j] - t.D[k * N + j] / (x[k] - x[j])) : 0.;
+  for (int k = 0; k <= n; ++k) {
+    double s = 0.;
+    for (int j = 0; j <= n; ++j)
+      if (k != j) s = s + t.D2[k * N + j];
+    t.D2[k * N + k] = -s;
+  }
+  // specfilter (filtering.f:1225-1243)
+  int kc = (int)(fackc * n);
+  t.sigma.assign(N, 1.0);
+  for (int k = 0; k <= n; ++k)
+    if (k >= kc) {
+      double theta = (double)(k - kc) / (double)(n - kc);
+      t.sigma[k] = std::exp(-amp * std::pow(theta, 2. * p));
+    }
+  // precombined filter: out(k1) = sum_j L(k1,j) f(j)
+  t.Lfil.assign((size_t)N * N, 0.0);
+  for (int k1 = 0; k1 < N; ++k1)
+    for (int jj = 0; jj < N; ++jj) {
+      long double s = 0;
+      for (int k = 0; k <= n; ++k) {
+        long double ck = (k == n) ? 0.5L * n : (k + 0.5L);
+        s += (long double)t.alpol[(size_t)k * N + k1] * t.sigma[k] * ck * t.wg[jj] * t.alpol[(size_t)k * N + jj];
+      }
+      t.Lfil[k1 * N + jj] = (double)s;
+    }
+  return t;
+}
+
+// penalty.f:57-157 param_set
+void h_param_set(double omega, const iw_params& pp, int ifbc, double& a0, double& b0, double& t0, double eps,
+                 double ybar) {
+  if (ifbc == 0) {
+    a0 = 1.;
+    b0 = 0.;
+    double fac = pp.facdir * ((2. / ybar) * (2. / ybar));
+    t0 = fac * eps / (a0 * (omega * omega));
+  } else if (ifbc == 1) {
+    a0 = 0.;
+    b0 = 1.;
+    double fac = pp.facneumn * 2. / ybar;
+    t0 = fac / (b0 * omega);
+  } else {
+    a0 = 1.;
+    b0 = 1.;
+    double ck = a0 * omega / b0;
+    double dn = 1. / (omega * eps * b0);
+    double t1 = std::sqrt(ck * ck + eps * ck);
+    double t2 = 2. * ck - 2. * t1;
+    double facm = ((1. / eps) >= 1.e5) ? pp.facrobin : 1.;
+    t0 = facm * dn * (eps + t2) * 2. / ybar;
+  }
+}
+
+// all penalty parameters of one system (penalty_setup + penalty_main ends)
+void h_penalty(int ns, int N, const iw_params& pp, double eps, int bot, int top, double* out /*6*ns*/) {
+  double omega = 2. / (double)((N + 1) * (N + 2));
+  double *pa = out, *pb = out + ns, *pg = out + 2 * ns, *pd = out + 3 * ns, *pt1 = out + 4 * ns, *pt2 = out + 5 * ns;
+  for (int i = 0; i < 6 * ns; ++i) out[i] = 0.0;
+  double a0, b0, t0;
+  for (int ks = 1; ks < ns - 1; ++ks) {
+    h_param_set(omega, pp, 2, a0, b0, t0, eps, pp.zh[ks]);
+    pa[ks] = a0;
+    pb[ks] = b0;
+    pt1[ks] = t0;
+    pg[ks] = a0;
+    pd[ks] = b0;
+    pt2[ks] = t0;
+  }
+  h_param_set(omega, pp, bot, a0, b0, t0, eps, pp.zh[0]);
+  pa[0] = a0;
+  pb[0] = b0;
+  pt1[0] = t0;
+  if (ns > 1) {
+    h_param_set(omega, pp, 2, a0, b0, t0, eps, pp.zh[0]);
+    pg[0] = a0;
+    pd[0] = b0;
+    pt2[0] = t0;
+  }
+  h_param_set(omega, pp, top, a0, b0, t0, eps, pp.zh[ns - 1]);
+  pg[ns - 1] = a0;
+  pd[ns - 1] = b0;
+  pt2[ns - 1] = t0;
+  if (ns > 1) {
+    h_param_set(omega, pp, 2, a0, b0, t0, eps, pp.zh[ns - 1]);
+    pa[ns - 1] = a0;
+    pb[ns - 1] = b0;
+    pt1[ns - 1] = t0;
+  }
+}
+
+FftPlan make_plan(int M) {
+  FftPlan p;
+  memset(&p, 0, sizeof p);
+  p.M = M;
+  int m = M, ns = 1;
+  auto push = [&](int r) {
+    p.rad[p.npass] = r;
+    p.ns[p.npass] = ns;
+    ns *= r;
+    p.npass++;
+  };
+  while (m % 4 == 0) {
+    push(4);
+    m /= 4;
+  }
+  while (m % 2 == 0) {
+    push(2);
+    m /= 2;
+  }
+  while (m % 3 == 0) {
+    push(3);
+    m /= 3;
+  }
+  while (m % 5 == 0) {
+    push(5);
+    m /= 5;
+  }
+  if (m != 1) p.npass = -1;
+  return p;
+}
+
+template <typename C>
+std::vector<C> twiddles(int n, int count) {  // exp(-2 pi i e / n), e < count
+  std::vector<C> w(count);
+  for (int e = 0; e < count; ++e) {
+    long double a = -2.0L * 3.14159265358979323846264338327950288L * e / n;
+    w[e].x = (decltype(w[e].x))std::cos(a);
+    w[e].y = (decltype(w[e].x))std::sin(a);
+  }
+  return w;
+}
+
+// One system kind: 0 pressure, 1 u/v, 2 w, 3 rho.
+enum { SYS_P = 0, SYS_U, SYS_W, SYS_T, SYS_KINDS };
+
+}  // namespace
+
+// per-precision device buffers
+template <typename T>
+struct FieldSet {
+  T* F[4] = {0, 0, 0, 0};
+  T* Fn[4] = {0, 0, 0, 0};
+  T* Fnm[4] = {0, 0, 0, 0};
+  T* Sn[4] = {0, 0, 0, 0};
+  T* Snm[4] = {0, 0, 0, 0};
+  T* F1[4] = {0, 0, 0, 0};
+  T* Z4[4] = {0, 0, 0, 0};
+  T* Y12[12] = {0};
+  T* X11[11] = {0};
+  T* B8[8] = {0};
+  T* G = 0;  // interface planes
+  typename cplx_t<T>::type *Wm = 0, *Wn = 0, *Wy = 0;
+};
+
+struct iw_handle {
+  iw_dims d;
+  iw_params p;
+  int dev = 0;
+  cudaStream_t st = 0;
+  int nx, ny, nz, N, ns, nxpp, nxh, nxhp, nyh, ndims, ncol;
+  size_t ntot, plane;
+  bool mixed = false;
+  Tables tab;
+  // device tables
+  double *dD = 0, *dD2 = 0, *dL = 0, *dh = 0, *dxw = 0, *dyw = 0, *dcf = 0, *dzg = 0, *dzh = 0;
+  double *dwg = 0, *dal = 0, *dsig = 0, *dmeang = 0;
+  double *dwnl = 0, *dwvr = 0, *dred = 0;
+  int* dcnt = 0;
+  int* dflag = 0;
+  FftPlan plx, ply;
+  FieldSet<double> f64;
+  FieldSet<float> f32;
+  // systems
+  std::vector<double> akv;     // distinct kx^2+ky^2 values
+  std::vector<int> col_u;      // column -> distinct index
+  int nsys_kind[SYS_KINDS] = {0, 0, 0, 0};
+  double* dab[SYS_KINDS] = {0, 0, 0, 0};
+  int* dipiv[SYS_KINDS] = {0, 0, 0, 0};
+  int* dinfo[SYS_KINDS] = {0, 0, 0, 0};
+  SysDesc* dsys[SYS_KINDS] = {0, 0, 0, 0};
+  double* dpen[SYS_KINDS] = {0, 0, 0, 0};
+  int* dcolsys[SYS_KINDS] = {0, 0, 0, 0};
+  double fac_bdfv[SYS_KINDS] = {-1, -1, -1, -1};  // bdfv the factors were built for
+  double fac_dt[SYS_KINDS] = {-1, -1, -1, -1};
+  // time stepping
+  double t = 0;
+  int istep = 0;
+  Coefs c{1, 0, 0, 1, 0, 0, 1, 0};
+  int avg_count[4] = {0, 0, 0, 0};
+  size_t bytes = 0;
+  cudaGraphExec_t gexec = 0;
+  // helm batched
+  std::map<std::string, int> helm_keys;
+  // per-phase timing with CUDA events on the handle's stream
+  int prof = 0;
+  cudaEvent_t ev[32];
+  int nev = 0;
+  int ev_phase[32];
+  double phase_ms[16] = {0};
+  long phase_n[16] = {0};
+};
+
+// phases: 0 stageA, 1 yinv, 2 xrow, 3 yfwd, 4 wviscrot, 5 stageE, 6 press,
+// 7 visc_uv, 8 visc_w, 9 visc_t, 10 iface, 11 factor
+static void mark(iw_handle* h, int phase) {
+  if (!h->prof || h->nev >= 32) return;
+  cudaEventRecord(h->ev[h->nev], h->st);
+  h->ev_phase[h->nev] = phase;
+  h->nev++;
+}
+static void prof_flush(iw_handle* h) {
+  if (!h->prof || h->nev < 2) {
+    h->nev = 0;
+    return;
+  }
+  cudaEventSynchronize(h->ev[h->nev - 1]);
+  for (int i = 1; i < h->nev; ++i) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev[i - 1], h->ev[i]);
+    int ph = h->ev_phase[i];
+    h->phase_ms[ph] += ms;
+    h->phase_n[ph] += 1;
+  }
+  h->nev = 0;
+}
+
+static iw_handle* g_bound = nullptr;
+
+template <typename T>
+static int dalloc(iw_handle* h, T** p, size_t n) {
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return set_err(IW_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  h->bytes += n * sizeof(T);
+  return 0;
+}
+template <typename T>
+static int up(iw_handle* h, T** p, const std::vector<T>& v) {
+  int r = dalloc(h, p, v.size());
+  if (r) return r;
+  CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static double pi2_of(const iw_handle*) { return 8.0 * std::atan(1.0); }
+
+static Geo geo(const iw_handle* h) {
+  Geo g;
+  g.nx = h->nx;
+  g.ny = h->ny;
+  g.nz = h->nz;
+  g.N = h->N;
+  g.ns = h->ns;
+  g.nxpp = h->nxpp;
+  g.nxh = h->nxh;
+  g.nxhp = h->nxhp;
+  g.nyh = h->nyh;
+  g.plane = h->plane;
+  g.ntot = h->ntot;
+  g.scaley = 1. / (double)h->ny;
+  g.dt = h->p.dt;
+  g.D = h->dD;
+  g.Lfil = h->dL;
+  g.hfac = h->dh;
+  g.xw = h->dxw;
+  g.yw = h->dyw;
+  g.cfour = h->dcf;
+  g.zg = h->dzg;
+  return g;
+}
+
+template <typename T>
+static int alloc_fields(iw_handle* h, FieldSet<T>& fs) {
+  size_t n = h->ntot;
+  for (int q = 0; q < 4; ++q) {
+    for (T** p : {&fs.F[q], &fs.Fn[q], &fs.Fnm[q], &fs.Sn[q], &fs.Snm[q], &fs.F1[q], &fs.Z4[q]}) {
+      if (dalloc(h, p, n)) return IW_ERR_NOMEM;
+      CK(cudaMemset(*p, 0, n * sizeof(T)));
+    }
+  }
+  for (int q = 0; q < 12; ++q)
+    if (dalloc(h, &fs.Y12[q], n)) return IW_ERR_NOMEM;
+  for (int q = 0; q < 11; ++q)
+    if (dalloc(h, &fs.X11[q], n)) return IW_ERR_NOMEM;
+  for (int q = 0; q < 8; ++q)
+    if (dalloc(h, &fs.B8[q], n)) return IW_ERR_NOMEM;
+  if (h->ns > 1 && dalloc(h, &fs.G, h->plane * 16 * (size_t)(h->ns - 1))) return IW_ERR_NOMEM;
+  typedef typename cplx_t<T>::type C;
+  int M = h->nx / 2;
+  auto wm = twiddles<C>(M, M);
+  auto wn = twiddles<C>(h->nx, M + 1);
+  auto wy = twiddles<C>(h->ny, h->ny);
+  if (up(h, &fs.Wm, wm) || up(h, &fs.Wn, wn) || up(h, &fs.Wy, wy)) return IW_ERR_NOMEM;
+  return 0;
+}
+
+template <typename T>
+static void free_fields(FieldSet<T>& fs) {
+  for (int q = 0; q < 4; ++q)
+    for (T* p : {fs.F[q], fs.Fn[q], fs.Fnm[q], fs.Sn[q], fs.Snm[q], fs.F1[q], fs.Z4[q]}) cudaFree(p);
+  for (int q = 0; q < 12; ++q) cudaFree(fs.Y12[q]);
+  for (int q = 0; q < 11; ++q) cudaFree(fs.X11[q]);
+  for (int q = 0; q < 8; ++q) cudaFree(fs.B8[q]);
+  cudaFree(fs.G);
+  cudaFree(fs.Wm);
+  cudaFree(fs.Wn);
+  cudaFree(fs.Wy);
+}
+
+// ---------------------------------------------------------------------------
+// systems: distinct kx^2+ky^2 (the matrix of a column depends on it only)
+// ---------------------------------------------------------------------------
+static void build_distinct(iw_handle* h) {
+  std::vector<double> ak(h->ncol);
+  for (int j = 0; j < h->ny; ++j)
+    for (int ii = 0; ii < h->nxhp; ++ii) {
+      double xw = ii * (8.0 * std::atan(1.0) / h->p.xlen);
+      double ywv = 0.0;
+      if (h->ny > 1) {
+        double beta = 8.0 * std::atan(1.0) / h->p.ylen;
+        int jj = j + 1;  // 1-based
+        ywv = (jj <= h->nyh) ? (jj - 1) * beta : -(h->ny + 1 - jj) * beta;
+      }
+      ak[(size_t)j * h->nxhp + ii] = xw * xw + ywv * ywv;
+    }
+  std::vector<double> s = ak;
+  std::sort(s.begin(), s.end());
+  s.erase(std::unique(s.begin(), s.end()), s.end());
+  h->akv = s;
+  h->col_u.resize(h->ncol);
+  for (int c = 0; c < h->ncol; ++c) h->col_u[c] = (int)(std::lower_bound(s.begin(), s.end(), ak[c]) - s.begin());
+}
+
+static int kind_bcs(const iw_handle* h, int kind, int& bot, int& top) {
+  if (kind == SYS_P || kind == SYS_T) {
+    bot = 1;
+    top = 1;
+  } else if (kind == SYS_U) {
+    bot = h->p.bc_variant == IW_BC_NOSLIP ? 0 : 1;
+    top = 1;
+  } else {
+    bot = 0;
+    top = 0;
+  }
+  return 0;
+}
+
+// (re)build the factors of one kind for the current bdfv/dt
+static int build_factors(iw_handle* h, int kind) {
+  const int ns = h->ns, N = h->N, n = h->nz, ldab = 3 * N + 1;
+  const int nd = (int)h->akv.size();
+  int bot, top;
+  kind_bcs(h, kind, bot, top);
+  // distinct systems of this kind; pressure and w skip ak == 0
+  std::vector<int> dmap(nd, -1);
+  std::vector<SysDesc> sys;
+  std::vector<double> pen;
+  const double facvel = 1. / (h->p.xnu * h->p.dt), fact = 1. / (h->p.xkappa * h->p.dt);
+  for (int u = 0; u < nd; ++u) {
+    double ak = h->akv[u];
+    if ((kind == SYS_P || kind == SYS_W) && ak == 0.0) continue;
+    double eps;
+    if (kind == SYS_P)
+      eps = 1. / ak;
+    else if (kind == SYS_T)
+      eps = 1. / (ak + h->c.bdfv * fact);
+    else
+      eps = 1. / (ak + h->c.bdfv * facvel);
+    SysDesc sd;
+    memset(&sd, 0, sizeof sd);
+    sd.eps = eps;
+    sd.ifbcbot = bot;
+    sd.ifbctop = top;
+    std::vector<double> pp(6 * ns);
+    h_penalty(ns, N, h->p, eps, bot, top, pp.data());
+    sd.tau1_bot = pp[4 * ns + 0];
+    sd.tau2_top = pp[5 * ns + ns - 1];
+    dmap[u] = (int)sys.size();
+    sys.push_back(sd);
+    pen.insert(pen.end(), pp.begin(), pp.end());
+  }
+  std::vector<int> colsys(h->ncol);
+  for (int c = 0; c < h->ncol; ++c) colsys[c] = dmap[h->col_u[c]];
+  const int nsys = (int)sys.size();
+  if (h->nsys_kind[kind] != nsys) {
+    cudaFree(h->dab[kind]);
+    cudaFree(h->dipiv[kind]);
+    cudaFree(h->dinfo[kind]);
+    cudaFree(h->dsys[kind]);
+    cudaFree(h->dpen[kind]);
+    cudaFree(h->dcolsys[kind]);
+    h->dab[kind] = 0;
+    if (nsys > 0) {
+      if (dalloc(h, &h->dab[kind], (size_t)nsys * ldab * n) || dalloc(h, &h->dipiv[kind], (size_t)nsys * n) ||
+          dalloc(h, &h->dinfo[kind], (size_t)nsys) || dalloc(h, &h->dsys[kind], (size_t)nsys) ||
+          dalloc(h, &h->dpen[kind], (size_t)nsys * 6 * ns))
+        return IW_ERR_NOMEM;
+    }
+    if (dalloc(h, &h->dcolsys[kind], (size_t)h->ncol)) return IW_ERR_NOMEM;
+    h->nsys_kind[kind] = nsys;
+  }
+  if (nsys > 0) {
+    CK(cudaMemcpyAsync(h->dsys[kind], sys.data(), nsys * sizeof(SysDesc), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->dpen[kind], pen.data(), pen.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  }
+  CK(cudaMemcpyAsync(h->dcolsys[kind], colsys.data(), colsys.size() * sizeof(int), cudaMemcpyHostToDevice, h->st));
+  if (nsys > 0) {
+    FactorArgs fa;
+    fa.sys = h->dsys[kind];
+    fa.pen = h->dpen[kind];
+    fa.ab = h->dab[kind];
+    fa.ipiv = h->dipiv[kind];
+    fa.info = h->dinfo[kind];
+    fa.nsys = nsys;
+    fa.D = h->dD;
+    fa.D2 = h->dD2;
+    fa.zh = h->dzh;
+    int warps = 4;
+    k_factor<<<(nsys + warps - 1) / warps, 32 * warps, 0, h->st>>>(geo(h), fa);
+    CK(cudaGetLastError());
+    // host copies must stay alive until the copies finish
+    CK(cudaStreamSynchronize(h->st));
+    std::vector<int> info(nsys);
+    CK(cudaMemcpy(info.data(), h->dinfo[kind], nsys * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < nsys; ++s)
+      if (info[s] != 0) return set_err(IW_ERR_PIVOT, "zero pivot in band factorisation");
+  } else {
+    CK(cudaStreamSynchronize(h->st));
+  }
+  h->fac_bdfv[kind] = h->c.bdfv;
+  h->fac_dt[kind] = h->p.dt;
+  return 0;
+}
+
+static int ensure_factors(iw_handle* h) {
+  for (int k = 0; k < SYS_KINDS; ++k) {
+    bool need = h->fac_dt[k] != h->p.dt || (k != SYS_P && h->fac_bdfv[k] != h->c.bdfv);
+    if (h->fac_dt[k] < 0) need = true;
+    if (need) {
+      int r = build_factors(h, k);
+      if (r) return r;
+    }
+  }
+  return 0;
+}
+
+static SolveTabs solve_tabs(iw_handle* h, int kind) {
+  SolveTabs tb;
+  tb.ab = h->dab[kind];
+  tb.ipiv = h->dipiv[kind];
+  tb.sys = h->dsys[kind];
+  tb.col_sys = h->dcolsys[kind];
+  tb.wg = h->dwg;
+  tb.alpol = h->dal;
+  tb.sigma = h->dsig;
+  tb.meang = h->dmeang;
+  return tb;
+}
+
+// ---------------------------------------------------------------------------
+// the step
+// ---------------------------------------------------------------------------
+template <typename T, int NM>
+static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
+  long total = (long)h->nxpp * h->ny * h->ns;
+  dim3 grid((unsigned)((total + 127) / 128), 1, 4);
+  k_stageA<T, NM><<<grid, 128, 0, h->st>>>(geo(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.F1[0], fs.F1[1], fs.F1[2],
+                                           fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj);
+}
+template <typename T, int NM>
+static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
+  EArgs<T> a;
+  for (int q = 0; q < 4; ++q) {
+    a.B[q] = fs.B8[q];
+    a.Z[q] = fs.B8[4 + q];
+    a.F1[q] = fs.F1[q];
+    a.Fn[q] = fs.Fn[q];
+    a.Snold[q] = fs.Sn[q];
+    a.Snm_w[q] = fs.Snm[q];
+    a.Fnm_w[q] = fs.Fnm[q];
+    a.F[q] = fs.F[q];
+  }
+  a.wnl = h->dwnl;
+  a.filter = h->p.ispecfilternl == 1;
+  long total = (long)h->nxpp * h->ny * h->ns;
+  dim3 grid((unsigned)((total + 127) / 128), 1, 4);
+  k_stageE<T, NM><<<grid, 128, 0, h->st>>>(geo(h), a, h->c);
+}
+
+template <typename T>
+static int ytx(const iw_handle* h) {  // y-FFT tile width
+  size_t cs = 2 * sizeof(T);
+  int tx = 8;
+  while (tx > 1 && 4 * (size_t)tx * h->ny * cs > 200 * 1024) tx /= 2;
+  return tx;
+}
+
+template <typename T>
+static void launch_y(iw_handle* h, FieldSet<T>& fs, YJobs<T>& jobs, int njobs, int nplanes, bool four) {
+  typedef typename cplx_t<T>::type C;
+  int tx = ytx<T>(h);
+  int ntile = (h->nxhp + tx - 1) / tx;
+  dim3 grid(ntile, nplanes, njobs);
+  size_t smem = (four ? 4 : 2) * (size_t)tx * h->ny * sizeof(C);
+  Geo g = geo(h);
+  switch (tx) {
+    case 8:
+      cudaFuncSetAttribute(k_yfft<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_yfft<T, 8><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
+      break;
+    case 4:
+      cudaFuncSetAttribute(k_yfft<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_yfft<T, 4><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
+      break;
+    case 2:
+      cudaFuncSetAttribute(k_yfft<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_yfft<T, 2><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
+      break;
+    default:
+      cudaFuncSetAttribute(k_yfft<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_yfft<T, 1><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
+      break;
+  }
+}
+
+#define DISPATCH_N(h, FN, ...)                    \
+  do {                                            \
+    if ((h)->N <= 16)                             \
+      FN<T, 16>(__VA_ARGS__);                     \
+    else if ((h)->N <= 24)                        \
+      FN<T, 24>(__VA_ARGS__);                     \
+    else if ((h)->N <= 32)                        \
+      FN<T, 32>(__VA_ARGS__);                     \
+    else                                          \
+      FN<T, 48>(__VA_ARGS__);                     \
+  } while (0)
+
+// convec (solver.f:6-514).  proj=1 also applies the maxcalc round trip that
+// precedes it in the main loop (main.f:657).
+template <typename T>
+static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
+  typedef typename cplx_t<T>::type C;
+  Geo g = geo(h);
+  const int M = h->nx / 2;
+  mark(h, -1);
+  // K_A
+  DISPATCH_N(h, launch_stageA, h, fs, proj);
+  mark(h, 0);
+  // K_B: y-inverse of 12 arrays
+  {
+    YJobs<T> jb;
+    memset(&jb, 0, sizeof jb);
+    for (int q = 0; q < 4; ++q) {
+      jb.j[q] = YJob<T>{fs.F1[q], nullptr, fs.Y12[q], 0};
+      jb.j[4 + q] = YJob<T>{fs.F1[q], nullptr, fs.Y12[4 + q], 1};
+      jb.j[8 + q] = YJob<T>{fs.Z4[q], nullptr, fs.Y12[8 + q], 0};
+    }
+    launch_y<T>(h, fs, jb, 12, h->nz, false);
+  }
+  mark(h, 1);
+  // K_C
+  {
+    NLArgs<T> a;
+    memset(&a, 0, sizeof a);
+    for (int q = 0; q < 4; ++q) {
+      a.in[q] = fs.Y12[q];       // u v w t
+      a.in[4 + q] = fs.Y12[4 + q];  // dy
+      a.in[8 + q] = fs.Y12[8 + q];  // dz
+    }
+    for (int q = 0; q < 11; ++q) a.out[q] = fs.X11[q];
+    const double bz = h->p.brunt;
+    const double rg = -(h->p.rho0 * (bz * bz) / h->p.grav);
+    a.coef_buoy = (bz * bz) / rg;
+    a.rg = rg;
+    const double omega = 2. / (double)((h->N + 1) * (h->N + 2));
+    for (int ks = 0; ks < h->ns; ++ks) a.tau_pen[ks] = 0.5 / omega * (2. / h->p.zh[ks]);
+    a.forcing = h->p.forcing;
+    if (h->p.forcing) {
+      double pi2 = 8. * std::atan(1.0);
+      double xk = pi2 / h->p.xlen, xm = pi2 / (2. * h->p.zlen);
+      double om = (h->p.brunt * xk) / std::sqrt(xk * xk + xm * xm);
+      double zdim = h->p.xlen, um = h->p.umax, xa = h->p.xacrit;
+      double ph = (h->t <= h->p.fwave * (pi2 / om)) ? 1.0 : 0.0;
+      a.f_xk = xk;
+      a.f_xm = xm;
+      a.f_om = om;
+      a.f_t = h->t;
+      a.f_amp_u = -(1 / xk) * (xa * um) * xm * um / zdim * ph;
+      a.f_amp_w = (xa * um) * (um / zdim) * ph;
+      a.f_amp_r = (xa * um) * (-(1 / om)) * bz * bz * (h->p.rho0 / h->p.grav) * (um / zdim) * ph;
+    }
+    a.dx = (pi2_of(h) / (pi2_of(h) / h->p.xlen)) / h->nx;
+    size_t smem = 2 * 20 * (size_t)M * sizeof(C);
+    cudaFuncSetAttribute(k_xrow_nl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid(h->ny, h->nz);
+    k_xrow_nl<T><<<grid, 256, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);
+  }
+  mark(h, 2);
+  // K_D: y-forward; B_q = Y(A_q) + i ky Y(P_q), Z_q = Y(P_zq)
+  {
+    YJobs<T> jb;
+    memset(&jb, 0, sizeof jb);
+    // X11: Au Av Aw At | uv vv vw vt | uw ww wt ;  B8: Bu Bv Bw Bt | Zu Zv Zw Zt
+    for (int q = 0; q < 4; ++q) jb.j[q] = YJob<T>{fs.X11[q], fs.X11[4 + q], fs.B8[q], 3};
+    launch_y<T>(h, fs, jb, 4, h->nz, true);
+    YJobs<T> jz;
+    memset(&jz, 0, sizeof jz);
+    jz.j[0] = YJob<T>{fs.X11[8], nullptr, fs.B8[4], 2};   // uw
+    jz.j[1] = YJob<T>{fs.X11[6], nullptr, fs.B8[5], 2};   // vw
+    jz.j[2] = YJob<T>{fs.X11[9], nullptr, fs.B8[6], 2};   // ww
+    jz.j[3] = YJob<T>{fs.X11[10], nullptr, fs.B8[7], 2};  // wt
+    launch_y<T>(h, fs, jz, 4, h->nz, false);
+  }
+  mark(h, 3);
+  // wall pressure BC term (before the histories rotate)
+  {
+    long total = (long)h->nxhp * h->ny * 2;
+    k_wviscrot<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F1[0], fs.F1[1], fs.F1[2], fs.Fn[0],
+                                                                      fs.Fn[1], fs.Fn[2], fs.Fnm[0], fs.Fnm[1],
+                                                                      fs.Fnm[2], h->c, h->p.xnu, h->dwvr);
+  }
+  mark(h, 4);
+  // K_E
+  DISPATCH_N(h, launch_stageE, h, fs);
+  mark(h, 5);
+  for (int q = 0; q < 4; ++q) {
+    std::swap(fs.Sn[q], fs.Snm[q]);  // Snm buffer now holds S (level n) -> becomes Sn
+    std::swap(fs.Fn[q], fs.Fnm[q]);
+  }
+  return 0;
+}
+
+static void schedule_after_convec(iw_handle* h) {
+  // coefficient schedule for the next step (main.f:700-777)
+  if (h->istep < 2) {
+    h->c.fac1 = 2.;
+    h->c.fac2 = -1.;
+    h->c.fac3 = 0.;
+    h->c.bdf1 = 2.;
+    h->c.bdf2 = -0.5;
+    h->c.bdf3 = 0.;
+  } else {
+    h->c.fac1 = 3.;
+    h->c.fac2 = -3.;
+    h->c.fac3 = 1.;
+    h->c.bdf1 = 3.;
+    h->c.bdf2 = -1.5;
+    h->c.bdf3 = 1. / 3.;
+  }
+}
+
+// calcuvwt (calcuvwt_noslip.f / calcuvwt.f) on u*,v*,w*,rho* held in F.
+template <typename T>
+static int calcuvwt_impl(iw_handle* h, FieldSet<T>& fs, int cpen) {
+  Geo g = geo(h);
+  const int warps = 4;
+  const unsigned nblk = (unsigned)((h->ncol + warps - 1) / warps);
+  const size_t smem = (size_t)warps * 4 * h->nz * sizeof(double);
+  const int kstart = h->p.bc_variant == IW_BC_NOSLIP ? 1 : 0;
+  cudaFuncSetAttribute(k_press<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_visc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_press<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_P), fs.F[0], fs.F[1], fs.F[2], h->dwnl, h->dwvr,
+                                                 cpen, kstart);
+  mark(h, 6);
+  const double xnudt = h->p.xnu * h->p.dt, dtk = h->p.dt * h->p.xkappa;
+  k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_U), fs.F[0], fs.F[1], xnudt, 0, cpen,
+                                                h->p.meanu_damping);
+  mark(h, 7);
+  k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_W), fs.F[2], fs.F[2], xnudt, 1, cpen, 0);
+  mark(h, 8);
+  k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_T), fs.F[3], fs.F[3], dtk, 2, cpen, 0);
+  mark(h, 9);
+  return 0;
+}
+
+template <typename T>
+static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
+  typedef typename cplx_t<T>::type C;
+  Geo g = geo(h);
+  if (h->ns < 2) {
+    long total = (long)h->ny * h->nz * 4;
+    k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
+    return 0;
+  }
+  const int ng = nf * (h->ns - 1);  // plane groups (field, interface)
+  const long tot = (long)h->plane * ng * 4;  // 4 planes per group
+  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 0);
+  {
+    YJobs<T> jb;
+    memset(&jb, 0, sizeof jb);
+    jb.j[0] = YJob<T>{fs.G, nullptr, fs.G, 0};
+    launch_y<T>(h, fs, jb, 1, ng * 4, false);
+  }
+  if (count) CK(cudaMemsetAsync(h->dcnt, 0, 4 * sizeof(int), h->st));
+  {
+    const int M = h->nx / 2;
+    size_t smem = 2 * 4 * (size_t)M * sizeof(C);
+    cudaFuncSetAttribute(k_iface_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid(h->ny, ng);
+    k_iface_rows<T><<<grid, 128, smem, h->st>>>(g, fs.G, h->plx, fs.Wm, fs.Wn, h->dcnt);
+  }
+  {
+    YJobs<T> jb;
+    memset(&jb, 0, sizeof jb);
+    jb.j[0] = YJob<T>{fs.G, nullptr, fs.G, 2};
+    launch_y<T>(h, fs, jb, 1, ng * 4, false);
+  }
+  long total = (long)h->ny * h->nz * nf;
+  k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 1);
+  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1);
+  return 0;
+}
+
+template <typename T>
+static int full_step(iw_handle* h, FieldSet<T>& fs) {
+  h->istep += 1;
+  int r = ensure_factors(h);
+  if (r) return r;
+  convec_impl<T>(h, fs, 1);
+  schedule_after_convec(h);
+  const int cpen = (h->p.ispecfilterexp == 1) && (h->istep % h->p.nspecfilterexp == 0);
+  calcuvwt_impl<T>(h, fs, cpen);
+  h->c.bdfv = (h->istep < 2) ? 1.5 : 11. / 6.;
+  h->t = h->t + h->p.dt;
+  if (h->p.navgintrfc > 0 && h->istep % h->p.navgintrfc == 0) {
+    iface_avg<T>(h, fs, true);
+    mark(h, 10);
+  }
+  prof_flush(h);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* iw_last_error(void) { return g_err.c_str(); }
+
+int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** out) {
+  if (!dims || !prm || !out) return set_err(IW_ERR_CONFIG, "null argument");
+  *out = nullptr;
+  const iw_dims& d = *dims;
+  if (d.nx < 4 || d.nx % 2 || make_plan(d.nx / 2).npass < 0) return set_err(IW_ERR_CONFIG, "nx: need even, radices 2,3,5");
+  if (d.ny < 1 || (d.ny > 1 && (d.ny % 2 || make_plan(d.ny).npass < 0)))
+    return set_err(IW_ERR_CONFIG, "ny: need 1 or even with radices 2,3,5");
+  if (d.nzloc < 3 || d.nzloc > 48) return set_err(IW_ERR_CONFIG, "nzloc outside [3,48]");
+  if (d.nsubd < 1 || d.nsubd > IW_MAX_SUBD) return set_err(IW_ERR_CONFIG, "nsubd outside [1,64]");
+  if ((size_t)d.nx / 2 * 20 * 2 * 16 > 220 * 1024 && prm->precision == IW_PREC_FP64)
+    return set_err(IW_ERR_CONFIG, "nx too large for the FP64 row kernel");
+  double zsum = 0;
+  for (int k = 0; k < d.nsubd; ++k) {
+    if (!(prm->zh[k] > 0)) return set_err(IW_ERR_CONFIG, "subdomain height must be positive");
+    zsum += prm->zh[k];
+  }
+  if (std::fabs(zsum - prm->zlen) > 1e-9 * std::max(1.0, prm->zlen))
+    return set_err(IW_ERR_CONFIG, "subdomain heights do not add up to zlen");
+  if (!(prm->dt > 0) || !(prm->xnu > 0) || !(prm->xkappa > 0)) return set_err(IW_ERR_CONFIG, "dt, xnu, xkappa > 0");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(IW_ERR_CUDA, "no CUDA device");
+  iw_handle* h = new iw_handle();
+  h->d = d;
+  h->p = *prm;
+  if (device >= 0) {
+    h->dev = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+      delete h;
+      return set_err(IW_ERR_CUDA, "cudaSetDevice failed");
+    }
+  } else {
+    cudaGetDevice(&h->dev);
+  }
+  h->nx = d.nx;
+  h->ny = d.ny;
+  h->N = d.nzloc;
+  h->ns = d.nsubd;
+  h->nz = d.nzloc * d.nsubd;
+  h->nxpp = d.nx + 2;
+  h->nxh = d.nx / 2;
+  h->nxhp = h->nxh + 1;
+  h->nyh = d.ny / 2;
+  h->ndims = d.ny > 1 ? 3 : 2;
+  h->plane = (size_t)h->nxpp * h->ny;
+  h->ntot = h->plane * h->nz;
+  h->ncol = h->nxhp * h->ny;
+  h->mixed = prm->precision == IW_PREC_MIXED;
+  h->plx = make_plan(h->nx / 2);
+  h->ply = make_plan(h->ny);
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return set_err(IW_ERR_CUDA, "stream");
+  }
+  h->tab = h_tables(h->N, prm->p, prm->amp, prm->fackc);
+  // wavenumbers and grids (setup.f:77-166)
+  const double pi2 = 8.0 * std::atan(1.0);
+  const double alpha = pi2 / prm->xlen, beta = pi2 / prm->ylen;
+  std::vector<double> xw(h->nxhp), yw(h->ny, 0.0), zg(h->nz), hf(h->ns), zh(h->ns), mg(h->nz);
+  for (int i = 0; i < h->nxhp; ++i) xw[i] = i * alpha;
+  for (int j = 1; j <= h->nyh; ++j) {
+    yw[j - 1] = (j - 1) * beta;
+    yw[h->ny - j] = -j * beta;
+  }
+  for (int ks = 0; ks < h->ns; ++ks) {
+    hf[ks] = 2. / prm->zh[ks];
+    zh[ks] = prm->zh[ks];
+    for (int kl = 0; kl < h->N; ++kl) zg[ks * h->N + kl] = prm->z0[ks] + 0.5 * prm->zh[ks] * (h->tab.zpts[kl] + 1.0);
+  }
+  for (int k = 0; k < h->nz; ++k) {
+    double r = (zg[k] - prm->zcen) / prm->xlen;
+    mg[k] = 1.0 - std::exp(-prm->xbcrit * (r * r));
+  }
+  // Fourier filter factor per column (filtering.f:849-900 with kc = 0)
+  std::vector<double> cf(h->ncol);
+  {
+    double akmax = std::sqrt(xw[h->nxhp - 1] * xw[h->nxhp - 1] + yw[h->nyh] * yw[h->nyh]);
+    for (int j = 0; j < h->ny; ++j)
+      for (int ii = 0; ii < h->nxhp; ++ii) {
+        double ak = std::sqrt(xw[ii] * xw[ii] + yw[j] * yw[j]);
+        double theta = ak / akmax;
+        cf[(size_t)j * h->nxhp + ii] = std::exp(-prm->amp * std::pow(theta, 2. * prm->pf));
+      }
+  }
+  int r = 0;
+  r |= up(h, &h->dD, h->tab.D) || up(h, &h->dD2, h->tab.D2) || up(h, &h->dL, h->tab.Lfil) || up(h, &h->dh, hf) ||
+       up(h, &h->dxw, xw) || up(h, &h->dyw, yw) || up(h, &h->dcf, cf) || up(h, &h->dzg, zg) || up(h, &h->dzh, zh) ||
+       up(h, &h->dwg, h->tab.wg) || up(h, &h->dal, h->tab.alpol) || up(h, &h->dsig, h->tab.sigma) ||
+       up(h, &h->dmeang, mg);
+  r |= dalloc(h, &h->dwnl, h->plane * 2) || dalloc(h, &h->dwvr, h->plane * 2) || dalloc(h, &h->dred, std::max<size_t>(64, 4 * (size_t)h->nz)) ||
+       dalloc(h, &h->dcnt, 8) || dalloc(h, &h->dflag, 4);
+  if (!r) {
+    cudaMemset(h->dcnt, 0, 8 * sizeof(int));
+    cudaMemset(h->dwnl, 0, h->plane * 2 * sizeof(double));
+    cudaMemset(h->dwvr, 0, h->plane * 2 * sizeof(double));
+    r = h->mixed ? alloc_fields(h, h->f32) : alloc_fields(h, h->f64);
+  }
+  if (r) {
+    iw_destroy(h);
+    return IW_ERR_NOMEM;
+  }
+  build_distinct(h);
+  h->c = Coefs{1., 0., 0., 1., 0., 0., 1., prm->dt};
+  *out = h;
+  return IW_OK;
+}
+
+int iw_destroy(iw_handle* h) {
+  if (!h) return IW_OK;
+  cudaSetDevice(h->dev);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  free_fields(h->f64);
+  free_fields(h->f32);
+  for (double* p : {h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
+                    h->dmeang, h->dwnl, h->dwvr, h->dred})
+    cudaFree(p);
+  cudaFree(h->dcnt);
+  cudaFree(h->dflag);
+  for (int k = 0; k < SYS_KINDS; ++k) {
+    cudaFree(h->dab[k]);
+    cudaFree(h->dipiv[k]);
+    cudaFree(h->dinfo[k]);
+    cudaFree(h->dsys[k]);
+    cudaFree(h->dpen[k]);
+    cudaFree(h->dcolsys[k]);
+  }
+  if (h->st) cudaStreamDestroy(h->st);
+  if (g_bound == h) g_bound = nullptr;
+  delete h;
+  return IW_OK;
+}
+
+static int copy_level(iw_handle* h, int level, double* host, bool up_dir) {
+  // level 0 F, 1 Fn, 2 Fnm, 3 Sn, 4 Snm
+  const size_t n = h->ntot;
+  for (int q = 0; q < 4; ++q) {
+    void* dp;
+    if (h->mixed) {
+      float* const* L = level == 0 ? h->f32.F : level == 1 ? h->f32.Fn : level == 2 ? h->f32.Fnm : level == 3 ? h->f32.Sn : h->f32.Snm;
+      dp = L[q];
+      // convert through a scratch double buffer (F1 of the FP64 set is absent: use a temp)
+      double* tmp = nullptr;
+      CK(cudaMalloc(&tmp, n * sizeof(double)));
+      if (up_dir) {
+        CK(cudaMemcpy(tmp, host + q * n, n * sizeof(double), cudaMemcpyHostToDevice));
+        k_convert<double, float><<<1024, 256, 0, h->st>>>(tmp, (float*)dp, n);
+      } else {
+        k_convert<float, double><<<1024, 256, 0, h->st>>>((const float*)dp, tmp, n);
+        CK(cudaStreamSynchronize(h->st));
+        CK(cudaMemcpy(host + q * n, tmp, n * sizeof(double), cudaMemcpyDeviceToHost));
+      }
+      CK(cudaStreamSynchronize(h->st));
+      cudaFree(tmp);
+    } else {
+      double* const* L = level == 0 ? h->f64.F : level == 1 ? h->f64.Fn : level == 2 ? h->f64.Fnm : level == 3 ? h->f64.Sn : h->f64.Snm;
+      dp = L[q];
+      if (up_dir)
+        CK(cudaMemcpyAsync(dp, host + q * n, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
+      else
+        CK(cudaMemcpyAsync(host + q * n, dp, n * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    }
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int iw_upload_state(iw_handle* h, const double* uvwt, const double* uvwt_n, const double* uvwt_nm, const double* s_n,
+                    const double* s_nm, double t, int istep_done) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  cudaSetDevice(h->dev);
+  const double* src[5] = {uvwt, uvwt_n, uvwt_nm, s_n, s_nm};
+  for (int l = 0; l < 5; ++l)
+    if (src[l]) {
+      int r = copy_level(h, l, const_cast<double*>(src[l]), true);
+      if (r) return r;
+    }
+  h->t = t;
+  h->istep = istep_done;
+  if (istep_done == 0) {
+    h->c = Coefs{1., 0., 0., 1., 0., 0., 1., h->p.dt};
+  } else if (istep_done == 1) {
+    h->c = Coefs{2., -1., 0., 2., -0.5, 0., 1.5, h->p.dt};
+  } else {
+    h->c = Coefs{3., -3., 1., 3., -1.5, 1. / 3., 11. / 6., h->p.dt};
+  }
+  return IW_OK;
+}
+
+int iw_download_state(iw_handle* h, double* uvwt, double* uvwt_n, double* uvwt_nm, double* s_n, double* s_nm) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  cudaSetDevice(h->dev);
+  double* dst[5] = {uvwt, uvwt_n, uvwt_nm, s_n, s_nm};
+  for (int l = 0; l < 5; ++l)
+    if (dst[l]) {
+      int r = copy_level(h, l, dst[l], false);
+      if (r) return r;
+    }
+  return IW_OK;
+}
+
+int iw_step(iw_handle* h) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  cudaSetDevice(h->dev);
+  return h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64);
+}
+
+int iw_run(iw_handle* h, int nsteps, int use_graph) {
+  (void)use_graph;
+  for (int s = 0; s < nsteps; ++s) {
+    int r = iw_step(h);
+    if (r) return r;
+  }
+  return IW_OK;
+}
+
+int iw_step_coefs(iw_handle* h, const iw_coefs* c) {
+  if (!h || !c) return set_err(IW_ERR_STATE, "null argument");
+  h->c = Coefs{c->fac1, c->fac2, c->fac3, c->bdf1, c->bdf2, c->bdf3, c->bdfv, c->dt};
+  if (c->dt > 0 && c->dt != h->p.dt) h->p.dt = c->dt;
+  return iw_step(h);
+}
+
+int iw_sync(iw_handle* h) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  CK(cudaStreamSynchronize(h->st));
+  return IW_OK;
+}
+
+int iw_field_ptr(iw_handle* h, int f, void** dptr) {
+  if (!h || f < 0 || f > 3 || !dptr) return set_err(IW_ERR_STATE, "bad argument");
+  *dptr = h->mixed ? (void*)h->f32.F[f] : (void*)h->f64.F[f];
+  return IW_OK;
+}
+
+int iw_stream(iw_handle* h, void** stream) {
+  if (!h || !stream) return set_err(IW_ERR_STATE, "bad argument");
+  *stream = (void*)h->st;
+  return IW_OK;
+}
+
+int iw_device_bytes(iw_handle* h, size_t* bytes) {
+  if (!h || !bytes) return set_err(IW_ERR_STATE, "bad argument");
+  *bytes = h->bytes;
+  return IW_OK;
+}
+
+int iw_bind(iw_handle* h) {
+  g_bound = h;
+  return IW_OK;
+}
+
+// Per-phase device time (CUDA events on the handle's stream).  enable=1
+// starts recording (and zeroes the totals), 0 stops.  Phases: 0 stageA,
+// 1 y-inverse, 2 x-row NL, 3 y-forward, 4 wviscrot, 5 stageE, 6 pressure,
+// 7 u/v solve, 8 w solve, 9 rho solve, 10 interface averaging.
+int iw_profile(iw_handle* h, int enable) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  if (enable && !h->prof) {
+    for (int i = 0; i < 32; ++i) cudaEventCreate(&h->ev[i]);
+  }
+  if (!enable && h->prof) {
+    for (int i = 0; i < 32; ++i) cudaEventDestroy(h->ev[i]);
+  }
+  h->prof = enable;
+  h->nev = 0;
+  for (int i = 0; i < 16; ++i) {
+    h->phase_ms[i] = 0;
+    h->phase_n[i] = 0;
+  }
+  return IW_OK;
+}
+
+int iw_profile_read(iw_handle* h, double* ms16, long* n16) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  for (int i = 0; i < 16; ++i) {
+    if (ms16) ms16[i] = h->phase_ms[i];
+    if (n16) n16[i] = h->phase_n[i];
+  }
+  return IW_OK;
+}
+
+}  // extern "C"
+
+
+// ---------------------------------------------------------------------------
+// isolated batched Helmholtz solves (one system per column, lambda given)
+// ---------------------------------------------------------------------------
+struct HelmCache {
+  int nsys = 0;
+  double* ab = nullptr;
+  float* ab32 = nullptr;
+  int* ipiv = nullptr;
+  int* info = nullptr;
+  SysDesc* sys = nullptr;
+  double* pen = nullptr;
+  int* colsys = nullptr;
+};
+static std::map<std::pair<iw_handle*, std::string>, HelmCache> g_helm;
+
+// y = A x for the penalty matrix of system s (matrix-free, FP64)
+__device__ double apply_A_row(const Geo& g, const double* __restrict__ D2, const double* __restrict__ zh, double eps,
+                              const double* __restrict__ pen, const double* x, int r) {
+  const int N = g.N, ns = g.ns;
+  const int ks = r / N, k1 = r % N, km = ks * N;
+  const double *pa = pen, *pb = pen + ns, *pg = pen + 2 * ns, *pd = pen + 3 * ns, *pt1 = pen + 4 * ns,
+               *pt2 = pen + 5 * ns;
+  const double h2 = (2.0 / zh[ks]);
+  double s2 = 0;
+  for (int k = 0; k < N; ++k) s2 += D2[k1 * N + k] * x[km + k];
+  double y = x[r] - eps * h2 * h2 * s2;
+  if (k1 == 0) {
+    double s0 = 0;
+    for (int k = 0; k < N; ++k) s0 += g.D[0 * N + k] * x[km + k];
+    y += pt1[ks] * pa[ks] * x[km] - pt1[ks] * pb[ks] * eps * h2 * s0;
+    if (ks > 0) {
+      double hl = 2.0 / zh[ks - 1];
+      double sl = 0;
+      for (int k = 0; k < N; ++k) sl += g.D[(N - 1) * N + k] * x[km - N + k];
+      y += -0.5 * pt1[ks] * pa[ks] * x[km] + 0.5 * pt1[ks] * pb[ks] * eps * h2 * s0 - 0.5 * pt1[ks] * pa[ks] * x[km - 1] +
+           0.5 * pt1[ks] * pb[ks] * eps * hl * sl;
+    }
+  }
+  if (k1 == N - 1) {
+    double s1 = 0;
+    for (int k = 0; k < N; ++k) s1 += g.D[(N - 1) * N + k] * x[km + k];
+    y += pt2[ks] * pg[ks] * x[km + N - 1] + pt2[ks] * pd[ks] * eps * h2 * s1;
+    if (ks < ns - 1) {
+      double hr = 2.0 / zh[ks + 1];
+      double sr = 0;
+      for (int k = 0; k < N; ++k) sr += g.D[0 * N + k] * x[km + N + k];
+      y += -0.5 * pt2[ks] * pg[ks] * x[km + N - 1] - 0.5 * pt2[ks] * pd[ks] * eps * h2 * s1 -
+           0.5 * pt2[ks] * pg[ks] * x[km + N] - 0.5 * pt2[ks] * pd[ks] * eps * hr * sr;
+    }
+  }
+  return y;
+}
+
+__device__ void band_solve_warp_f(const float* __restrict__ ab, const int* __restrict__ ipiv, float* b, int nr, int n,
+                                  int kl, int ku, int lane) {
+  const int ldab = 2 * kl + ku + 1, kd = ku + kl + 1;
+  for (int j = 1; j <= n - 1; ++j) {
+    const int lm = min(kl, n - j);
+    const int l = __ldg(ipiv + j - 1);
+    const float* col = ab + (size_t)ldab * (j - 1);
+    for (int r = 0; r < nr; ++r) {
+      float* br = b + (size_t)r * n;
+      const float bj = br[j - 1], bl = br[l - 1];
+      const float y = (l != j) ? bl : bj;
+      float nv0 = 0, nv1 = 0;
+      const int i0 = lane + 1, i1 = lane + 33;
+      if (i0 <= lm) {
+        int row = j + i0;
+        float old = (row == l) ? bj : br[row - 1];
+        nv0 = old - __ldg(col + kd + i0 - 1) * y;
+      }
+      if (i1 <= lm) {
+        int row = j + i1;
+        float old = (row == l) ? bj : br[row - 1];
+        nv1 = old - __ldg(col + kd + i1 - 1) * y;
+      }
+      __syncwarp();
+      if (i0 <= lm) br[j + i0 - 1] = nv0;
+      if (i1 <= lm) br[j + i1 - 1] = nv1;
+      if (lane == 0) br[j - 1] = y;
+      __syncwarp();
+    }
+  }
+  const int k = kl + ku, kplus1 = k + 1;
+  for (int j = n; j >= 1; --j) {
+    const float* col = ab + (size_t)ldab * (j - 1);
+    const float dg = __ldg(col + kplus1 - 1);
+    const int lo = max(1, j - k), l = kplus1 - j;
+    for (int r = 0; r < nr; ++r) {
+      float* br = b + (size_t)r * n;
+      float xj = br[j - 1] / dg;
+      float nv[3];
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        int i = j - 1 - lane - 32 * m;
+        nv[m] = (i >= lo) ? br[i - 1] - xj * __ldg(col + l + i - 1) : 0.f;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        int i = j - 1 - lane - 32 * m;
+        if (i >= lo) br[i - 1] = nv[m];
+      }
+      if (lane == 0) br[j - 1] = xj;
+      __syncwarp();
+    }
+  }
+}
+
+// mode 0: FP64 factors and solve; mode 1: FP32 solve + one FP64 residual
+// refinement sweep.  rhs/sol: [ncol][nz] complex (re,im).
+__global__ void k_helm(Geo g, HelmCache hc, const double* __restrict__ rhs, double* __restrict__ sol, int ncol,
+                       int mode, const double* __restrict__ D2, const double* __restrict__ zh) {
+  extern __shared__ __align__(16) double smh[];
+  const int warps = blockDim.x / 32, wid = threadIdx.x / 32, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * warps + wid;
+  if (c >= ncol) return;
+  const int n = g.nz, N = g.N, ldab = 3 * N + 1;
+  const int s = hc.colsys[c];
+  double* b = smh + (size_t)wid * 6 * n;  // b (2n), x (2n), r (2n)
+  for (int k = lane; k < n; k += 32) {
+    b[k] = rhs[((size_t)c * n + k) * 2];
+    b[n + k] = rhs[((size_t)c * n + k) * 2 + 1];
+  }
+  __syncwarp();
+  if (mode == 0) {
+    band_solve_warp(hc.ab + (size_t)s * ldab * n, hc.ipiv + (size_t)s * n, b, 2, n, N, N, lane);
+    for (int k = lane; k < n; k += 32) {
+      sol[((size_t)c * n + k) * 2] = b[k];
+      sol[((size_t)c * n + k) * 2 + 1] = b[n + k];
+    }
+    return;
+  }
+  double* x = b + 2 * n;
+  float* xf = (float*)(b + 4 * n);  // 2n floats
+  for (int k = lane; k < 2 * n; k += 32) xf[k] = (float)b[k];
+  __syncwarp();
+  const float* ab32 = hc.ab32 + (size_t)s * ldab * n;
+  const int* ip = hc.ipiv + (size_t)s * n;
+  band_solve_warp_f(ab32, ip, xf, 2, n, N, N, lane);
+  for (int k = lane; k < 2 * n; k += 32) x[k] = (double)xf[k];
+  __syncwarp();
+  const double eps = hc.sys[s].eps;
+  const double* pen = hc.pen + (size_t)s * 6 * g.ns;
+  for (int k = lane; k < n; k += 32) {
+    double r0 = b[k] - apply_A_row(g, D2, zh, eps, pen, x, k);
+    double r1 = b[n + k] - apply_A_row(g, D2, zh, eps, pen, x + n, k);
+    xf[k] = (float)r0;
+    xf[n + k] = (float)r1;
+  }
+  __syncwarp();
+  band_solve_warp_f(ab32, ip, xf, 2, n, N, N, lane);
+  for (int k = lane; k < n; k += 32) {
+    sol[((size_t)c * n + k) * 2] = x[k] + (double)xf[k];
+    sol[((size_t)c * n + k) * 2 + 1] = x[n + k] + (double)xf[n + k];
+  }
+}
+
+static int helm_batched(iw_handle* h, const double* lam_dev, int ncol, int bot, int top, const double* rhs,
+                        double* sol, int mode) {
+  std::vector<double> lam(ncol);
+  CK(cudaMemcpy(lam.data(), lam_dev, ncol * sizeof(double), cudaMemcpyDeviceToHost));
+  // key: the lambda set and BCs
+  uint64_t hs = 1469598103934665603ULL;
+  for (double v : lam) {
+    uint64_t b;
+    memcpy(&b, &v, 8);
+    hs = (hs ^ b) * 1099511628211ULL;
+  }
+  char kb[96];
+  snprintf(kb, sizeof kb, "%d|%d|%d|%llx", ncol, bot, top, (unsigned long long)hs);
+  auto key = std::make_pair(h, std::string(kb));
+  const int n = h->nz, N = h->N, ldab = 3 * N + 1, ns = h->ns;
+  auto it = g_helm.find(key);
+  if (it == g_helm.end()) {
+    std::vector<double> s = lam;
+    std::sort(s.begin(), s.end());
+    s.erase(std::unique(s.begin(), s.end()), s.end());
+    HelmCache hc;
+    hc.nsys = (int)s.size();
+    std::vector<SysDesc> sys(hc.nsys);
+    std::vector<double> pen((size_t)hc.nsys * 6 * ns);
+    for (int u = 0; u < hc.nsys; ++u) {
+      memset(&sys[u], 0, sizeof(SysDesc));
+      sys[u].eps = 1. / s[u];
+      sys[u].ifbcbot = bot;
+      sys[u].ifbctop = top;
+      h_penalty(ns, N, h->p, sys[u].eps, bot, top, pen.data() + (size_t)u * 6 * ns);
+      sys[u].tau1_bot = pen[(size_t)u * 6 * ns + 4 * ns];
+      sys[u].tau2_top = pen[(size_t)u * 6 * ns + 5 * ns + ns - 1];
+    }
+    std::vector<int> cs(ncol);
+    for (int c = 0; c < ncol; ++c) cs[c] = (int)(std::lower_bound(s.begin(), s.end(), lam[c]) - s.begin());
+    if (dalloc(h, &hc.ab, (size_t)hc.nsys * ldab * n) || dalloc(h, &hc.ab32, (size_t)hc.nsys * ldab * n) ||
+        dalloc(h, &hc.ipiv, (size_t)hc.nsys * n) || dalloc(h, &hc.info, (size_t)hc.nsys) ||
+        up(h, &hc.sys, sys) || up(h, &hc.pen, pen) || up(h, &hc.colsys, cs))
+      return IW_ERR_NOMEM;
+    FactorArgs fa;
+    fa.sys = hc.sys;
+    fa.pen = hc.pen;
+    fa.ab = hc.ab;
+    fa.ipiv = hc.ipiv;
+    fa.info = hc.info;
+    fa.nsys = hc.nsys;
+    fa.D = h->dD;
+    fa.D2 = h->dD2;
+    fa.zh = h->dzh;
+    fa.assemble = 1;
+    k_factor<<<(hc.nsys + 3) / 4, 128, 0, h->st>>>(geo(h), fa);
+    size_t tot = (size_t)hc.nsys * ldab * n;
+    k_convert<double, float><<<2048, 256, 0, h->st>>>(hc.ab, hc.ab32, tot);
+    CK(cudaStreamSynchronize(h->st));
+    it = g_helm.emplace(key, hc).first;
+  }
+  const HelmCache& hc = it->second;
+  const int warps = 4;
+  size_t smem = (size_t)warps * 6 * n * sizeof(double);
+  cudaFuncSetAttribute(k_helm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_helm<<<(ncol + warps - 1) / warps, 32 * warps, smem, h->st>>>(geo(h), hc, rhs, sol, ncol, mode, h->dD2, h->dzh);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+#include "iw_abi.inl"

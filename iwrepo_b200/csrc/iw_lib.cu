@@ -1,0 +1,1242 @@
+// B200 time step of the stratified Boussinesq solver (Fourier x,y /
+// Legendre multidomain penalty z) and its C ABI (include/iw_b200.h).
+//
+// One step (main.f:653-1066) on device-resident fields:
+//   K_A  k_stageA      maxcalc/convec round-trip projection, w mean = 0,
+//                      z-derivatives of u,v,w,rho                   (z columns)
+//   K_B  k_yfft        y-inverse of u,v,w,rho, dz, and i ky (.)      (planes)
+//   K_C  k_xrow_nl     x-inverse of 16 rows -> skew-symmetric products,
+//                      buoyancy, upwind interface penalty, paddle ->
+//                      x-forward with i kx folded in                 (rows)
+//   K_D  k_yfft        y-forward with i ky folded in                 (planes)
+//   K_E  k_stageE      S = B + dz(Z), SS extrapolation, BDF u*, history,
+//                      Fourier x Legendre filter                     (z columns)
+//        k_wviscrot    rotational viscous pressure BC              (walls)
+//   K_F  k_press       pressure Poisson (band LU), filter, projection
+//   K_G  k_visc        u,v / w / rho Helmholtz solves, filters, mean mode
+//   K_H  interface averaging: planes next to interfaces go to physical space
+//        and back; every other plane gets the spectral effect of the round trip.
+// The band factors (penalty.f + band_lu.f) are assembled and factored on the
+// device (k_factor) when epsilon changes (steps 1-3 and a dt change), one per
+// distinct kx^2+ky^2 and system type.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/iw_b200.h"
+#include "iw_fft.cuh"
+#include "iw_kernels.cuh"
+
+using namespace iw;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static int set_err(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+#define CK(x)                                                                            \
+  do {                                                                                   \
+    cudaError_t e_ = (x);                                                                \
+    if (e_ != cudaSuccess) return set_err(IW_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// small device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* p) {
+  return __ldg(p);
+}
+
+// ===========================================================================
+// K_A: round-trip projection + w(1,1,:)=0 + z derivatives.
+// Thread per (real x index i, y index j, subdomain ks, field q).
+// Inputs F (spectral state n); outputs F1 = P(F) (w mean zeroed) and dz(F1).
+// P is the exact effect of horfft(+1) followed by horfft(-1) (maxcalc,
+// various.f:726-729,848-851): the kx=0 column becomes Hermitian in ky, the
+// x-Nyquist column keeps its real part divided by ny, all else is unchanged.
+// ===========================================================================
+template <typename T>
+__device__ __forceinline__ T proj_val(const Geo& g, const T* __restrict__ f, int i, int j, int k) {
+  if (i < 2) {
+    int jp = (g.ny - j) % g.ny;
+    T a = f[fidx<T>(g, i, j, k)];
+    T b = f[fidx<T>(g, i, jp, k)];
+    return i == 0 ? (T)0.5 * (a + b) : (T)0.5 * (a - b);
+  }
+  if (i >= g.nx) {
+    return i == g.nx ? f[fidx<T>(g, i, j, k)] * (T)g.scaley : (T)0;
+  }
+  return f[fidx<T>(g, i, j, k)];
+}
+
+template <typename T, int NM>
+__global__ void k_stageA(Geo g, const T* __restrict__ F0, const T* __restrict__ F1_, const T* __restrict__ F2_,
+                         const T* __restrict__ F3_, T* __restrict__ O0, T* __restrict__ O1, T* __restrict__ O2,
+                         T* __restrict__ O3, T* __restrict__ Z0, T* __restrict__ Z1, T* __restrict__ Z2,
+                         T* __restrict__ Z3, int proj) {
+  __shared__ double sD[NM * NM];
+  for (int t = threadIdx.x; t < g.N * g.N; t += blockDim.x) sD[t] = g.D[t];
+  __syncthreads();
+  const int q = blockIdx.z;
+  const T* F = q == 0 ? F0 : q == 1 ? F1_ : q == 2 ? F2_ : F3_;
+  T* O = q == 0 ? O0 : q == 1 ? O1 : q == 2 ? O2 : O3;
+  T* Z = q == 0 ? Z0 : q == 1 ? Z1 : q == 2 ? Z2 : Z3;
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long total = (long)g.nxpp * g.ny * g.ns;
+  if (gid >= total) return;
+  int i = gid % g.nxpp;
+  long r = gid / g.nxpp;
+  int j = r % g.ny;
+  int ks = r / g.ny;
+  const int N = g.N;
+  T v[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k)
+    if (k < N) {
+      int kk = ks * N + k;
+      T x = proj ? proj_val<T>(g, F, i, j, kk) : F[fidx<T>(g, i, j, kk)];
+      if (q == 2 && j == 0 && i < 2) x = (T)0;  // wc(1,1,:) = 0, solver.f:66-69
+      v[k] = x;
+      O[fidx<T>(g, i, j, kk)] = x;
+    }
+  const T fac = (T)g.hfac[ks];
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1)
+    if (k1 < N) {
+      T s = 0;
+#pragma unroll
+      for (int k2 = 0; k2 < NM; ++k2)
+        if (k2 < N) s += (T)sD[k1 * N + k2] * v[k2];
+      Z[fidx<T>(g, i, j, ks * N + k1)] = s * fac;
+    }
+}
+
+// ===========================================================================
+// y transforms (CFFT99 semantics, horfft.f:21-30,51-57): LOT = nx/2 columns,
+// the x-Nyquist column is never transformed; forward is scaled by 1/ny (the
+// Nyquist column too).  One CTA per (plane, tile of TX kx columns, job).
+// Job modes:
+//   0 inverse:  dst = Yinv(src)
+//   1 inverse:  dst = Yinv(i ky src)
+//   2 forward:  dst = Yfwd(src)/ny
+//   3 forward:  dst = Yfwd(src)/ny + i ky Yfwd(src2)/ny
+// ===========================================================================
+template <typename T>
+struct YJob {
+  const T* src;
+  const T* src2;
+  T* dst;
+  int mode;
+};
+template <typename T>
+struct YJobs {
+  YJob<T> j[16];
+};
+
+template <typename T, int TX>
+__global__ void k_yfft(Geo g, YJobs<T> jobs, int nplanes, FftPlan pl, const typename cplx_t<T>::type* __restrict__ Wy) {
+  typedef typename cplx_t<T>::type C;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* A = (C*)smraw;
+  C* B = A + (size_t)TX * g.ny;
+  C* A2 = B + (size_t)TX * g.ny;
+  C* B2 = A2 + (size_t)TX * g.ny;
+  const YJob<T> jb = jobs.j[blockIdx.z];
+  const int k = blockIdx.y;
+  const int ntile = (g.nxhp + TX - 1) / TX;  // includes the Nyquist column
+  const int ii0 = blockIdx.x * TX;
+  const int ny = g.ny;
+  const bool fwd = jb.mode >= 2;
+  const bool two = jb.mode == 3;
+  (void)ntile;
+  (void)nplanes;
+  // load: A[b*ny + j] = column (ii0+b), row j
+  for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
+    int b = t % TX, j = t / TX;
+    int ii = ii0 + b;
+    C v = cmk<C>(0, 0), v2 = cmk<C>(0, 0);
+    if (ii < g.nxhp) {
+      const T* p = jb.src + fidx<T>(g, 2 * ii, j, k);
+      v = cmk<C>(p[0], p[1]);
+      if (two) {
+        const T* p2 = jb.src2 + fidx<T>(g, 2 * ii, j, k);
+        v2 = cmk<C>(p2[0], p2[1]);
+      }
+      if (jb.mode == 1) {
+        T ky = (T)g.yw[j];
+        v = cmk<C>(-(ky * v.y), ky * v.x);
+      }
+    }
+    A[b * ny + j] = v;
+    if (two) A2[b * ny + j] = v2;
+  }
+  __syncthreads();
+  C* res = A;
+  C* res2 = A2;
+  int nb = min(TX, g.nxh - ii0);  // transformed columns in this tile
+  if (nb > 0 && ny > 1) {
+    res = fft_run<C>(A, B, pl, nb, Wy, !fwd, threadIdx.x, blockDim.x);
+    if (two) res2 = fft_run<C>(A2, B2, pl, nb, Wy, !fwd, threadIdx.x, blockDim.x);
+  }
+  // the Nyquist column (ii = nxh) stays where it was: copy it if the
+  // transform wrote the result to the other buffer
+  const T sc = fwd ? (T)g.scaley : (T)1;
+  for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
+    int b = t % TX, j = t / TX;
+    int ii = ii0 + b;
+    if (ii >= g.nxhp) continue;
+    bool tr = (ii < g.nxh) && ny > 1;
+    C v = tr ? res[b * ny + j] : A[b * ny + j];
+    C o = cmk<C>(v.x * sc, v.y * sc);
+    if (two) {
+      C v2 = tr ? res2[b * ny + j] : A2[b * ny + j];
+      C w2 = cmk<C>(v2.x * sc, v2.y * sc);
+      T ky = (T)g.yw[j];
+      o = cmk<C>(o.x - ky * w2.y, o.y + ky * w2.x);
+    }
+    T* p = jb.dst + fidx<T>(g, 2 * ii, j, k);
+    p[0] = o.x;
+    p[1] = o.y;
+  }
+}
+
+// ===========================================================================
+// x transforms of rows.  Real length nx = 2M through complex length M.
+// ===========================================================================
+template <typename C, typename T>
+__device__ __forceinline__ void xinv_prep(const T* __restrict__ row, C* Z, int M, const C* __restrict__ Wn, int mulkx,
+                                          T kxstep, int t0, int nthr) {
+  // row: nxhp complex (interleaved); optional multiply by i*kx (kx = m*kxstep)
+  for (int k = t0; k < M; k += nthr) {
+    C Xk = cmk<C>(row[2 * k], row[2 * k + 1]);
+    C Xm = cmk<C>(row[2 * (M - k)], row[2 * (M - k) + 1]);
+    if (mulkx) {
+      T a = kxstep * (T)k, b = kxstep * (T)(M - k);
+      Xk = cmk<C>(-(a * Xk.y), a * Xk.x);
+      Xm = cmk<C>(-(b * Xm.y), b * Xm.x);
+    }
+    if (k == 0) {
+      Xk.y = 0;
+      Xm.y = 0;
+    }
+    C s = cadd(Xk, cconj(Xm));
+    C d = csub(Xk, cconj(Xm));
+    C w = Wn[k];  // exp(-2 pi i k/N); need i*conj(w)*d
+    C wc = cconj(w);
+    C t = cmul(wc, d);
+    Z[k] = cmk<C>(s.x - t.y, s.y + t.x);
+  }
+}
+
+// forward post: Z = FFT_M(z) -> X_k k=0..M (scaled by 1/N)
+template <typename C>
+__device__ __forceinline__ C xfwd_post(const C* Z, int k, int M, const C* __restrict__ Wn, decltype(C().x) invN) {
+  typedef decltype(C().x) T;
+  if (k == 0) return cmk<C>((Z[0].x + Z[0].y) * invN, (T)0);
+  if (k == M) return cmk<C>((Z[0].x - Z[0].y) * invN, (T)0);
+  C a = Z[k], b = cconj(Z[M - k]);
+  C e = cmk<C>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y + b.y));
+  C dd = csub(a, b);
+  C o = cmk<C>((T)0.5 * dd.y, (T)-0.5 * dd.x);  // (a-b)/(2i)
+  C w = Wn[k];
+  C wo = cmul(w, o);
+  return cmk<C>((e.x + wo.x) * invN, (e.y + wo.y) * invN);
+}
+
+// Parameters of the fused NL row kernel.
+template <typename T>
+struct NLArgs {
+  const T* in[12];  // (kx,y): u v w t | dy u v w t | dz u v w t
+  T* out[11];       // (kx,y): Au Av Aw At | uv vv vw vt | uw ww wt
+  double coef_buoy; // N^2 / rhograd
+  double rg;        // rhograd
+  double tau_pen[IW_MAX_SUBD];  // 0.5/omega*(2/zh)
+  int forcing;
+  double f_xk, f_xm, f_om, f_t, f_amp_u, f_amp_w, f_amp_r;  // paddle
+  double dx;
+};
+
+// K_C: CTA per (j,k) row.  smem: two buffers of 20 rows of M complex.
+template <typename T>
+__global__ void __launch_bounds__(256) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl, const typename cplx_t<T>::type* __restrict__ Wm,
+                                                 const typename cplx_t<T>::type* __restrict__ Wn) {
+  typedef typename cplx_t<T>::type C;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int M = g.nx / 2;
+  C* A = (C*)smraw;
+  C* B = A + 20 * M;
+  const int j = blockIdx.x, k = blockIdx.y;
+  const int N = g.N;
+  const int kl = k % N, ks = k / N;
+  const bool nb_lo = (kl == 0 && k > 0);
+  const bool nb_hi = (kl == N - 1 && k < g.nz - 1);
+  const int knb = nb_lo ? k - 1 : k + 1;
+  const int nrow = 16 + ((nb_lo || nb_hi) ? 4 : 0);
+  const T kxs = (T)g.xw[1];
+  // rows 0..3 u v w t, 4..7 dx, 8..11 dy, 12..15 dz, 16..19 neighbour u v w t
+  for (int r = 0; r < nrow; ++r) {
+    const T* src;
+    int mk = 0;
+    size_t off;
+    if (r < 4) {
+      src = a.in[r];
+      off = fidx<T>(g, 0, j, k);
+    } else if (r < 8) {
+      src = a.in[r - 4];
+      mk = 1;
+      off = fidx<T>(g, 0, j, k);
+    } else if (r < 16) {
+      src = a.in[r - 4];
+      off = fidx<T>(g, 0, j, k);
+    } else {
+      src = a.in[r - 16];
+      off = fidx<T>(g, 0, j, knb);
+    }
+    xinv_prep<C, T>(src + off, A + r * M, M, Wn, mk, kxs, threadIdx.x, blockDim.x);
+  }
+  __syncthreads();
+  C* ph = fft_run<C>(A, B, pl, nrow, Wm, true, threadIdx.x, blockDim.x);
+  C* pr = (ph == A) ? B : A;  // products go to the other buffer
+  const T* P = (const T*)ph;   // physical row r: P[r*2M + i]
+  T* Q = (T*)pr;
+  const int nx = g.nx;
+  // upwind interface penalty (solver.f:700-839)
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    T u = P[0 * nx + i], v = P[1 * nx + i], w = P[2 * nx + i], t = P[3 * nx + i];
+    T ux = P[4 * nx + i], vx = P[5 * nx + i], wx = P[6 * nx + i], tx = P[7 * nx + i];
+    T uy = P[8 * nx + i], vy = P[9 * nx + i], wy = P[10 * nx + i];
+    T uz = P[12 * nx + i], vz = P[13 * nx + i], wz = P[14 * nx + i];
+    (void)tx;
+    T qu = (T)-0.5 * (u * ux + v * uy + w * uz);
+    T qv = (T)-0.5 * (u * vx + v * vy + w * vz);
+    T qw = (T)-0.5 * (u * wx + v * wy + w * wz) + (T)a.coef_buoy * t;
+    T qt = -(w * (T)a.rg);
+    if (kl == 0 && k > 0) {
+      // bottom point of subdomain ks: inflow from below when w > 0
+      if (w > (T)0) {
+        T tau = (T)a.tau_pen[ks];
+        T al = w;
+        qu -= tau * (al * u - al * P[16 * nx + i]);
+        qv -= tau * (al * v - al * P[17 * nx + i]);
+        qw -= tau * (al * w - al * P[18 * nx + i]);
+        qt -= tau * (al * t - al * P[19 * nx + i]);
+      }
+    }
+    if (kl == N - 1 && k < g.nz - 1) {
+      if (w < (T)0) {
+        T tau = (T)a.tau_pen[ks];
+        T ga = -w;
+        qu -= tau * (ga * u - ga * P[16 * nx + i]);
+        qv -= tau * (ga * v - ga * P[17 * nx + i]);
+        qw -= tau * (ga * w - ga * P[18 * nx + i]);
+        qt -= tau * (ga * t - ga * P[19 * nx + i]);
+      }
+    }
+    if (a.forcing) {
+      double xx = (double)i * a.dx, zz = g.zg[k];
+      double arg = a.f_xk * xx - a.f_om * a.f_t;
+      double sf, cf;
+      sincos(arg, &sf, &cf);
+      double czm = cos(a.f_xm * zz), szm = sin(a.f_xm * zz);
+      qu += (T)(a.f_amp_u * czm * sf);
+      qw += (T)(a.f_amp_w * szm * cf);
+      qt += (T)(a.f_amp_r * szm * sf);
+    }
+    // 13 rows to transform: Qu Qv Qw Qt | uu uv uw ut | vv vw vt | ww wt
+    Q[0 * nx + i] = qu;
+    Q[1 * nx + i] = qv;
+    Q[2 * nx + i] = qw;
+    Q[3 * nx + i] = qt;
+    Q[4 * nx + i] = (T)-0.5 * u * u;
+    Q[5 * nx + i] = (T)-0.5 * u * v;
+    Q[6 * nx + i] = (T)-0.5 * u * w;
+    Q[7 * nx + i] = -(u * t);
+    Q[8 * nx + i] = (T)-0.5 * v * v;
+    Q[9 * nx + i] = (T)-0.5 * v * w;
+    Q[10 * nx + i] = -(v * t);
+    Q[11 * nx + i] = (T)-0.5 * w * w;
+    Q[12 * nx + i] = -(w * t);
+  }
+  __syncthreads();
+  C* sp = fft_run<C>(pr, ph, pl, 13, Wm, false, threadIdx.x, blockDim.x);
+  const T invN = (T)1 / (T)nx;
+  // outputs: A_q = X(Q_q) + i kx X(P_uq) for q = u v w t ; then uv vv vw vt uw ww wt
+  const int nout = M + 1;
+  for (int t = threadIdx.x; t < 11 * nout; t += blockDim.x) {
+    int o = t / nout, kk = t % nout;
+    C val;
+    if (o < 4) {
+      C x1 = xfwd_post<C>(sp + o * M, kk, M, Wn, invN);
+      C x2 = xfwd_post<C>(sp + (4 + o) * M, kk, M, Wn, invN);
+      T kx = kxs * (T)kk;
+      val = cmk<C>(x1.x - kx * x2.y, x1.y + kx * x2.x);
+    } else {
+      // map: 4->uv(5) 5->vv(8) 6->vw(9) 7->vt(10) 8->uw(6) 9->ww(11) 10->wt(12)
+      const int src_row[7] = {5, 8, 9, 10, 6, 11, 12};
+      val = xfwd_post<C>(sp + src_row[o - 4] * M, kk, M, Wn, invN);
+    }
+    T* p = a.out[o] + fidx<T>(g, 2 * kk, j, k);
+    p[0] = val.x;
+    p[1] = val.y;
+  }
+}
+
+// ===========================================================================
+// K_E: per (field q, real x index i, y index j, subdomain ks):
+//   S    = B + (2/h) D Z                     (NL term at level n, spectral)
+//   wnl  = fac1 S + fac2 Sn + fac3 Snm at the walls (w only, solver.f:267-284)
+//   F2   = P(F1)                             (end-of-rhsfm round trip)
+//   F*   = dt (fac1 S + fac2 Sn + fac3 Snm) + bdf1 F2 + bdf2 Fn + bdf3 Fnm
+//   Snm <- S (becomes Sn), Fnm <- F2 (becomes Fn)      (solver.f:447-478)
+//   F   <- cf(ii,j) * L F* per subdomain    (filter_3dlegenfourier)
+// ===========================================================================
+struct Coefs {
+  double fac1, fac2, fac3, bdf1, bdf2, bdf3, bdfv, dt;
+};
+
+template <typename T>
+struct EArgs {
+  const T* B[4];
+  const T* Z[4];
+  const T* F1[4];
+  const T* Fn[4];
+  const T* Snold[4];
+  T* Snm_w[4];  // in: S_{n-2}; out: S (new level n-1 after rotation)
+  T* Fnm_w[4];  // in: F_{n-2}; out: F2 (new level n-1)
+  T* F[4];      // out: filtered u*
+  double* wnl;  // (nxpp,ny,2)
+  int filter;
+};
+
+template <typename T, int NM>
+__global__ void k_stageE(Geo g, EArgs<T> a, Coefs c) {
+  __shared__ double sD[NM * NM];
+  __shared__ double sL[NM * NM];
+  for (int t = threadIdx.x; t < g.N * g.N; t += blockDim.x) {
+    sD[t] = g.D[t];
+    sL[t] = g.Lfil[t];
+  }
+  __syncthreads();
+  const int q = blockIdx.z;
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long total = (long)g.nxpp * g.ny * g.ns;
+  if (gid >= total) return;
+  int i = gid % g.nxpp;
+  long r = gid / g.nxpp;
+  int j = r % g.ny;
+  int ks = r / g.ny;
+  const int N = g.N;
+  T z[NM], fs[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k)
+    if (k < N) z[k] = a.Z[q][fidx<T>(g, i, j, ks * N + k)];
+  const T fac = (T)g.hfac[ks];
+  const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1)
+    if (k1 < N) {
+      const int kk = ks * N + k1;
+      const size_t p = fidx<T>(g, i, j, kk);
+      T s = 0;
+#pragma unroll
+      for (int k2 = 0; k2 < NM; ++k2)
+        if (k2 < N) s += (T)sD[k1 * N + k2] * z[k2];
+      T S = a.B[q][p] + s * fac;
+      T sn = a.Snold[q][p];
+      T snm = a.Snm_w[q][p];
+      if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
+        int side = kk == 0 ? 0 : 1;
+        a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] =
+            (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
+      }
+      T se = f1 * S + f2 * sn + f3 * snm;
+      T F2 = proj_val<T>(g, a.F1[q], i, j, kk);
+      T fn = a.Fn[q][p];
+      T fnm = a.Fnm_w[q][p];
+      fs[k1] = (T)c.dt * se + (T)c.bdf1 * F2 + (T)c.bdf2 * fn + (T)c.bdf3 * fnm;
+      a.Snm_w[q][p] = S;
+      a.Fnm_w[q][p] = F2;
+    }
+  const int ii = i >> 1;
+  const T cf = a.filter ? (T)g.cfour[(size_t)j * g.nxhp + ii] : (T)1;
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1)
+    if (k1 < N) {
+      T o;
+      if (a.filter) {
+        T s = 0;
+#pragma unroll
+        for (int k2 = 0; k2 < NM; ++k2)
+          if (k2 < N) s += (T)sL[k1 * N + k2] * fs[k2];
+        o = cf * s;
+      } else {
+        o = fs[k1];
+      }
+      a.F[q][fidx<T>(g, i, j, ks * N + k1)] = o;
+    }
+}
+
+// rotational viscous term at the walls (solver.f:318-394, rotvisc 1210-1253):
+// wviscrot = -nu * (fac1 rot(n) + fac2 rot(n-1) + fac3 rot(n-2)),
+// rot = (kx^2+ky^2) w + i kx du/dz + i ky dv/dz at k0.
+template <typename T>
+__global__ void k_wviscrot(Geo g, const T* __restrict__ u1, const T* __restrict__ v1, const T* __restrict__ w1,
+                           const T* __restrict__ un, const T* __restrict__ vn, const T* __restrict__ wn,
+                           const T* __restrict__ unm, const T* __restrict__ vnm, const T* __restrict__ wnm, Coefs c,
+                           double xnu, double* __restrict__ wvr) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long total = (long)g.nxhp * g.ny * 2;
+  if (gid >= total) return;
+  int ii = gid % g.nxhp;
+  long r = gid / g.nxhp;
+  int j = r % g.ny;
+  int side = r / g.ny;
+  const int N = g.N;
+  int ks = side == 0 ? 0 : g.ns - 1;
+  int k0 = side == 0 ? 0 : N - 1;
+  double fac = g.hfac[ks];
+  double xw = g.xw[ii], yw = g.yw[j];
+  double rr = 0, ri = 0;
+  for (int l = 0; l < 3; ++l) {
+    const T* U = l == 0 ? u1 : l == 1 ? un : unm;
+    const T* V = l == 0 ? v1 : l == 1 ? vn : vnm;
+    const T* W = l == 0 ? w1 : l == 1 ? wn : wnm;
+    double dur = 0, dui = 0, dvr = 0, dvi = 0;
+    for (int k2 = 0; k2 < N; ++k2) {
+      int kk = ks * N + k2;
+      double d = g.D[k0 * N + k2];
+      double ur, ui, vr, vi;
+      if (l == 0) {
+        ur = proj_val<T>(g, U, 2 * ii, j, kk);
+        ui = proj_val<T>(g, U, 2 * ii + 1, j, kk);
+        vr = proj_val<T>(g, V, 2 * ii, j, kk);
+        vi = proj_val<T>(g, V, 2 * ii + 1, j, kk);
+      } else {
+        ur = U[fidx<T>(g, 2 * ii, j, kk)];
+        ui = U[fidx<T>(g, 2 * ii + 1, j, kk)];
+        vr = V[fidx<T>(g, 2 * ii, j, kk)];
+        vi = V[fidx<T>(g, 2 * ii + 1, j, kk)];
+      }
+      dur += d * ur;
+      dui += d * ui;
+      dvr += d * vr;
+      dvi += d * vi;
+    }
+    dur *= fac;
+    dui *= fac;
+    dvr *= fac;
+    dvi *= fac;
+    int kk0 = ks * N + k0;
+    double wr, wi;
+    if (l == 0) {
+      wr = proj_val<T>(g, W, 2 * ii, j, kk0);
+      wi = proj_val<T>(g, W, 2 * ii + 1, j, kk0);
+    } else {
+      wr = W[fidx<T>(g, 2 * ii, j, kk0)];
+      wi = W[fidx<T>(g, 2 * ii + 1, j, kk0)];
+    }
+    double re = xw * xw * wr + yw * yw * wr - xw * dui - yw * dvi;
+    double im = xw * xw * wi + yw * yw * wi + xw * dur + yw * dvr;
+    double f = l == 0 ? c.fac1 : l == 1 ? c.fac2 : c.fac3;
+    rr += f * re;
+    ri += f * im;
+  }
+  size_t base = (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side) + 2 * ii;
+  wvr[base] = -(xnu * rr);
+  wvr[base + 1] = -(xnu * ri);
+}
+
+// ===========================================================================
+// Band factorisation (penalty.f:403-634 assembly, band_lu.f:19-34 packing,
+// bandludcmp.f:238-440 SGBTF2).  One warp per system; the arithmetic follows
+// the reference order with no fused multiply-add, so the factors equal the
+// CPU ones bit for bit.
+// ===========================================================================
+struct SysDesc {
+  double eps;
+  double tau1_bot, tau2_top;  // for the RHS boundary rows
+  int ifbcbot, ifbctop;
+  int pad[2];
+};
+
+struct FactorArgs {
+  const SysDesc* sys;
+  const double* pen;  // per system: 6*ns (alpha,beta,gamma,delta,tau1,tau2)
+  double* ab;         // per system: ldab*nz
+  int* ipiv;          // per system: nz
+  int* info;          // per system
+  int nsys;
+  const double* D;
+  const double* D2;
+  const double* zh;  // ns
+  int assemble;      // 0: ab already holds the packed matrix (bandlu_solve_)
+};
+
+__device__ __forceinline__ double& ABr(double* ab, int ldab, int r, int c) {
+  return ab[(size_t)(r - 1) + (size_t)ldab * (size_t)(c - 1)];
+}
+
+__global__ void k_factor(Geo g, FactorArgs fa) {
+  const int warps = blockDim.x / 32;
+  const int s = blockIdx.x * warps + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (s >= fa.nsys) return;
+  const int n = g.nz, N = g.N, ns = g.ns, kl = N, ku = N, ldab = 2 * kl + ku + 1;
+  double* ab = fa.ab + (size_t)s * ldab * n;
+  int* ipiv = fa.ipiv + (size_t)s * n;
+  const double eps = fa.sys[s].eps;
+  const double* pen = fa.pen + (size_t)s * 6 * ns;
+  const double *pa = pen, *pb = pen + ns, *pg = pen + 2 * ns, *pd = pen + 3 * ns, *pt1 = pen + 4 * ns,
+               *pt2 = pen + 5 * ns;
+  const double* d = fa.D;
+  const double* d2 = fa.D2;
+  if (fa.assemble) {
+  // zero the band
+  for (size_t t = lane; t < (size_t)ldab * n; t += 32) ab[t] = 0.0;
+  __syncwarp();
+  // A(r,c) 0-based -> band row kl+ku+1+r-c (1-based), column c+1
+#define AEL(r, c) ABr(ab, ldab, kl + ku + 1 + (r) - (c), (c) + 1)
+  for (int ks = 0; ks < ns; ++ks) {
+    const double ybar = fa.zh[ks];
+    const double ybarl = ks > 0 ? fa.zh[ks - 1] : 0.0;
+    const double ybarr = ks < ns - 1 ? fa.zh[ks + 1] : 0.0;
+    const int km = ks * N;
+    const double h2 = rmul(2.0 / ybar, 2.0 / ybar);
+    const double eh = rmul(eps, h2);
+    for (int t = lane; t < N * N; t += 32) {
+      int k1 = t / N, k2 = t % N;
+      AEL(km + k1, km + k2) = -rmul(eh, d2[k1 * N + k2]);
+    }
+    __syncwarp();
+    for (int k1 = lane; k1 < N; k1 += 32) AEL(km + k1, km + k1) = radd(AEL(km + k1, km + k1), 1.0);
+    __syncwarp();
+    if (lane == 0) AEL(km, km) = radd(AEL(km, km), rmul(pt1[ks], pa[ks]));
+    __syncwarp();
+    {
+      double cf = -__ddiv_rn(rmul(rmul(rmul(pt1[ks], pb[ks]), eps), 2.0), ybar);
+      for (int k = lane; k < N; k += 32) AEL(km, km + k) = radd(AEL(km, km + k), rmul(cf, d[0 * N + k]));
+    }
+    __syncwarp();
+    if (lane == 0) AEL(km + N - 1, km + N - 1) = radd(AEL(km + N - 1, km + N - 1), rmul(pt2[ks], pg[ks]));
+    __syncwarp();
+    {
+      double cf = __ddiv_rn(rmul(rmul(rmul(pt2[ks], pd[ks]), eps), 2.0), ybar);
+      for (int k = lane; k < N; k += 32)
+        AEL(km + N - 1, km + k) = radd(AEL(km + N - 1, km + k), rmul(cf, d[(N - 1) * N + k]));
+    }
+    __syncwarp();
+    if (ns > 1 && ks != 0) {
+      if (lane == 0) AEL(km, km) = rsub(AEL(km, km), rmul(rmul(0.5, pt1[ks]), pa[ks]));
+      __syncwarp();
+      double cf = __ddiv_rn(rmul(rmul(rmul(rmul(0.5, pt1[ks]), pb[ks]), eps), 2.0), ybar);
+      for (int k = lane; k < N; k += 32) AEL(km, km + k) = radd(AEL(km, km + k), rmul(cf, d[0 * N + k]));
+      __syncwarp();
+      for (int k = lane; k < N; k += 32) AEL(km, km - N + k) = 0.0;
+      __syncwarp();
+      if (lane == 0) AEL(km, km - 1) = -rmul(rmul(0.5, pt1[ks]), pa[ks]);
+      __syncwarp();
+      cf = __ddiv_rn(rmul(rmul(rmul(rmul(0.5, pt1[ks]), pb[ks]), eps), 2.0), ybarl);
+      for (int k = lane; k < N; k += 32)
+        AEL(km, km - N + k) = radd(AEL(km, km - N + k), rmul(cf, d[(N - 1) * N + k]));
+      __syncwarp();
+    }
+    if (ns > 1 && ks != ns - 1) {
+      if (lane == 0) AEL(km + N - 1, km + N - 1) = rsub(AEL(km + N - 1, km + N - 1), rmul(rmul(0.5, pt2[ks]), pg[ks]));
+      __syncwarp();
+      double cf = -__ddiv_rn(rmul(rmul(rmul(rmul(0.5, pt2[ks]), pd[ks]), eps), 2.0), ybar);
+      for (int k = lane; k < N; k += 32)
+        AEL(km + N - 1, km + k) = radd(AEL(km + N - 1, km + k), rmul(cf, d[(N - 1) * N + k]));
+      __syncwarp();
+      // a(km+1, km+nzloc+k) = 0: outside the band for nzloc >= 2 except the
+      // row's own band part, which is zero here already
+      if (lane == 0) AEL(km + N - 1, km + N) = rsub(AEL(km + N - 1, km + N), rmul(rmul(0.5, pt2[ks]), pg[ks]));
+      __syncwarp();
+      cf = -__ddiv_rn(rmul(rmul(rmul(rmul(0.5, pt2[ks]), pd[ks]), eps), 2.0), ybarr);
+      for (int k = lane; k < N; k += 32)
+        AEL(km + N - 1, km + N + k) = radd(AEL(km + N - 1, km + N + k), rmul(cf, d[0 * N + k]));
+      __syncwarp();
+    }
+  }
+#undef AEL
+  }
+  // SGBTF2
+  const int kv = ku + kl;
+  int info = 0;
+  for (int jj = ku + 2; jj <= min(kv, n); ++jj)
+    for (int i = kv - jj + 2 + lane; i <= kl; i += 32) ABr(ab, ldab, i, jj) = 0.0;
+  __syncwarp();
+  int ju = 1;
+  for (int j = 1; j <= n; ++j) {
+    if (j + kv <= n)
+      for (int i = 1 + lane; i <= kl; i += 32) ABr(ab, ldab, i, j + kv) = 0.0;
+    __syncwarp();
+    const int km = min(kl, n - j);
+    // ISAMAX: first index of the largest |a|
+    double best = -1.0;
+    int bi = 1 << 30;
+    for (int i = 1 + lane; i <= km + 1; i += 32) {
+      double v = fabs(ABr(ab, ldab, kv + i, j));
+      if (v > best) {
+        best = v;
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    const int jp = bi;
+    if (lane == 0) ipiv[j - 1] = jp + j - 1;
+    const double piv = ABr(ab, ldab, kv + jp, j);
+    __syncwarp();
+    if (piv != 0.0) {
+      ju = max(ju, min(j + ku + jp - 1, n));
+      if (jp != 1) {
+        for (int cc = lane; cc < ju - j + 1; cc += 32) {
+          double t1 = ABr(ab, ldab, kv + jp - cc, j + cc);
+          ABr(ab, ldab, kv + jp - cc, j + cc) = ABr(ab, ldab, kv + 1 - cc, j + cc);
+          ABr(ab, ldab, kv + 1 - cc, j + cc) = t1;
+        }
+      }
+      __syncwarp();
+      if (km > 0) {
+        const double rcp = __ddiv_rn(1.0, ABr(ab, ldab, kv + 1, j));
+        for (int i = 1 + lane; i <= km; i += 32) ABr(ab, ldab, kv + 1 + i, j) = rmul(rcp, ABr(ab, ldab, kv + 1 + i, j));
+        __syncwarp();
+        if (ju > j) {
+          for (int jj = 1 + lane; jj <= ju - j; jj += 32) {
+            double y = ABr(ab, ldab, kv + 1 - jj, j + jj);
+            if (y != 0.0) {
+              double temp = -y;
+              for (int ii = 1; ii <= km; ++ii) {
+                double& x = ABr(ab, ldab, kv + 1 + ii - jj, j + jj);
+                x = radd(x, rmul(ABr(ab, ldab, kv + 1 + ii, j), temp));
+              }
+            }
+          }
+        }
+        __syncwarp();
+      }
+    } else if (info == 0) {
+      info = j;
+    }
+  }
+  if (lane == 0) fa.info[s] = info;
+}
+
+// ===========================================================================
+// Warp-cooperative banded solve (SGBTRS 'N' + STBSV, bandludcmp.f:883-1069)
+// for nr right-hand sides b[r*n + row] in shared memory; same arithmetic as
+// the reference (no FMA) so results equal the CPU ones bit for bit.
+// ===========================================================================
+__device__ void band_solve_warp(const double* __restrict__ ab, const int* __restrict__ ipiv, double* b, int nr,
+                                int n, int kl, int ku, int lane) {
+  const int ldab = 2 * kl + ku + 1;
+  const int kd = ku + kl + 1;
+  for (int j = 1; j <= n - 1; ++j) {
+    const int lm = min(kl, n - j);
+    const int l = __ldg(ipiv + j - 1);
+    const double* col = ab + (size_t)ldab * (j - 1);
+    for (int r = 0; r < nr; ++r) {
+      double* br = b + (size_t)r * n;
+      const double bj = br[j - 1];
+      const double bl = br[l - 1];
+      const double y = (l != j) ? bl : bj;
+      double nv0 = 0, nv1 = 0;
+      const int i0 = lane + 1, i1 = lane + 33;
+      if (i0 <= lm) {
+        int row = j + i0;
+        double old = (row == l) ? bj : br[row - 1];
+        nv0 = (y != 0.0) ? radd(old, rmul(__ldg(col + kd + i0 - 1), -y)) : old;
+      }
+      if (i1 <= lm) {
+        int row = j + i1;
+        double old = (row == l) ? bj : br[row - 1];
+        nv1 = (y != 0.0) ? radd(old, rmul(__ldg(col + kd + i1 - 1), -y)) : old;
+      }
+      __syncwarp();
+      if (i0 <= lm) br[j + i0 - 1] = nv0;
+      if (i1 <= lm) br[j + i1 - 1] = nv1;
+      if (lane == 0) br[j - 1] = y;
+      __syncwarp();
+    }
+  }
+  const int k = kl + ku, kplus1 = k + 1;
+  for (int j = n; j >= 1; --j) {
+    const double* col = ab + (size_t)ldab * (j - 1);
+    const double dg = __ldg(col + kplus1 - 1);
+    const int lo = max(1, j - k);
+    for (int r = 0; r < nr; ++r) {
+      double* br = b + (size_t)r * n;
+      double xj = br[j - 1];
+      if (xj != 0.0) {
+        xj = __ddiv_rn(xj, dg);
+        const int l = kplus1 - j;
+        double nv[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          int i = j - 1 - lane - 32 * m;
+          nv[m] = 0;
+          if (i >= lo) nv[m] = rsub(br[i - 1], rmul(xj, __ldg(col + l + i - 1)));
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          int i = j - 1 - lane - 32 * m;
+          if (i >= lo) br[i - 1] = nv[m];
+        }
+        if (lane == 0) br[j - 1] = xj;
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// Legendre filter of solution columns (filtering.f:729-808, filter_legenpen),
+// same order of operations as the reference.  One lane per subdomain column.
+__device__ void legen_filter_cols(double* b, int nr, int n, int N, int ns, const double* __restrict__ wg,
+                                  const double* __restrict__ alpol, const double* __restrict__ sigma, int lane) {
+  const int nzm = N - 1;
+  for (int t = lane; t < nr * ns; t += 32) {
+    double* f = b + (size_t)(t / ns) * n + (size_t)(t % ns) * N;
+    double af[kMaxN];
+    for (int kk = 0; kk <= nzm; ++kk) {
+      double sum = 0.0;
+      for (int k1 = 0; k1 < N; ++k1) sum = radd(sum, rmul(rmul(wg[k1], f[k1]), alpol[kk * N + k1]));
+      double a = (kk == nzm) ? rmul(rmul(0.5, (double)nzm), sum) : rmul((double)kk + 0.5, sum);
+      af[kk] = rmul(a, sigma[kk]);
+    }
+    for (int k1 = 0; k1 < N; ++k1) {
+      double sum = 0.0;
+      for (int kk = 0; kk <= nzm; ++kk) sum = radd(sum, rmul(af[kk], alpol[kk * N + k1]));
+      f[k1] = sum;
+    }
+  }
+}
+
+struct SolveTabs {
+  const double* ab;      // ldab*nz per system
+  const int* ipiv;       // nz per system
+  const SysDesc* sys;
+  const int* col_sys;    // per column (j*nxhp+ii): system index (-1: none)
+  const double* wg;
+  const double* alpol;   // N*N: alpol[k*N + k1] = P_k(z_k1)
+  const double* sigma;   // N
+  const double* meang;   // nz: 1 - fzgaus(z) (mean-u damping) or null
+};
+
+// K_F: pressure.  Warp per (ii,j) column.  Reads filtered u*,v*,w* (state F),
+// writes ub, vb, wb into the same arrays (calcuvwt.f:87-229 + update 826-901).
+template <typename T>
+__global__ void k_press(Geo g, SolveTabs tb, T* __restrict__ U, T* __restrict__ V, T* __restrict__ W,
+                        const double* __restrict__ wnl, const double* __restrict__ wvr, int cpen, int kstart) {
+  extern __shared__ __align__(16) double sm[];
+  const int warps = blockDim.x / 32;
+  const int wid = threadIdx.x / 32, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * warps + wid;
+  const int ncol = g.nxhp * g.ny;
+  if (c >= ncol) return;
+  const int n = g.nz, N = g.N;
+  double* buf = sm + (size_t)wid * 4 * n;  // [0,2n): w* re/im, [2n,4n): rhs/phi re/im
+  const int j = c / g.nxhp, ii = c % g.nxhp;
+  const double xw = g.xw[ii], yw = g.yw[j], dt = g.dt;
+  const int s = tb.col_sys[c];
+  for (int k = lane; k < n; k += 32) {
+    buf[k] = (double)W[fidx<T>(g, 2 * ii, j, k)];
+    buf[n + k] = (double)W[fidx<T>(g, 2 * ii + 1, j, k)];
+  }
+  __syncwarp();
+  double* rr = buf + 2 * n;
+  double* ri = buf + 3 * n;
+  if (s >= 0) {
+    const SysDesc sd = tb.sys[s];
+    const double eps = sd.eps;
+    // divcolc (derv.f:35-85) and rhs = div/dt, then rhs *= -eps
+    for (int k = lane; k < n; k += 32) {
+      int ks = k / N, k1 = k % N;
+      double sr = 0.0, si = 0.0;
+      for (int k2 = 0; k2 < N; ++k2) {
+        double dd = g.D[k1 * N + k2];
+        sr = radd(sr, rmul(dd, buf[ks * N + k2]));
+        si = radd(si, rmul(dd, buf[n + ks * N + k2]));
+      }
+      double fac = g.hfac[ks];
+      double dwr = rmul(sr, fac), dwi = rmul(si, fac);
+      double ur = (double)U[fidx<T>(g, 2 * ii, j, k)], ui = (double)U[fidx<T>(g, 2 * ii + 1, j, k)];
+      double vr = (double)V[fidx<T>(g, 2 * ii, j, k)], vi = (double)V[fidx<T>(g, 2 * ii + 1, j, k)];
+      double dr = radd(radd(0.0, -rmul(xw, ui)), -rmul(yw, vi));
+      double di = radd(radd(0.0, rmul(xw, ur)), rmul(yw, vr));
+      dr = radd(dr, dwr);
+      di = radd(di, dwi);
+      double r1 = __ddiv_rn(dr, dt), r2 = __ddiv_rn(di, dt);
+      rr[k] = -rmul(r1, eps);
+      ri[k] = -rmul(r2, eps);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      size_t p1 = (size_t)g.nxpp * j + 2 * ii, p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii;
+      double bcrbot = radd(wnl[p1], wvr[p1]), bcibot = radd(wnl[p1 + 1], wvr[p1 + 1]);
+      double bcrtop = radd(wnl[p2], wvr[p2]), bcitop = radd(wnl[p2 + 1], wvr[p2 + 1]);
+      // Neumann rows (penalty.f:594-604)
+      rr[0] = rsub(rr[0], rmul(rmul(sd.tau1_bot, bcrbot), eps));
+      ri[0] = rsub(ri[0], rmul(rmul(sd.tau1_bot, bcibot), eps));
+      rr[n - 1] = radd(rr[n - 1], rmul(rmul(sd.tau2_top, bcrtop), eps));
+      ri[n - 1] = radd(ri[n - 1], rmul(rmul(sd.tau2_top, bcitop), eps));
+    }
+    __syncwarp();
+    const int ldab = 3 * N + 1;
+    band_solve_warp(tb.ab + (size_t)s * ldab * n, tb.ipiv + (size_t)s * n, rr, 2, n, N, N, lane);
+    if (cpen) {
+      legen_filter_cols(rr, 2, n, N, g.ns, tb.wg, tb.alpol, tb.sigma, lane);
+      __syncwarp();
+    }
+  } else {
+    for (int k = lane; k < n; k += 32) {
+      rr[k] = 0.0;
+      ri[k] = 0.0;
+    }
+    __syncwarp();
+  }
+  // projection (update): ub = u* - dt i kx phi, vb likewise, wb = w* - dt dphi/dz
+  const bool lzero = (ii == 0 && j == 0);
+  const double dtx = rmul(dt, xw), dty = rmul(dt, yw);
+  for (int k = lane; k < n; k += 32) {
+    size_t pr = fidx<T>(g, 2 * ii, j, k), pi = pr + 1;
+    if (k < kstart) {
+      U[pr] = 0;
+      U[pi] = 0;
+      V[pr] = 0;
+      V[pi] = 0;
+      W[pr] = 0;
+      W[pi] = 0;
+      continue;
+    }
+    double phr = rr[k], phi = ri[k];
+    double ur = (double)U[pr], ui = (double)U[pi], vr = (double)V[pr], vi = (double)V[pi];
+    U[pr] = (T)rsub(ur, rsub(rmul(0.0, phr), rmul(dtx, phi)));
+    U[pi] = (T)rsub(ui, radd(rmul(0.0, phi), rmul(dtx, phr)));
+    V[pr] = (T)rsub(vr, rsub(rmul(0.0, phr), rmul(dty, phi)));
+    V[pi] = (T)rsub(vi, radd(rmul(0.0, phi), rmul(dty, phr)));
+    if (lzero) {
+      W[pr] = 0;
+      W[pi] = 0;
+    } else {
+      int ks = k / N, k1 = k % N;
+      double sr = 0.0, si = 0.0;
+      for (int k2 = 0; k2 < N; ++k2) {
+        double dd = g.D[k1 * N + k2];
+        sr = radd(sr, rmul(dd, rr[ks * N + k2]));
+        si = radd(si, rmul(dd, ri[ks * N + k2]));
+      }
+      double fac = g.hfac[ks];
+      W[pr] = (T)rsub(buf[k], rmul(dt, rmul(sr, fac)));
+      W[pi] = (T)rsub(buf[n + k], rmul(dt, rmul(si, fac)));
+    }
+  }
+}
+
+// K_G: viscous/diffusive solves.  role 0: u and v (4 RHS, one factor),
+// role 1: w, role 2: rho.  Warp per column.
+template <typename T>
+__global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ F1, double rdiv, int role, int cpen,
+                       int meanu) {
+  extern __shared__ __align__(16) double sm[];
+  const int warps = blockDim.x / 32;
+  const int wid = threadIdx.x / 32, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * warps + wid;
+  const int ncol = g.nxhp * g.ny;
+  if (c >= ncol) return;
+  const int n = g.nz, N = g.N;
+  const int nr = role == 0 ? 4 : 2;
+  double* b = sm + (size_t)wid * 4 * n;
+  const int j = c / g.nxhp, ii = c % g.nxhp;
+  const bool lzero = (ii == 0 && j == 0);
+  const int s = tb.col_sys[c];
+  T* Fs[2] = {F0, F1};
+  if (s < 0) {  // w of the (0,0) mode is zero (calcuvwt.f:488-496)
+    for (int k = lane; k < n; k += 32) {
+      F0[fidx<T>(g, 2 * ii, j, k)] = 0;
+      F0[fidx<T>(g, 2 * ii + 1, j, k)] = 0;
+    }
+    return;
+  }
+  const SysDesc sd = tb.sys[s];
+  const double eps = sd.eps;
+  for (int r = 0; r < nr; ++r) {
+    T* F = Fs[r / 2];
+    int part = r & 1;
+    for (int k = lane; k < n; k += 32) {
+      double x = (double)F[fidx<T>(g, 2 * ii + part, j, k)];
+      double rh = -__ddiv_rn(x, rdiv);
+      b[(size_t)r * n + k] = -rmul(rh, eps);
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    // homogeneous boundary values: Dirichlet adds tau*0, Neumann tau*0*eps
+    for (int r = 0; r < nr; ++r) {
+      double* br = b + (size_t)r * n;
+      br[0] = sd.ifbcbot == 0 ? radd(br[0], rmul(sd.tau1_bot, 0.0)) : rsub(br[0], rmul(rmul(sd.tau1_bot, 0.0), eps));
+      br[n - 1] = sd.ifbctop == 0 ? radd(br[n - 1], rmul(sd.tau2_top, 0.0))
+                                  : radd(br[n - 1], rmul(rmul(sd.tau2_top, 0.0), eps));
+    }
+  }
+  __syncwarp();
+  const int ldab = 3 * N + 1;
+  band_solve_warp(tb.ab + (size_t)s * ldab * n, tb.ipiv + (size_t)s * n, b, nr, n, N, N, lane);
+  if (cpen) {
+    legen_filter_cols(b, nr, n, N, g.ns, tb.wg, tb.alpol, tb.sigma, lane);
+    __syncwarp();
+  }
+  for (int r = 0; r < nr; ++r) {
+    T* F = Fs[r / 2];
+    int part = r & 1;
+    for (int k = lane; k < n; k += 32) {
+      double x = b[(size_t)r * n + k];
+      if (role == 0 && r < 2 && lzero && meanu) x = rmul(tb.meang[k], x);
+      F[fidx<T>(g, 2 * ii + part, j, k)] = (T)x;
+    }
+  }
+}
+
+// ===========================================================================
+// Interface averaging (penalty.f:714-775).
+// ===========================================================================
+// apply the round-trip projection P in place to all planes except the
+// interface planes (km, k of every interface), which go through real
+// transforms instead.  Thread per (j, k, field) for the kx=0 pair and the
+// Nyquist column.
+template <typename T>
+__global__ void k_project_planes(Geo g, T* F0, T* F1, T* F2, T* F3, int skip_iface) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long total = (long)g.ny * g.nz * 4;
+  if (gid >= total) return;
+  int j = gid % g.ny;
+  long r = gid / g.ny;
+  int k = r % g.nz;
+  int q = r / g.nz;
+  if (skip_iface) {
+    int kl = k % g.N;
+    if ((kl == 0 && k > 0) || (kl == g.N - 1 && k < g.nz - 1)) return;
+  }
+  T* F = q == 0 ? F0 : q == 1 ? F1 : q == 2 ? F2 : F3;
+  int jp = (g.ny - j) % g.ny;
+  // Nyquist: independent per j
+  size_t pn = fidx<T>(g, g.nx, j, k);
+  F[pn] = F[pn] * (T)g.scaley;
+  F[pn + 1] = 0;
+  if (j <= jp) {
+    size_t pa = fidx<T>(g, 0, j, k), pb = fidx<T>(g, 0, jp, k);
+    T ar = F[pa], ai = F[pa + 1], br = F[pb], bi = F[pb + 1];
+    T nr = (T)0.5 * (ar + br), ni = (T)0.5 * (ai - bi);
+    F[pa] = nr;
+    F[pa + 1] = ni;
+    if (jp != j) {
+      F[pb] = nr;
+      F[pb + 1] = -ni;
+    }
+  }
+}
+
+// gather the 4 planes around each interface into a compact buffer:
+// G[(q*(ns-1)+f)*4 + m] plane = F_q level (f+1)*N - 2 + m
+template <typename T>
+__global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, const T* F3, T* G, int back) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long per = (long)g.plane;
+  long total = per * 4 * (g.ns - 1) * 4;
+  if (gid >= total) return;
+  long e = gid % per;
+  long pl = gid / per;
+  int m = pl % 4;
+  int f = (pl / 4) % (g.ns - 1);
+  int q = pl / (4 * (g.ns - 1));
+  int k = (f + 1) * g.N - 2 + m;
+  const T* F = q == 0 ? F0 : q == 1 ? F1 : q == 2 ? F2 : F3;
+  if (!back) {
+    G[pl * per + e] = F[(size_t)k * per + e];
+  } else if (m == 1 || m == 2) {
+    ((T*)F)[(size_t)k * per + e] = G[pl * per + e];
+  }
+}
+
+// per (row j, interface plane group): x-inverse of 4 rows, average, x-forward
+// of the 2 interface rows.
+template <typename T>
+__global__ void k_iface_rows(Geo g, T* G, FftPlan pl, const typename cplx_t<T>::type* __restrict__ Wm,
+                             const typename cplx_t<T>::type* __restrict__ Wn, int* counts) {
+  typedef typename cplx_t<T>::type C;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int M = g.nx / 2, nx = g.nx;
+  C* A = (C*)smraw;
+  C* B = A + 4 * M;
+  const int j = blockIdx.x;
+  const int grp = blockIdx.y;  // q*(ns-1)+f
+  const int q = grp / (g.ns - 1);
+  const size_t per = g.plane;
+  for (int m = 0; m < 4; ++m)
+    xinv_prep<C, T>(G + (size_t)(grp * 4 + m) * per + (size_t)j * g.nxpp, A + m * M, M, Wn, 0, (T)0, threadIdx.x,
+                    blockDim.x);
+  __syncthreads();
+  C* ph = fft_run<C>(A, B, pl, 4, Wm, true, threadIdx.x, blockDim.x);
+  T* P = (T*)ph;
+  int cnt = 0;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    T fsp = P[2 * nx + i], fsm = P[1 * nx + i];
+    T favg2 = fsp + fsm;
+    T c0 = fabs(fsp - fsm) / fabs(favg2);
+    if (c0 > (T)0.005) {
+      T ff = P[0 * nx + i] * (T)0.5 + P[1 * nx + i] * (T)0 + P[2 * nx + i] * (T)0 + P[3 * nx + i] * (T)0.5;
+      P[1 * nx + i] = ff;
+      P[2 * nx + i] = ff;
+      ++cnt;
+    }
+  }
+  if (cnt) atomicAdd(counts + q, cnt);
+  __syncthreads();
+  C* other = (ph == A) ? B : A;
+  C* sp = fft_run<C>(ph + M, other + M, pl, 2, Wm, false, threadIdx.x, blockDim.x);
+  const T invN = (T)1 / (T)nx;
+  for (int t = threadIdx.x; t < 2 * (M + 1); t += blockDim.x) {
+    int m = t / (M + 1), kk = t % (M + 1);
+    C v = xfwd_post<C>(sp + m * M, kk, M, Wn, invN);
+    T* p = G + (size_t)(grp * 4 + 1 + m) * per + (size_t)j * g.nxpp + 2 * kk;
+    p[0] = v.x;
+    p[1] = v.y;
+  }
+}
+
+// ===========================================================================
+// generic whole-field helpers for the Fortran-style entry points
+// ===========================================================================
+template <typename T>
+__global__ void k_xfft_field(Geo g, T* F, int nk, int inv, FftPlan pl, const typename cplx_t<T>::type* __restrict__ Wm,
+                             const typename cplx_t<T>::type* __restrict__ Wn) {
+  typedef typename cplx_t<T>::type C;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int M = g.nx / 2, nx = g.nx;
+  C* A = (C*)smraw;
+  C* B = A + M;
+  const int row = blockIdx.x;  // j + ny*k
+  T* rp = F + (size_t)row * g.nxpp;
+  if (inv) {
+    xinv_prep<C, T>(rp, A, M, Wn, 0, (T)0, threadIdx.x, blockDim.x);
+    __syncthreads();
+    C* r = fft_run<C>(A, B, pl, 1, Wm, true, threadIdx.x, blockDim.x);
+    T* P = (T*)r;
+    for (int i = threadIdx.x; i < g.nxpp; i += blockDim.x) rp[i] = i < nx ? P[i] : (T)0;
+  } else {
+    for (int i = threadIdx.x; i < M; i += blockDim.x) A[i] = cmk<C>(rp[2 * i], rp[2 * i + 1]);
+    __syncthreads();
+    C* r = fft_run<C>(A, B, pl, 1, Wm, false, threadIdx.x, blockDim.x);
+    const T invN = (T)1 / (T)nx;
+    for (int t = threadIdx.x; t < M + 1; t += blockDim.x) {
+      C v = xfwd_post<C>(r, t, M, Wn, invN);
+      // write after everyone has read r: r is a different buffer than rp
+      rp[2 * t] = v.x;
+      rp[2 * t + 1] = v.y;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_mulikx(Geo g, T* F) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long)(g.ntot / 2)) return;
+  size_t p = 2 * (size_t)gid;
+  int ii = (int)((p % g.nxpp) / 2);
+  T kx = (T)g.xw[ii];
+  T a = F[p], b = F[p + 1];
+  F[p] = -(kx * b);
+  F[p + 1] = kx * a;
+}
+
+template <typename T>
+__global__ void k_dz_field(Geo g, const T* __restrict__ a, T* __restrict__ b) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long)g.ntot) return;
+  size_t e = gid % g.plane;
+  int k = gid / g.plane;
+  int ks = k / g.N, k1 = k % g.N;
+  double s = 0.0;
+  for (int k2 = 0; k2 < g.N; ++k2) s += g.D[k1 * g.N + k2] * (double)a[(size_t)(ks * g.N + k2) * g.plane + e];
+  b[gid] = (T)(s * g.hfac[ks]);
+}
+
+// filter_3dlegenfourier on a spectral field, in place
+template <typename T>
+__global__ void k_filter_field(Geo g, T* F, int ifourier, int ilegen) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long total = (long)g.nxpp * g.ny * g.ns;
+  if (gid >= total) return;
+  int i = gid % g.nxpp;
+  long r = gid / g.nxpp;
+  int j = r % g.ny;
+  int ks = r / g.ny;
+  const int N = g.N;
+  double v[kMaxN];
+  double cf = ifourier ? g.cfour[(size_t)j * g.nxhp + (i >> 1)] : 1.0;
+  for (int k = 0; k < N; ++k) v[k] = (double)F[fidx<T>(g, i, j, ks * N + k)] * cf;
+  for (int k1 = 0; k1 < N; ++k1) {
+    double s = 0;
+    if (ilegen)
+      for (int k2 = 0; k2 < N; ++k2) s += g.Lfil[k1 * N + k2] * v[k2];
+    else
+      s = v[k1];
+    F[fidx<T>(g, i, j, ks * N + k1)] = (T)s;
+  }
+}
+
+// reductions for diagnostics: physical-space sums over i<nx, k>=1
+template <typename T>
+__global__ void k_reduce_sq(Geo g, const T* __restrict__ a, int kmin, double* out) {
+  double s = 0;
+  long total = (long)g.nx * g.ny * (g.nz - kmin);
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    int i = t % g.nx;
+    long r = t / g.nx;
+    int j = r % g.ny;
+    int k = kmin + r / g.ny;
+    double x = (double)a[fidx<T>(g, i, j, k)];
+    s += x * x;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+template <typename T>
+__global__ void k_nonfinite(const T* __restrict__ a, size_t n, int* flag) {
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite((double)a[t])) {
+      atomicExch(flag, 1);
+      return;
+    }
+}
+
+template <typename T, typename U>
+__global__ void k_convert(const T* __restrict__ a, U* __restrict__ b, size_t n) {
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+    b[t] = (U)a[t];
+}
+
+#include "iw_host.inl"

@@ -1,0 +1,226 @@
+"""Host-side mirror of the reference's time-step interface on the B200 library.
+
+``Solver`` owns one device-resident run (the reference's COMMON blocks) and
+exposes the reference's subroutines with their names and semantics:
+
+=====================  ==========================================  =========================
+method                 reference routine                           device work
+=====================  ==========================================  =========================
+``step``               main.f:653-1066 (maxcalc, convec,           the fused step kernels
+                       calcuvwt, interface_avg3d)
+``convec``             solver.f:6-514                              K_A..K_E
+``calcuvwt``           calcuvwt_noslip.f / calcuvwt.f              pressure + viscous solves
+``horfft``             horfft.f:2-69                               x/y FFT kernels
+``dpdz``               derv.f:212-275                              z-derivative kernel
+``filter_3dlegenfourier``  filtering.f:811-983                     filter kernel
+``interface_avg3d``    penalty.f:714-775                           interface kernels
+``penalty_main``       penalty.f:162-251 (+ band_lu.f)             device assembly, LU, solve
+``bandlu_solve``       band_lu.f:15-54                             device LU and solve
+=====================  ==========================================  =========================
+
+Arrays use the reference layout ``(4 fields, nz, ny, nxpp)`` float64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .config import Config, IwCoefs, IwDiagOut
+
+
+def _pd(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ri(v: int):
+    return C.byref(C.c_int(int(v)))
+
+
+def _rd(v: float):
+    return C.byref(C.c_double(float(v)))
+
+
+class Solver:
+    """One run on one GPU (fields stay on the device between calls)."""
+
+    def __init__(self, cfg: Config, device: int = 0):
+        cfg.validate()
+        self.cfg = cfg
+        self._dims = cfg.c_dims()
+        self._prm = cfg.c_params()
+        h = C.c_void_p()
+        _lib.check(_lib.lib().iw_init(C.byref(self._dims), C.byref(self._prm), device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().iw_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------
+    @property
+    def shape(self):
+        c = self.cfg
+        return (4, c.nz, c.ny, c.nxpp)
+
+    def init_mode1(self, amplitude: float, noise: float, seed: int):
+        _lib.check(_lib.lib().iw_init_mode1(self.h, amplitude, noise, seed))
+
+    def set_state(self, uvwt, uvwt_n=None, uvwt_nm=None, s_n=None, s_nm=None, t=0.0, istep=0):
+        arrs = []
+        for a in (uvwt, uvwt_n, uvwt_nm, s_n, s_nm):
+            arrs.append(None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(self.shape))
+        ptrs = [None if a is None else _pd(a) for a in arrs]
+        _lib.check(_lib.lib().iw_upload_state(self.h, *ptrs, t, istep))
+
+    def state(self, level: int = 0) -> np.ndarray:
+        out = np.zeros(self.shape)
+        ptrs = [None] * 5
+        ptrs[level] = _pd(out)
+        _lib.check(_lib.lib().iw_download_state(self.h, *ptrs))
+        return out
+
+    def step(self, n: int = 1):
+        _lib.check(_lib.lib().iw_run(self.h, n, 0))
+
+    def step_coefs(self, fac, bdf, bdfv, dt):
+        c = IwCoefs(fac[0], fac[1], fac[2], bdf[0], bdf[1], bdf[2], bdfv, dt)
+        _lib.check(_lib.lib().iw_step_coefs(self.h, C.byref(c)))
+
+    def sync(self):
+        _lib.check(_lib.lib().iw_sync(self.h))
+
+    def diag(self) -> dict:
+        d = IwDiagOut()
+        _lib.check(_lib.lib().iw_diag(self.h, C.byref(d)))
+        return dict(ke=d.ke, eps=d.eps, t=d.t, istep=d.istep, avg=list(d.interface_avg_count))
+
+    def mean_profiles(self, out: np.ndarray = None) -> np.ndarray:
+        """(4, nz) mean profiles of u, v, w, rho (device -> host, synchronous)."""
+        if out is None:
+            out = np.zeros(4 * self.cfg.nz)
+        _lib.check(_lib.lib().iw_mean_profiles(self.h, _pd(out)))
+        return out.reshape(4, self.cfg.nz)
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        _lib.check(_lib.lib().iw_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def field_ptr(self, f: int) -> int:
+        p = C.c_void_p()
+        _lib.check(_lib.lib().iw_field_ptr(self.h, f, C.byref(p)))
+        return p.value
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        _lib.check(_lib.lib().iw_stream(self.h, C.byref(p)))
+        return p.value
+
+    def profile(self, enable: bool = True):
+        _lib.check(_lib.lib().iw_profile(self.h, 1 if enable else 0))
+
+    PHASES = ["stageA", "y_inverse", "x_row_nl", "y_forward", "wall_bc", "stageE", "pressure", "solve_uv",
+              "solve_w", "solve_rho", "interface_avg"]
+
+    def profile_read(self) -> dict:
+        ms = (C.c_double * 16)()
+        n = (C.c_long * 16)()
+        _lib.check(_lib.lib().iw_profile_read(self.h, ms, n))
+        return {p: (ms[i], n[i]) for i, p in enumerate(self.PHASES)}
+
+    # ------------------------------------------------------------------
+    # the reference's subroutines (Fortran-style entry points)
+    def _bind(self):
+        _lib.lib().iw_bind(self.h)
+
+    def horfft(self, b: np.ndarray, is_: int, nk: int = None) -> np.ndarray:
+        self._bind()
+        b = np.array(b, dtype=np.float64, order="C")
+        _lib.lib().horfft_(_pd(b), _ri(is_), _ri(nk or self.cfg.nz))
+        return b
+
+    def dpdz(self, a: np.ndarray) -> np.ndarray:
+        self._bind()
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.zeros_like(a)
+        _lib.lib().dpdz_(_pd(a), _pd(b))
+        return b
+
+    def filter_3dlegenfourier(self, f: np.ndarray, ifourier=1, ilegen=1) -> np.ndarray:
+        self._bind()
+        f = np.array(f, dtype=np.float64, order="C")
+        _lib.lib().filter_3dlegenfourier_(_pd(f), _ri(ifourier), _ri(ilegen), _ri(0))
+        return f
+
+    def filter_legenpen(self, fin: np.ndarray) -> np.ndarray:
+        self._bind()
+        fin = np.ascontiguousarray(fin, dtype=np.float64)
+        out = np.zeros_like(fin)
+        _lib.lib().filter_legenpen_(_pd(fin), _pd(out), _rd(1.0), _ri(0), _ri(1))
+        return out
+
+    def interface_avg3d(self, f: np.ndarray):
+        self._bind()
+        f = np.array(f, dtype=np.float64, order="C")
+        ic = C.c_int(0)
+        _lib.lib().interface_avg3d_(_pd(f), C.byref(ic))
+        return f, ic.value
+
+    def penalty_setup(self, eps: float):
+        self._bind()
+        _lib.lib().penalty_setup_(_rd(eps))
+
+    def penalty_main(self, eps, ifbcbot, ifbctop, bcs, rhsr, rhsi):
+        """penalty.f:162-251; rhsr/rhsi are scaled by -eps in place (returned)."""
+        self._bind()
+        rhsr = np.array(rhsr, dtype=np.float64)
+        rhsi = np.array(rhsi, dtype=np.float64)
+        fr, fi = np.zeros_like(rhsr), np.zeros_like(rhsi)
+        L = _lib.lib()
+        L.penalty_main_(_rd(eps), _ri(0), _rd(bcs[0]), _rd(bcs[1]), _rd(bcs[2]), _rd(bcs[3]), _ri(ifbcbot),
+                        _ri(ifbctop), _pd(rhsr), _pd(rhsi), _pd(fr), _pd(fi))
+        return fr, fi, rhsr, rhsi
+
+    def bandlu_solve(self, a_rowmajor: np.ndarray, xr, xi):
+        self._bind()
+        acm = np.ascontiguousarray(np.asarray(a_rowmajor, dtype=np.float64).T)
+        xr = np.array(xr, dtype=np.float64)
+        xi = np.array(xi, dtype=np.float64)
+        _lib.lib().bandlu_solve_(_pd(acm), _pd(xr), _pd(xi), _ri(0))
+        return xr, xi
+
+    def convec(self, istep: int):
+        self._bind()
+        _lib.lib().convec_(_ri(istep), _ri(0), _ri(self.cfg.ispecfilternl))
+
+    def calcuvwt(self, cpenspecfilter: bool = True):
+        self._bind()
+        _lib.lib().calcuvwt_(_ri(0), _ri(0), _ri(0), _ri(1 if cpenspecfilter else 0))
+
+
+def multistep(name: str, dt1: float, dt2: float, dt3: float) -> float:
+    """multistep.f:7-89 through the C ABI (abvar1_ ... bdfvar3_)."""
+    return getattr(_lib.lib(), name + "_")(_rd(dt1), _rd(dt2), _rd(dt3))
+
+
+def helm_solve_batched(solver: Solver, lam_dev_ptr: int, ncol: int, ifbcbot: int, ifbctop: int, rhs_dev_ptr: int,
+                       sol_dev_ptr: int, mode: int = 0):
+    """Batched isolated penalty solves on device buffers (see iw_helm_solve_batched)."""
+    _lib.check(_lib.lib().iw_helm_solve_batched(solver.h, C.c_void_p(lam_dev_ptr), ncol, ifbcbot, ifbctop,
+                                                C.c_void_p(rhs_dev_ptr), C.c_void_p(sol_dev_ptr), mode))

@@ -44,6 +44,7 @@ def lib():
             getattr(L, name).argtypes = [C.c_void_p]
         L.orc_run.argtypes = [C.c_void_p, C.c_int]
         L.orc_set_cache.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_fourier_scale.argtypes = [C.c_void_p, C.c_int]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_tables.argtypes = [C.c_void_p] + [PD] * 7
         L.orc_set_state.argtypes = [C.c_void_p, C.c_int, PD]
@@ -84,7 +85,7 @@ def _p(a: np.ndarray):
 class Oracle:
     """One run of the CPU restatement (state = the reference's COMMON blocks)."""
 
-    def __init__(self, cfg: Config, cache: bool = True):
+    def __init__(self, cfg: Config, cache: bool = True, fourier_scale: bool = False):
         self.cfg = cfg
         self._dims = cfg.c_dims()
         self._prm = cfg.c_params()
@@ -92,6 +93,7 @@ class Oracle:
         if not self.h:
             raise ValueError(lib().orc_last_error().decode())
         lib().orc_set_cache(self.h, 1 if cache else 0)
+        lib().orc_set_fourier_scale(self.h, 1 if fourier_scale else 0)
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -127,6 +127,10 @@ struct Orc {
   int avg_count[4] = {0, 0, 0, 0};
   // oracle-fast factor cache: bit-identical to re-factoring every call
   bool cache_on = true;
+  // Fourier filter as a plain scale instead of magnitude/phase (the two are
+  // equal in exact arithmetic; acos/cos/sin adds noise of about
+  // 1e-16*|fr|^2/|fi| when |fi| << |fr|).  Off = the reference's form.
+  bool fourier_scale = false;
   struct Fac {
     std::vector<double> ab;
     std::vector<int> ipiv;
@@ -483,7 +487,11 @@ void filter_3dlegenfourier(const Orc& o, double* f, int ifourier, int ilegen) {
             double fr = f[o.idx(i, j, k)], fi = f[o.idx(i + 1, j, k)];
             double fmag = std::sqrt(fr * fr + fi * fi);
             double cosc = fr / fmag, sinc = fi / fmag;
-            if (fmag != 0.) {
+            if (o.fourier_scale) {
+              double cf = specfilter_fourier2d(ak, akmax, 0, o.pp.pf, o.pp.amp);
+              fr = fr * cf;
+              fi = fi * cf;
+            } else if (fmag != 0.) {
               double phase = 0.0;
               if (sinc >= 0.) phase = std::acos(cosc);
               if (sinc < 0.) phase = -std::acos(cosc);
@@ -1583,6 +1591,8 @@ int orc_max_threads() {
   return 1;
 #endif
 }
+
+void orc_set_fourier_scale(void* h, int on) { ((Orc*)h)->fourier_scale = on != 0; }
 
 void orc_set_cache(void* h, int on) {
   Orc* o = (Orc*)h;
