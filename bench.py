@@ -249,7 +249,7 @@ def run_ours(args, rank, world):
         st0 = s.state(0)
         pinned = torch.empty(st0.size, dtype=torch.float64, pin_memory=True).numpy().reshape(st0.shape)
         pinned[:] = st0
-        prof_host = torch.empty(4 * cfg.nz * 2, dtype=torch.float64, pin_memory=True).numpy()
+        prof_host = torch.empty(4 * cfg.nz, dtype=torch.float64, pin_memory=True).numpy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         zeros = np.zeros_like(pinned)

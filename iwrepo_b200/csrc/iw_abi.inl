@@ -114,8 +114,8 @@ int factor_dense_or_params(iw_handle* h, const double* pen6, double eps, int bot
   CK(cudaMalloc(&dab, (size_t)ldab * n * sizeof(double)));
   CK(cudaMalloc(&dip, n * sizeof(int)));
   CK(cudaMalloc(&dinfo, sizeof(int)));
-  CK(cudaMemcpy(dsd, &sd, sizeof sd, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dpen, pen6, 6 * ns * sizeof(double), cudaMemcpyHostToDevice));
+  CK(scopy(h, dsd, &sd, sizeof sd, cudaMemcpyHostToDevice));
+  CK(scopy(h, dpen, pen6, 6 * ns * sizeof(double), cudaMemcpyHostToDevice));
   FactorArgs fa;
   fa.sys = dsd;
   fa.pen = dpen;
@@ -133,7 +133,7 @@ int factor_dense_or_params(iw_handle* h, const double* pen6, double eps, int bot
     for (int j = 1; j <= n; ++j)
       for (int i = std::max(1, j - N); i <= std::min(n, j + N); ++i)
         ab[(size_t)(2 * N + i - j) + (size_t)ldab * (j - 1)] = dense[(size_t)(i - 1) + (size_t)n * (j - 1)];
-    CK(cudaMemcpy(dab, ab.data(), ab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(scopy(h, dab, ab.data(), ab.size() * sizeof(double), cudaMemcpyHostToDevice));
     fa.assemble = 0;
   }
   k_factor<<<1, 32, 0, h->st>>>(geo(h), fa);
@@ -186,7 +186,7 @@ void horfft_(double* b, const int* is, const int* nk) {
   if (!h || !b || !is || !nk) return;
   size_t n = h->plane * (size_t)*nk;
   DBuf d(n);
-  cudaMemcpy(d.p, b, n * sizeof(double), cudaMemcpyHostToDevice);
+  scopy(h, d.p, b, n * sizeof(double), cudaMemcpyHostToDevice);
   FieldSet<double> tmp;
   typedef double2 C;
   int M = h->nx / 2;
@@ -196,7 +196,7 @@ void horfft_(double* b, const int* is, const int* nk) {
   if (up(h, &tmp.Wm, wm) || up(h, &tmp.Wn, wn) || up(h, &tmp.Wy, wy)) return;
   horfft_dev<double>(h, tmp, d.p, *is, *nk);
   cudaStreamSynchronize(h->st);
-  cudaMemcpy(b, d.p, n * sizeof(double), cudaMemcpyDeviceToHost);
+  scopy(h, b, d.p, n * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(tmp.Wm);
   cudaFree(tmp.Wn);
   cudaFree(tmp.Wy);
@@ -206,10 +206,10 @@ void dpdz_(const double* a, double* b) {
   iw_handle* h = bound();
   if (!h || !a || !b) return;
   DBuf da(h->ntot), db(h->ntot);
-  cudaMemcpy(da.p, a, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
+  scopy(h, da.p, a, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
   k_dz_field<double><<<(unsigned)((h->ntot + 255) / 256), 256, 0, h->st>>>(geo(h), da.p, db.p);
   cudaStreamSynchronize(h->st);
-  cudaMemcpy(b, db.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
+  scopy(h, b, db.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
 }
 
 void filter_3dlegenfourier_(double* f, const int* ifourier, const int* ilegen, const int* iout) {
@@ -217,12 +217,12 @@ void filter_3dlegenfourier_(double* f, const int* ifourier, const int* ilegen, c
   iw_handle* h = bound();
   if (!h || !f) return;
   DBuf d(h->ntot);
-  cudaMemcpy(d.p, f, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
+  scopy(h, d.p, f, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
   long total = (long)h->nxpp * h->ny * h->ns;
   k_filter_field<double><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(geo(h), d.p, ifourier ? *ifourier : 1,
                                                                             ilegen ? *ilegen : 1);
   cudaStreamSynchronize(h->st);
-  cudaMemcpy(f, d.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
+  scopy(h, f, d.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
 }
 
 void filter_legenpen_(const double* fin, double* fout, const double* ybar, const int* iprt, const int* ks) {
@@ -232,10 +232,10 @@ void filter_legenpen_(const double* fin, double* fout, const double* ybar, const
   iw_handle* h = bound();
   if (!h || !fin || !fout) return;
   DBuf d(h->N);
-  cudaMemcpy(d.p, fin, h->N * sizeof(double), cudaMemcpyHostToDevice);
+  scopy(h, d.p, fin, h->N * sizeof(double), cudaMemcpyHostToDevice);
   k_legen_one<<<1, 32, 0, h->st>>>(geo(h), h->dwg, h->dal, h->dsig, d.p, h->N);
   cudaStreamSynchronize(h->st);
-  cudaMemcpy(fout, d.p, h->N * sizeof(double), cudaMemcpyDeviceToHost);
+  scopy(h, fout, d.p, h->N * sizeof(double), cudaMemcpyDeviceToHost);
 }
 
 void interface_avg3d_(double* f, int* ic) {
@@ -249,15 +249,15 @@ void interface_avg3d_(double* f, int* ic) {
   auto wn = twiddles<C>(h->nx, M + 1);
   auto wy = twiddles<C>(h->ny, h->ny);
   if (up(h, &fs.Wm, wm) || up(h, &fs.Wn, wn) || up(h, &fs.Wy, wy)) return;
-  cudaMemcpy(d.p, f, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
+  scopy(h, d.p, f, h->ntot * sizeof(double), cudaMemcpyHostToDevice);
   for (int q = 0; q < 4; ++q) fs.F[q] = d.p;
   fs.G = G.p;
   iface_avg<double>(h, fs, true, 1);
   cudaStreamSynchronize(h->st);
-  cudaMemcpy(f, d.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
+  scopy(h, f, d.p, h->ntot * sizeof(double), cudaMemcpyDeviceToHost);
   if (ic) {
     int cnt[4];
-    cudaMemcpy(cnt, h->dcnt, sizeof cnt, cudaMemcpyDeviceToHost);
+    scopy(h, cnt, h->dcnt, sizeof cnt, cudaMemcpyDeviceToHost);
     *ic = cnt[0];
   }
   fs.F[0] = fs.F[1] = fs.F[2] = fs.F[3] = nullptr;
@@ -316,10 +316,10 @@ void penalty_main_(const double* epsilon, const int* ifuncreal, const double* bc
   int* dip;
   if (factor_dense_or_params(h, pen.data(), eps, *ifbcbot, *ifbctop, nullptr, &dab, &dip)) return;
   DBuf db(2 * (size_t)n);
-  cudaMemcpy(db.p, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice);
+  scopy(h, db.p, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice);
   k_solve_one<<<1, 32, 2 * n * sizeof(double), h->st>>>(geo(h), dab, dip, db.p, 2);
   cudaStreamSynchronize(h->st);
-  cudaMemcpy(b.data(), db.p, b.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  scopy(h, b.data(), db.p, b.size() * sizeof(double), cudaMemcpyDeviceToHost);
   for (int k = 0; k < n; ++k) {
     fr[k] = b[k];
     fi[k] = b[n + k];
@@ -343,10 +343,10 @@ void bandlu_solve_(const double* ain, double* xr, double* xi, const int* ifuncre
     b[n + k] = xi ? xi[k] : 0.0;
   }
   DBuf db(2 * (size_t)n);
-  cudaMemcpy(db.p, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice);
+  scopy(h, db.p, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice);
   k_solve_one<<<1, 32, 2 * n * sizeof(double), h->st>>>(geo(h), dab, dip, db.p, nr);
   cudaStreamSynchronize(h->st);
-  cudaMemcpy(b.data(), db.p, b.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  scopy(h, b.data(), db.p, b.size() * sizeof(double), cudaMemcpyDeviceToHost);
   for (int k = 0; k < n; ++k) {
     xr[k] = b[k];
     if (xi && nr == 2) xi[k] = b[n + k];
@@ -473,7 +473,7 @@ static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
   out->t = h->t;
   out->istep = h->istep;
   int cnt[4] = {0, 0, 0, 0};
-  CK(cudaMemcpy(cnt, h->dcnt, sizeof cnt, cudaMemcpyDeviceToHost));
+  CK(scopy(h, cnt, h->dcnt, sizeof cnt, cudaMemcpyDeviceToHost));
   for (int q = 0; q < 4; ++q) out->interface_avg_count[q] = cnt[q];
   // non-finite check of the state
   CK(cudaMemsetAsync(h->dflag, 0, sizeof(int), h->st));

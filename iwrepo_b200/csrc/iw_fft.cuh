@@ -57,7 +57,9 @@ struct FftPlan {
   int M;
   int npass;
   int rad[12];
-  int ns[12];  // accumulated size before the pass
+  int ns[12];       // accumulated size before the pass
+  int nbsh[12];     // log2(M/R) if a power of two, else -1
+  int nssh[12];     // log2(ns) if a power of two, else -1
 };
 
 // One Stockham pass over `nb` batched transforms stored contiguously
@@ -65,17 +67,18 @@ struct FftPlan {
 template <typename C>
 __device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restrict__ dst, int M, int R,
                                          int Ns, int nbatch, const C* __restrict__ W, bool inv, int tid,
-                                         int nthr) {
+                                         int nthr, int nbsh, int nssh) {
   const int nb = M / R;
   const int total = nb * nbatch;
   const int step = M / (Ns * R);
   for (int w = tid; w < total; w += nthr) {
-    int b = w / nb;
-    int j = w - b * nb;
+    const int b = nbsh >= 0 ? (w >> nbsh) : (w / nb);
+    const int j = w - b * nb;
     const C* s = src + (size_t)b * M;
     C* d = dst + (size_t)b * M;
     C v[5];
-    int jm = j % Ns;
+    const int jq = nssh >= 0 ? (j >> nssh) : (j / Ns);
+    const int jm = j - jq * Ns;
 #pragma unroll
     for (int r = 0; r < 5; ++r)
       if (r < R) v[r] = s[j + r * nb];
@@ -83,7 +86,7 @@ __device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restric
 #pragma unroll
       for (int r = 1; r < 5; ++r)
         if (r < R) {
-          C tw = W[(r * jm * step) % M];
+          C tw = W[r * jm * step];  // r*jm*step < R*Ns*step = M
           if (inv) tw.y = -tw.y;
           v[r] = cmul(v[r], tw);
         }
@@ -115,7 +118,7 @@ __device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restric
           o[q] = acc;
         }
     }
-    int base = (j / Ns) * Ns * R + jm;
+    const int base = jq * Ns * R + jm;
 #pragma unroll
     for (int r = 0; r < 5; ++r)
       if (r < R) d[base + r * Ns] = o[r];
@@ -129,7 +132,7 @@ __device__ C* fft_run(C* a, C* b, const FftPlan& pl, int nbatch, const C* W, boo
   C* src = a;
   C* dst = b;
   for (int p = 0; p < pl.npass; ++p) {
-    fft_pass<C>(src, dst, pl.M, pl.rad[p], pl.ns[p], nbatch, W, inv, tid, nthr);
+    fft_pass<C>(src, dst, pl.M, pl.rad[p], pl.ns[p], nbatch, W, inv, tid, nthr, pl.nbsh[p], pl.nssh[p]);
     __syncthreads();
     C* t = src;
     src = dst;

@@ -223,9 +223,17 @@ FftPlan make_plan(int M) {
   memset(&p, 0, sizeof p);
   p.M = M;
   int m = M, ns = 1;
+  auto lg2 = [](int v) {
+    if (v <= 0 || (v & (v - 1))) return -1;
+    int l = 0;
+    while ((1 << l) < v) ++l;
+    return l;
+  };
   auto push = [&](int r) {
     p.rad[p.npass] = r;
     p.ns[p.npass] = ns;
+    p.nbsh[p.npass] = lg2(M / r);
+    p.nssh[p.npass] = lg2(ns);
     ns *= r;
     p.npass++;
   };
@@ -303,6 +311,7 @@ struct iw_handle {
   // systems
   std::vector<double> akv;     // distinct kx^2+ky^2 values
   std::vector<int> col_u;      // column -> distinct index
+  int* dcolorder = 0;          // columns sorted by distinct index
   int nsys_kind[SYS_KINDS] = {0, 0, 0, 0};
   double* dab[SYS_KINDS] = {0, 0, 0, 0};
   int* dipiv[SYS_KINDS] = {0, 0, 0, 0};
@@ -356,6 +365,16 @@ static void prof_flush(iw_handle* h) {
 
 static iw_handle* g_bound = nullptr;
 
+// Every host<->device copy goes through the handle's (non-blocking) stream
+// and waits for it: a plain cudaMemcpy from pageable memory may return before
+// its DMA reaches device memory, and work queued on a non-blocking stream is
+// not ordered after it.
+static cudaError_t scopy(iw_handle* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, h->st);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(h->st);
+}
+
 template <typename T>
 static int dalloc(iw_handle* h, T** p, size_t n) {
   cudaError_t e = cudaMalloc((void**)p, n * sizeof(T) + 16);
@@ -367,7 +386,7 @@ template <typename T>
 static int up(iw_handle* h, T** p, const std::vector<T>& v) {
   int r = dalloc(h, p, v.size());
   if (r) return r;
-  CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  CK(scopy(h, *p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -458,6 +477,10 @@ static void build_distinct(iw_handle* h) {
   h->akv = s;
   h->col_u.resize(h->ncol);
   for (int c = 0; c < h->ncol; ++c) h->col_u[c] = (int)(std::lower_bound(s.begin(), s.end(), ak[c]) - s.begin());
+  std::vector<int> order(h->ncol);
+  for (int c = 0; c < h->ncol; ++c) order[c] = c;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h->col_u[a] < h->col_u[b]; });
+  up(h, &h->dcolorder, order);
 }
 
 static int kind_bcs(const iw_handle* h, int kind, int& bot, int& top) {
@@ -550,7 +573,7 @@ static int build_factors(iw_handle* h, int kind) {
     // host copies must stay alive until the copies finish
     CK(cudaStreamSynchronize(h->st));
     std::vector<int> info(nsys);
-    CK(cudaMemcpy(info.data(), h->dinfo[kind], nsys * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(scopy(h, info.data(), h->dinfo[kind], nsys * sizeof(int), cudaMemcpyDeviceToHost));
     for (int s = 0; s < nsys; ++s)
       if (info[s] != 0) return set_err(IW_ERR_PIVOT, "zero pivot in band factorisation");
   } else {
@@ -583,6 +606,7 @@ static SolveTabs solve_tabs(iw_handle* h, int kind) {
   tb.alpol = h->dal;
   tb.sigma = h->dsig;
   tb.meang = h->dmeang;
+  tb.col_order = h->dcolorder;
   return tb;
 }
 
@@ -984,6 +1008,7 @@ int iw_destroy(iw_handle* h) {
     cudaFree(p);
   cudaFree(h->dcnt);
   cudaFree(h->dflag);
+  cudaFree(h->dcolorder);
   for (int k = 0; k < SYS_KINDS; ++k) {
     cudaFree(h->dab[k]);
     cudaFree(h->dipiv[k]);
@@ -1010,12 +1035,12 @@ static int copy_level(iw_handle* h, int level, double* host, bool up_dir) {
       double* tmp = nullptr;
       CK(cudaMalloc(&tmp, n * sizeof(double)));
       if (up_dir) {
-        CK(cudaMemcpy(tmp, host + q * n, n * sizeof(double), cudaMemcpyHostToDevice));
+        CK(scopy(h, tmp, host + q * n, n * sizeof(double), cudaMemcpyHostToDevice));
         k_convert<double, float><<<1024, 256, 0, h->st>>>(tmp, (float*)dp, n);
       } else {
         k_convert<float, double><<<1024, 256, 0, h->st>>>((const float*)dp, tmp, n);
         CK(cudaStreamSynchronize(h->st));
-        CK(cudaMemcpy(host + q * n, tmp, n * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(scopy(h, host + q * n, tmp, n * sizeof(double), cudaMemcpyDeviceToHost));
       }
       CK(cudaStreamSynchronize(h->st));
       cudaFree(tmp);
@@ -1311,7 +1336,7 @@ __global__ void k_helm(Geo g, HelmCache hc, const double* __restrict__ rhs, doub
 static int helm_batched(iw_handle* h, const double* lam_dev, int ncol, int bot, int top, const double* rhs,
                         double* sol, int mode) {
   std::vector<double> lam(ncol);
-  CK(cudaMemcpy(lam.data(), lam_dev, ncol * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(scopy(h, lam.data(), lam_dev, ncol * sizeof(double), cudaMemcpyDeviceToHost));
   // key: the lambda set and BCs
   uint64_t hs = 1469598103934665603ULL;
   for (double v : lam) {

@@ -751,62 +751,121 @@ __global__ void k_factor(Geo g, FactorArgs fa) {
 // ===========================================================================
 __device__ void band_solve_warp(const double* __restrict__ ab, const int* __restrict__ ipiv, double* b, int nr,
                                 int n, int kl, int ku, int lane) {
+  // The factor entries a step needs do not depend on the data, so they are
+  // fetched PF steps ahead into a register ring (indices are compile-time
+  // constants after unrolling), hiding the global-memory latency that would
+  // otherwise stall every step of the sequential sweep.
+  constexpr int PF = 8;
   const int ldab = 2 * kl + ku + 1;
   const int kd = ku + kl + 1;
-  for (int j = 1; j <= n - 1; ++j) {
-    const int lm = min(kl, n - j);
-    const int l = __ldg(ipiv + j - 1);
-    const double* col = ab + (size_t)ldab * (j - 1);
-    for (int r = 0; r < nr; ++r) {
-      double* br = b + (size_t)r * n;
-      const double bj = br[j - 1];
-      const double bl = br[l - 1];
-      const double y = (l != j) ? bl : bj;
-      double nv0 = 0, nv1 = 0;
-      const int i0 = lane + 1, i1 = lane + 33;
-      if (i0 <= lm) {
-        int row = j + i0;
-        double old = (row == l) ? bj : br[row - 1];
-        nv0 = (y != 0.0) ? radd(old, rmul(__ldg(col + kd + i0 - 1), -y)) : old;
-      }
-      if (i1 <= lm) {
-        int row = j + i1;
-        double old = (row == l) ? bj : br[row - 1];
-        nv1 = (y != 0.0) ? radd(old, rmul(__ldg(col + kd + i1 - 1), -y)) : old;
-      }
-      __syncwarp();
-      if (i0 <= lm) br[j + i0 - 1] = nv0;
-      if (i1 <= lm) br[j + i1 - 1] = nv1;
-      if (lane == 0) br[j - 1] = y;
-      __syncwarp();
+  const int i0 = lane + 1, i1 = lane + 33;
+  int rl[PF];
+  double rm0[PF], rm1[PF];
+#pragma unroll
+  for (int d = 0; d < PF; ++d) {
+    const int j = 1 + d;
+    rl[d] = 0;
+    rm0[d] = rm1[d] = 0.0;
+    if (j <= n - 1) {
+      const int lm = min(kl, n - j);
+      const double* col = ab + (size_t)ldab * (j - 1);
+      rl[d] = __ldg(ipiv + j - 1);
+      if (i0 <= lm) rm0[d] = __ldg(col + kd + i0 - 1);
+      if (i1 <= lm) rm1[d] = __ldg(col + kd + i1 - 1);
     }
   }
+  for (int jb = 1; jb <= n - 1; jb += PF) {
+#pragma unroll
+    for (int d = 0; d < PF; ++d) {
+      const int j = jb + d;
+      if (j <= n - 1) {
+        const int lm = min(kl, n - j);
+        const int l = rl[d];
+        const double m0 = rm0[d], m1 = rm1[d];
+        const int jn = j + PF;
+        if (jn <= n - 1) {
+          const int lmn = min(kl, n - jn);
+          const double* coln = ab + (size_t)ldab * (jn - 1);
+          rl[d] = __ldg(ipiv + jn - 1);
+          rm0[d] = (i0 <= lmn) ? __ldg(coln + kd + i0 - 1) : 0.0;
+          rm1[d] = (i1 <= lmn) ? __ldg(coln + kd + i1 - 1) : 0.0;
+        }
+        for (int r = 0; r < nr; ++r) {
+          double* br = b + (size_t)r * n;
+          const double bj = br[j - 1];
+          const double bl = br[l - 1];
+          const double y = (l != j) ? bl : bj;
+          double nv0 = 0, nv1 = 0;
+          if (i0 <= lm) {
+            int row = j + i0;
+            double old = (row == l) ? bj : br[row - 1];
+            nv0 = (y != 0.0) ? radd(old, rmul(m0, -y)) : old;
+          }
+          if (i1 <= lm) {
+            int row = j + i1;
+            double old = (row == l) ? bj : br[row - 1];
+            nv1 = (y != 0.0) ? radd(old, rmul(m1, -y)) : old;
+          }
+          __syncwarp();
+          if (i0 <= lm) br[j + i0 - 1] = nv0;
+          if (i1 <= lm) br[j + i1 - 1] = nv1;
+          if (lane == 0) br[j - 1] = y;
+          __syncwarp();
+        }
+      }
+    }
+  }
+  // back substitution with the upper band (STBSV)
   const int k = kl + ku, kplus1 = k + 1;
-  for (int j = n; j >= 1; --j) {
-    const double* col = ab + (size_t)ldab * (j - 1);
-    const double dg = __ldg(col + kplus1 - 1);
-    const int lo = max(1, j - k);
-    for (int r = 0; r < nr; ++r) {
-      double* br = b + (size_t)r * n;
-      double xj = br[j - 1];
-      if (xj != 0.0) {
-        xj = __ddiv_rn(xj, dg);
-        const int l = kplus1 - j;
-        double nv[3];
+  double rdg[PF], rv0[PF], rv1[PF], rv2[PF];
+  // lane's rows below j are i = j-1-lane-32m; AB(kplus1-j+i, j) = col[k-1-lane-32m]
+  const int o0 = k - 1 - lane, o1 = k - 1 - lane - 32, o2 = k - 1 - lane - 64;
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          int i = j - 1 - lane - 32 * m;
-          nv[m] = 0;
-          if (i >= lo) nv[m] = rsub(br[i - 1], rmul(xj, __ldg(col + l + i - 1)));
-        }
-        __syncwarp();
+  for (int d = 0; d < PF; ++d) {
+    const int j = n - d;
+    rdg[d] = rv0[d] = rv1[d] = rv2[d] = 0.0;
+    if (j >= 1) {
+      const double* col = ab + (size_t)ldab * (j - 1);
+      rdg[d] = __ldg(col + kplus1 - 1);
+      if (o0 >= 0) rv0[d] = __ldg(col + o0);
+      if (o1 >= 0) rv1[d] = __ldg(col + o1);
+      if (o2 >= 0) rv2[d] = __ldg(col + o2);
+    }
+  }
+  for (int jb = n; jb >= 1; jb -= PF) {
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          int i = j - 1 - lane - 32 * m;
-          if (i >= lo) br[i - 1] = nv[m];
+    for (int d = 0; d < PF; ++d) {
+      const int j = jb - d;
+      if (j >= 1) {
+        const double dg = rdg[d];
+        const double v0 = rv0[d], v1 = rv1[d], v2 = rv2[d];
+        const int jn = j - PF;
+        if (jn >= 1) {
+          const double* coln = ab + (size_t)ldab * (jn - 1);
+          rdg[d] = __ldg(coln + kplus1 - 1);
+          rv0[d] = (o0 >= 0) ? __ldg(coln + o0) : 0.0;
+          rv1[d] = (o1 >= 0) ? __ldg(coln + o1) : 0.0;
+          rv2[d] = (o2 >= 0) ? __ldg(coln + o2) : 0.0;
         }
-        if (lane == 0) br[j - 1] = xj;
-        __syncwarp();
+        const int lo = max(1, j - k);
+        const int ia = j - 1 - lane, ib = ia - 32, ic = ia - 64;
+        for (int r = 0; r < nr; ++r) {
+          double* br = b + (size_t)r * n;
+          double xj = br[j - 1];
+          if (xj != 0.0) {
+            xj = __ddiv_rn(xj, dg);
+            double n0 = 0, n1 = 0, n2 = 0;
+            if (ia >= lo) n0 = rsub(br[ia - 1], rmul(xj, v0));
+            if (ib >= lo) n1 = rsub(br[ib - 1], rmul(xj, v1));
+            if (ic >= lo) n2 = rsub(br[ic - 1], rmul(xj, v2));
+            __syncwarp();
+            if (ia >= lo) br[ia - 1] = n0;
+            if (ib >= lo) br[ib - 1] = n1;
+            if (ic >= lo) br[ic - 1] = n2;
+            if (lane == 0) br[j - 1] = xj;
+            __syncwarp();
+          }
+        }
       }
     }
   }
@@ -843,6 +902,7 @@ struct SolveTabs {
   const double* alpol;   // N*N: alpol[k*N + k1] = P_k(z_k1)
   const double* sigma;   // N
   const double* meang;   // nz: 1 - fzgaus(z) (mean-u damping) or null
+  const int* col_order;  // columns sorted by kx^2+ky^2, so neighbouring warps share a factor
 };
 
 // K_F: pressure.  Warp per (ii,j) column.  Reads filtered u*,v*,w* (state F),
@@ -853,9 +913,10 @@ __global__ void k_press(Geo g, SolveTabs tb, T* __restrict__ U, T* __restrict__ 
   extern __shared__ __align__(16) double sm[];
   const int warps = blockDim.x / 32;
   const int wid = threadIdx.x / 32, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * warps + wid;
+  const int cw = blockIdx.x * warps + wid;
   const int ncol = g.nxhp * g.ny;
-  if (c >= ncol) return;
+  if (cw >= ncol) return;
+  const int c = tb.col_order[cw];
   const int n = g.nz, N = g.N;
   double* buf = sm + (size_t)wid * 4 * n;  // [0,2n): w* re/im, [2n,4n): rhs/phi re/im
   const int j = c / g.nxhp, ii = c % g.nxhp;
@@ -963,9 +1024,10 @@ __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ 
   extern __shared__ __align__(16) double sm[];
   const int warps = blockDim.x / 32;
   const int wid = threadIdx.x / 32, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * warps + wid;
+  const int cw = blockIdx.x * warps + wid;
   const int ncol = g.nxhp * g.ny;
-  if (c >= ncol) return;
+  if (cw >= ncol) return;
+  const int c = tb.col_order[cw];
   const int n = g.nz, N = g.N;
   const int nr = role == 0 ? 4 : 2;
   double* b = sm + (size_t)wid * 4 * n;
