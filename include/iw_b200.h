@@ -60,6 +60,13 @@ extern "C" {
 #define IW_PREC_FP64 0  /* everything FP64 (parity path)                         */
 #define IW_PREC_MIXED 1 /* FP32 fields/FFTs/products/filters, FP64 solves        */
 
+/* vertical solves: AUTO = banded LU (the reference's SGBTRF/SGBTRS arithmetic)
+ * for the pressure, subdomain block inverses + interface system for the
+ * viscous and diffusive systems (FP32 inverses + one FP64 residual sweep in
+ * the mixed path); LU = the reference's banded LU for every system. */
+#define IW_SOLVE_AUTO 0
+#define IW_SOLVE_LU 1
+
 /* dim.h PARAMETERs, made runtime values (dim.h:12-28). */
 typedef struct iw_dims {
   int32_t nx;    /* points in x (even; radices 2,3,5)            */
@@ -93,6 +100,8 @@ typedef struct iw_params {
   int32_t meanu_damping; /* (1,1)-mode u *= 1-fzgaus (calcuvwt.f:343) */
   int32_t forcing;       /* virtual paddle in rhsfm (solver.f:942)   */
   int32_t precision;     /* IW_PREC_*                                */
+  int32_t solver;        /* IW_SOLVE_AUTO or IW_SOLVE_LU             */
+  int32_t pad_;
   /* subd.dat */
   double z0[IW_MAX_SUBD];
   double zh[IW_MAX_SUBD];

@@ -26,6 +26,8 @@ IW_BC_FREESLIP = 0
 IW_BC_NOSLIP = 1
 IW_PREC_FP64 = 0
 IW_PREC_MIXED = 1
+IW_SOLVE_AUTO = 0
+IW_SOLVE_LU = 1
 
 
 class ConfigError(ValueError):
@@ -49,7 +51,7 @@ class IwParams(C.Structure):
         ("ispecfilternl", C.c_int32), ("ispecfilterexp", C.c_int32),
         ("nspecfilterexp", C.c_int32), ("navgintrfc", C.c_int32),
         ("bc_variant", C.c_int32), ("meanu_damping", C.c_int32), ("forcing", C.c_int32),
-        ("precision", C.c_int32),
+        ("precision", C.c_int32), ("solver", C.c_int32), ("pad_", C.c_int32),
         ("z0", C.c_double * IW_MAX_SUBD), ("zh", C.c_double * IW_MAX_SUBD),
     ]
 
@@ -113,6 +115,8 @@ class Config:
     meanu_damping: int = 1
     forcing: int = 0
     precision: int = IW_PREC_FP64
+    solver: int = IW_SOLVE_AUTO
+    pad_: int = 0
     z0: Optional[List[float]] = None
     zh: Optional[List[float]] = None
     name: str = "custom"

@@ -300,6 +300,7 @@ struct iw_handle {
   bool mixed = false;
   Tables tab;
   // device tables
+  double *dDt = 0, *dD2t = 0;  // transposed D, D2 (t[k*N + k1] = D[k1][k])
   double *dD = 0, *dD2 = 0, *dL = 0, *dh = 0, *dxw = 0, *dyw = 0, *dcf = 0, *dzg = 0, *dzh = 0;
   double *dwg = 0, *dal = 0, *dsig = 0, *dmeang = 0;
   double *dwnl = 0, *dwvr = 0, *dred = 0;
@@ -319,6 +320,21 @@ struct iw_handle {
   SysDesc* dsys[SYS_KINDS] = {0, 0, 0, 0};
   double* dpen[SYS_KINDS] = {0, 0, 0, 0};
   int* dcolsys[SYS_KINDS] = {0, 0, 0, 0};
+  // block inverses of the viscous / diffusive systems
+  struct BI {
+    void* ainv = 0;
+    double *cvec = 0, *dvec = 0, *minv = 0, *pen = 0, *lvec = 0;
+    SysDesc* sys = 0;
+    int* colsys = 0;
+    int nsys = 0;
+  } bi[SYS_KINDS];
+  bool use_bi = true;
+  // grouped solve tasks per kind (columns sharing a system, <= G per task)
+  Task* dtasks[SYS_KINDS] = {0, 0, 0, 0};
+  int ntask[SYS_KINDS] = {0, 0, 0, 0};
+  double bi_bdfv[SYS_KINDS] = {-1, -1, -1, -1};
+  bool bi_f32[SYS_KINDS] = {false, false, false, false};
+  double bi_dt[SYS_KINDS] = {-1, -1, -1, -1};
   double fac_bdfv[SYS_KINDS] = {-1, -1, -1, -1};  // bdfv the factors were built for
   double fac_dt[SYS_KINDS] = {-1, -1, -1, -1};
   // time stepping
@@ -497,6 +513,28 @@ static int kind_bcs(const iw_handle* h, int kind, int& bot, int& top) {
   return 0;
 }
 
+// tasks: runs of the sorted column order that share one system, split into
+// pieces of at most G columns
+static int build_tasks(iw_handle* h, int kind, const std::vector<int>& colsys, int G) {
+  std::vector<int> order(h->ncol);
+  for (int c = 0; c < h->ncol; ++c) order[c] = c;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h->col_u[a] < h->col_u[b]; });
+  std::vector<Task> tasks;
+  int i = 0;
+  while (i < h->ncol) {
+    const int s = colsys[order[i]];
+    int jn = i;
+    while (jn < h->ncol && colsys[order[jn]] == s && jn - i < (s < 0 ? 1 : G)) ++jn;
+    tasks.push_back(Task{s, i, jn - i});
+    i = jn;
+  }
+  cudaFree(h->dtasks[kind]);
+  h->dtasks[kind] = nullptr;
+  if (up(h, &h->dtasks[kind], tasks)) return IW_ERR_NOMEM;
+  h->ntask[kind] = (int)tasks.size();
+  return 0;
+}
+
 // (re)build the factors of one kind for the current bdfv/dt
 static int build_factors(iw_handle* h, int kind) {
   const int ns = h->ns, N = h->N, n = h->nz, ldab = 3 * N + 1;
@@ -534,6 +572,7 @@ static int build_factors(iw_handle* h, int kind) {
   std::vector<int> colsys(h->ncol);
   for (int c = 0; c < h->ncol; ++c) colsys[c] = dmap[h->col_u[c]];
   const int nsys = (int)sys.size();
+  if (build_tasks(h, kind, colsys, 2)) return IW_ERR_NOMEM;
   if (h->nsys_kind[kind] != nsys) {
     cudaFree(h->dab[kind]);
     cudaFree(h->dipiv[kind]);
@@ -584,8 +623,141 @@ static int build_factors(iw_handle* h, int kind) {
   return 0;
 }
 
+// distinct systems of one kind for the current coefficients
+static void enumerate_systems(iw_handle* h, int kind, std::vector<SysDesc>& sys, std::vector<double>& pen,
+                              std::vector<int>& colsys) {
+  const int ns = h->ns, N = h->N;
+  const int nd = (int)h->akv.size();
+  int bot, top;
+  kind_bcs(h, kind, bot, top);
+  std::vector<int> dmap(nd, -1);
+  sys.clear();
+  pen.clear();
+  const double facvel = 1. / (h->p.xnu * h->p.dt), fact = 1. / (h->p.xkappa * h->p.dt);
+  for (int u = 0; u < nd; ++u) {
+    double ak = h->akv[u];
+    if ((kind == SYS_P || kind == SYS_W) && ak == 0.0) continue;
+    double eps = kind == SYS_P ? 1. / ak : kind == SYS_T ? 1. / (ak + h->c.bdfv * fact) : 1. / (ak + h->c.bdfv * facvel);
+    SysDesc sd;
+    memset(&sd, 0, sizeof sd);
+    sd.eps = eps;
+    sd.ifbcbot = bot;
+    sd.ifbctop = top;
+    std::vector<double> pp(6 * ns);
+    h_penalty(ns, N, h->p, eps, bot, top, pp.data());
+    sd.tau1_bot = pp[4 * ns + 0];
+    sd.tau2_top = pp[5 * ns + ns - 1];
+    dmap[u] = (int)sys.size();
+    sys.push_back(sd);
+    pen.insert(pen.end(), pp.begin(), pp.end());
+  }
+  colsys.resize(h->ncol);
+  for (int c = 0; c < h->ncol; ++c) colsys[c] = dmap[h->col_u[c]];
+}
+
+// block inverses (FP32 for the mixed path, FP64 otherwise) of one kind
+static int build_blockinv(iw_handle* h, int kind) {
+  const int ns = h->ns, N = h->N, n = h->nz, ldab = 3 * N + 1, m = 2 * (ns - 1);
+  const bool f32 = false;  // the solves run in FP64 in both precisions
+  const size_t tib = f32 ? sizeof(float) : sizeof(double);
+  std::vector<SysDesc> sys;
+  std::vector<double> pen;
+  std::vector<int> colsys;
+  enumerate_systems(h, kind, sys, pen, colsys);
+  const int nsys = (int)sys.size();
+  iw_handle::BI& B = h->bi[kind];
+  if (B.nsys != nsys) {
+    cudaFree(B.ainv);
+    cudaFree(B.cvec);
+    cudaFree(B.dvec);
+    cudaFree(B.minv);
+    cudaFree(B.pen);
+    cudaFree(B.lvec);
+    cudaFree(B.sys);
+    cudaFree(B.colsys);
+    B = iw_handle::BI();
+    char* ai = nullptr;
+    if (dalloc(h, &ai, (size_t)std::max(nsys, 1) * ns * N * N * tib) ||
+        dalloc(h, &B.cvec, (size_t)std::max(nsys, 1) * ns * N) || dalloc(h, &B.dvec, (size_t)std::max(nsys, 1) * ns * N) ||
+        dalloc(h, &B.minv, (size_t)std::max(nsys, 1) * std::max(m * m, 1)) ||
+        dalloc(h, &B.pen, (size_t)std::max(nsys, 1) * 6 * ns) || dalloc(h, &B.sys, (size_t)std::max(nsys, 1)) ||
+        dalloc(h, &B.lvec, (size_t)std::max(nsys, 1) * std::max(m, 1) * N) ||
+        dalloc(h, &B.colsys, (size_t)h->ncol))
+      return IW_ERR_NOMEM;
+    B.ainv = ai;
+    B.nsys = nsys;
+  }
+  if (nsys > 0) {
+    CK(scopy(h, B.sys, sys.data(), nsys * sizeof(SysDesc), cudaMemcpyHostToDevice));
+    CK(scopy(h, B.pen, pen.data(), pen.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  CK(scopy(h, B.colsys, colsys.data(), colsys.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (build_tasks(h, kind, colsys, kind == SYS_U ? 1 : 2)) return IW_ERR_NOMEM;
+  h->bi_f32[kind] = f32;
+  // chunked: assemble -> invert blocks -> interface matrix -> store
+  const int CH = std::max(1, std::min(nsys, (int)(1200000000ull / ((size_t)ldab * n * 8 + (size_t)ns * N * N * 8 + 1))));
+  double *tab = nullptr, *tinv = nullptr, *twork = nullptr;
+  int* tinfo = nullptr;
+  CK(cudaMalloc(&tab, (size_t)CH * ldab * n * sizeof(double)));
+  CK(cudaMalloc(&tinv, (size_t)CH * ns * N * N * sizeof(double)));
+  CK(cudaMalloc(&twork, (size_t)CH * 2 * std::max(m * m, 1) * sizeof(double)));
+  CK(cudaMalloc(&tinfo, (size_t)CH * sizeof(int)));
+  Geo g = geo(h);
+  for (int s0 = 0; s0 < nsys; s0 += CH) {
+    const int cn = std::min(CH, nsys - s0);
+    FactorArgs fa;
+    memset(&fa, 0, sizeof fa);
+    fa.sys = B.sys + s0;
+    fa.pen = B.pen + (size_t)s0 * 6 * ns;
+    fa.ab = tab;
+    fa.ipiv = nullptr;
+    fa.info = tinfo;
+    fa.nsys = cn;
+    fa.D = h->dD;
+    fa.D2 = h->dD2;
+    fa.zh = h->dzh;
+    fa.assemble = 1;
+    fa.factor = 0;
+    k_factor<<<(cn + 3) / 4, 128, 0, h->st>>>(g, fa);
+    const int wpb = 2;
+    size_t sm = (size_t)wpb * N * 2 * N * sizeof(double);
+    cudaFuncSetAttribute(k_block_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_block_invert<<<(cn * ns + wpb - 1) / wpb, 32 * wpb, sm, h->st>>>(g, tab, cn, tinv, B.cvec + (size_t)s0 * ns * N,
+                                                                      B.dvec + (size_t)s0 * ns * N);
+    if (m > 0)
+      k_iface_matrix<<<(cn + 63) / 64, 64, 0, h->st>>>(g, cn, tinv, B.cvec + (size_t)s0 * ns * N,
+                                                       B.dvec + (size_t)s0 * ns * N, B.minv + (size_t)s0 * m * m, twork);
+    if (m > 0)
+      k_left_vecs<<<1184, 256, 0, h->st>>>(g, cn, tinv, B.cvec + (size_t)s0 * ns * N, B.dvec + (size_t)s0 * ns * N,
+                                         B.lvec + (size_t)s0 * m * N);
+    const size_t cnt = (size_t)cn * ns * N * N;
+    if (f32)
+      k_convert<double, float><<<2048, 256, 0, h->st>>>(tinv, (float*)B.ainv + (size_t)s0 * ns * N * N, cnt);
+    else
+      CK(cudaMemcpyAsync((double*)B.ainv + (size_t)s0 * ns * N * N, tinv, cnt * sizeof(double),
+                         cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(h->st));
+  cudaFree(tab);
+  cudaFree(tinv);
+  cudaFree(twork);
+  cudaFree(tinfo);
+  h->bi_bdfv[kind] = h->c.bdfv;
+  h->bi_dt[kind] = h->p.dt;
+  return 0;
+}
+
 static int ensure_factors(iw_handle* h) {
+  if (h->use_bi) {
+    for (int k = SYS_P; k <= SYS_T; ++k)
+      if (h->bi_dt[k] != h->p.dt || (k != SYS_P && h->bi_bdfv[k] != h->c.bdfv) || h->bi_dt[k] < 0) {
+        int r = build_blockinv(h, k);
+        if (r) return r;
+      }
+  }
   for (int k = 0; k < SYS_KINDS; ++k) {
+    if (h->use_bi) continue;
     bool need = h->fac_dt[k] != h->p.dt || (k != SYS_P && h->fac_bdfv[k] != h->c.bdfv);
     if (h->fac_dt[k] < 0) need = true;
     if (need) {
@@ -613,14 +785,14 @@ static SolveTabs solve_tabs(iw_handle* h, int kind) {
 // ---------------------------------------------------------------------------
 // the step
 // ---------------------------------------------------------------------------
-template <typename T, int NM>
+template <typename T>
 static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
-  long total = (long)h->nxpp * h->ny * h->ns;
-  dim3 grid((unsigned)((total + 127) / 128), 1, 4);
-  k_stageA<T, NM><<<grid, 128, 0, h->st>>>(geo(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.F1[0], fs.F1[1], fs.F1[2],
-                                           fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj);
+  dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
+  size_t smem = (size_t)(h->N * h->N + h->N * kTX) * sizeof(T);
+  k_stageA<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.F1[0], fs.F1[1],
+                                                fs.F1[2], fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj);
 }
-template <typename T, int NM>
+template <typename T>
 static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   EArgs<T> a;
   for (int q = 0; q < 4; ++q) {
@@ -635,9 +807,9 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   }
   a.wnl = h->dwnl;
   a.filter = h->p.ispecfilternl == 1;
-  long total = (long)h->nxpp * h->ny * h->ns;
-  dim3 grid((unsigned)((total + 127) / 128), 1, 4);
-  k_stageE<T, NM><<<grid, 128, 0, h->st>>>(geo(h), a, h->c);
+  dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
+  size_t smem = (size_t)(2 * h->N * h->N + 2 * h->N * kTX) * sizeof(T);
+  k_stageE<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c);
 }
 
 template <typename T>
@@ -697,7 +869,7 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
   const int M = h->nx / 2;
   mark(h, -1);
   // K_A
-  DISPATCH_N(h, launch_stageA, h, fs, proj);
+  launch_stageA<T>(h, fs, proj);
   mark(h, 0);
   // K_B: y-inverse of 12 arrays
   {
@@ -774,7 +946,7 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
   }
   mark(h, 4);
   // K_E
-  DISPATCH_N(h, launch_stageE, h, fs);
+  launch_stageE<T>(h, fs);
   mark(h, 5);
   for (int q = 0; q < 4; ++q) {
     std::swap(fs.Sn[q], fs.Snm[q]);  // Snm buffer now holds S (level n) -> becomes Sn
@@ -802,6 +974,43 @@ static void schedule_after_convec(iw_handle* h) {
   }
 }
 
+template <typename T>
+static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, int kstart) {
+  constexpr int R = 4;
+  const int kind = role == 0 ? SYS_U : role == 1 ? SYS_W : role == 2 ? SYS_T : SYS_P;
+  const int refine = kind == SYS_P ? 1 : 0;  // the pressure can be ill conditioned (eps = 1/k^2)
+  BlockInv bi;
+  bi.ainv = h->bi[kind].ainv;
+  bi.cvec = h->bi[kind].cvec;
+  bi.dvec = h->bi[kind].dvec;
+  bi.minv = h->bi[kind].minv;
+  bi.pen = h->bi[kind].pen;
+  bi.sys = h->bi[kind].sys;
+  bi.col_sys = h->bi[kind].colsys;
+  bi.col_order = h->dcolorder;
+  bi.lvec = h->bi[kind].lvec;
+  const int mm = std::max(2 * (h->ns - 1), 1);
+  const size_t sm = ((size_t)2 * R * h->nz + 2 * R * mm) * sizeof(double);
+  T *F0, *F1 = nullptr, *F2 = nullptr;
+  if (role == 3) {
+    F0 = fs.F[0];
+    F1 = fs.F[1];
+    F2 = fs.F[2];
+  } else if (role == 0) {
+    F0 = fs.F[0];
+    F1 = fs.F[1];
+  } else {
+    F0 = role == 1 ? fs.F[2] : fs.F[3];
+  }
+  const double rd = role == 2 ? h->p.dt * h->p.xkappa : h->p.xnu * h->p.dt;
+  const int meanu = role == 0 ? h->p.meanu_damping : 0;
+  if (sm > 48 * 1024) cudaFuncSetAttribute(k_solve_cta<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (h->ntask[kind] > 0)
+    k_solve_cta<T, R><<<h->ntask[kind], kSolveThreads, sm, h->st>>>(
+        geo(h), bi, solve_tabs(h, kind), h->dtasks[kind], F0, F1, F2, rd, role, cpen, meanu, refine, h->dDt, h->dD2t,
+        h->dzh, h->dwnl, h->dwvr, kstart);
+}
+
 // calcuvwt (calcuvwt_noslip.f / calcuvwt.f) on u*,v*,w*,rho* held in F.
 template <typename T>
 static int calcuvwt_impl(iw_handle* h, FieldSet<T>& fs, int cpen) {
@@ -812,17 +1021,35 @@ static int calcuvwt_impl(iw_handle* h, FieldSet<T>& fs, int cpen) {
   const int kstart = h->p.bc_variant == IW_BC_NOSLIP ? 1 : 0;
   cudaFuncSetAttribute(k_press<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_visc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_press<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_P), fs.F[0], fs.F[1], fs.F[2], h->dwnl, h->dwvr,
-                                                 cpen, kstart);
+  if (h->use_bi) {
+    launch_solve_bi<T>(h, fs, 3, cpen, kstart);
+  } else {
+  {
+    constexpr int G = 2;
+    const int wpb = 4;
+    const size_t smp = (size_t)wpb * 2 * G * h->nz * sizeof(double);
+    cudaFuncSetAttribute(k_press_g<T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
+    k_press_g<T, G><<<(h->ntask[SYS_P] + wpb - 1) / wpb, 32 * wpb, smp, h->st>>>(
+        g, solve_tabs(h, SYS_P), h->dtasks[SYS_P], h->ntask[SYS_P], fs.F[0], fs.F[1], fs.F[2], h->dwnl, h->dwvr, cpen,
+        kstart);
+  }
+  }
   mark(h, 6);
   const double xnudt = h->p.xnu * h->p.dt, dtk = h->p.dt * h->p.xkappa;
-  k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_U), fs.F[0], fs.F[1], xnudt, 0, cpen,
-                                                h->p.meanu_damping);
-  mark(h, 7);
-  k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_W), fs.F[2], fs.F[2], xnudt, 1, cpen, 0);
-  mark(h, 8);
-  k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_T), fs.F[3], fs.F[3], dtk, 2, cpen, 0);
-  mark(h, 9);
+  if (h->use_bi) {
+    for (int role = 0; role < 3; ++role) {
+      launch_solve_bi<T>(h, fs, role, cpen, kstart);
+      mark(h, 7 + role);
+    }
+  } else {
+    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_U), fs.F[0], fs.F[1], xnudt, 0, cpen,
+                                                  h->p.meanu_damping);
+    mark(h, 7);
+    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_W), fs.F[2], fs.F[2], xnudt, 1, cpen, 0);
+    mark(h, 8);
+    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_T), fs.F[3], fs.F[3], dtk, 2, cpen, 0);
+    mark(h, 9);
+  }
   return 0;
 }
 
@@ -938,6 +1165,7 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
   h->ntot = h->plane * h->nz;
   h->ncol = h->nxhp * h->ny;
   h->mixed = prm->precision == IW_PREC_MIXED;
+  h->use_bi = prm->solver == 0 && d.nsubd <= 16;
   h->plx = make_plan(h->nx / 2);
   h->ply = make_plan(h->ny);
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -974,7 +1202,14 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
         cf[(size_t)j * h->nxhp + ii] = std::exp(-prm->amp * std::pow(theta, 2. * prm->pf));
       }
   }
+  std::vector<double> Dt(h->N * h->N), D2t(h->N * h->N);
+  for (int k1 = 0; k1 < h->N; ++k1)
+    for (int k = 0; k < h->N; ++k) {
+      Dt[(size_t)k * h->N + k1] = h->tab.D[(size_t)k1 * h->N + k];
+      D2t[(size_t)k * h->N + k1] = h->tab.D2[(size_t)k1 * h->N + k];
+    }
   int r = 0;
+  r |= up(h, &h->dDt, Dt) || up(h, &h->dD2t, D2t);
   r |= up(h, &h->dD, h->tab.D) || up(h, &h->dD2, h->tab.D2) || up(h, &h->dL, h->tab.Lfil) || up(h, &h->dh, hf) ||
        up(h, &h->dxw, xw) || up(h, &h->dyw, yw) || up(h, &h->dcf, cf) || up(h, &h->dzg, zg) || up(h, &h->dzh, zh) ||
        up(h, &h->dwg, h->tab.wg) || up(h, &h->dal, h->tab.alpol) || up(h, &h->dsig, h->tab.sigma) ||
@@ -1003,13 +1238,22 @@ int iw_destroy(iw_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   free_fields(h->f64);
   free_fields(h->f32);
-  for (double* p : {h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
+  for (double* p : {h->dDt, h->dD2t, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
                     h->dmeang, h->dwnl, h->dwvr, h->dred})
     cudaFree(p);
   cudaFree(h->dcnt);
   cudaFree(h->dflag);
   cudaFree(h->dcolorder);
   for (int k = 0; k < SYS_KINDS; ++k) {
+    cudaFree(h->dtasks[k]);
+    cudaFree(h->bi[k].ainv);
+    cudaFree(h->bi[k].cvec);
+    cudaFree(h->bi[k].dvec);
+    cudaFree(h->bi[k].minv);
+    cudaFree(h->bi[k].pen);
+    cudaFree(h->bi[k].lvec);
+    cudaFree(h->bi[k].sys);
+    cudaFree(h->bi[k].colsys);
     cudaFree(h->dab[k]);
     cudaFree(h->dipiv[k]);
     cudaFree(h->dinfo[k]);

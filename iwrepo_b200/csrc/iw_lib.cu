@@ -85,46 +85,51 @@ __device__ __forceinline__ T proj_val(const Geo& g, const T* __restrict__ f, int
   return f[fidx<T>(g, i, j, k)];
 }
 
-template <typename T, int NM>
-__global__ void k_stageA(Geo g, const T* __restrict__ F0, const T* __restrict__ F1_, const T* __restrict__ F2_,
-                         const T* __restrict__ F3_, T* __restrict__ O0, T* __restrict__ O1, T* __restrict__ O2,
-                         T* __restrict__ O3, T* __restrict__ Z0, T* __restrict__ Z1, T* __restrict__ Z2,
-                         T* __restrict__ Z3, int proj) {
-  __shared__ double sD[NM * NM];
-  for (int t = threadIdx.x; t < g.N * g.N; t += blockDim.x) sD[t] = g.D[t];
-  __syncthreads();
+// Tiled z-column kernels: a block owns 32 consecutive real x indices of one
+// (y index, subdomain) and keeps the N x 32 tile in shared memory; the N x N
+// operators (D, filter) are applied with compact loops over the tile.
+constexpr int kTX = 32;   // x points per tile (one warp wide)
+constexpr int kTW = 8;    // warps per block
+
+template <typename T>
+__global__ void __launch_bounds__(kTX* kTW) k_stageA(Geo g, const T* __restrict__ F0, const T* __restrict__ F1_,
+                                                     const T* __restrict__ F2_, const T* __restrict__ F3_,
+                                                     T* __restrict__ O0, T* __restrict__ O1, T* __restrict__ O2,
+                                                     T* __restrict__ O3, T* __restrict__ Z0, T* __restrict__ Z1,
+                                                     T* __restrict__ Z2, T* __restrict__ Z3, int proj) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = g.N;
+  T* sD = (T*)smraw;             // N*N
+  T* tile = sD + N * N;          // N*kTX
+  for (int t = threadIdx.x; t < N * N; t += blockDim.x) sD[t] = (T)g.D[t];
   const int q = blockIdx.z;
   const T* F = q == 0 ? F0 : q == 1 ? F1_ : q == 2 ? F2_ : F3_;
   T* O = q == 0 ? O0 : q == 1 ? O1 : q == 2 ? O2 : O3;
   T* Z = q == 0 ? Z0 : q == 1 ? Z1 : q == 2 ? Z2 : Z3;
-  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long total = (long)g.nxpp * g.ny * g.ns;
-  if (gid >= total) return;
-  int i = gid % g.nxpp;
-  long r = gid / g.nxpp;
-  int j = r % g.ny;
-  int ks = r / g.ny;
-  const int N = g.N;
-  T v[NM];
-#pragma unroll
-  for (int k = 0; k < NM; ++k)
-    if (k < N) {
-      int kk = ks * N + k;
-      T x = proj ? proj_val<T>(g, F, i, j, kk) : F[fidx<T>(g, i, j, kk)];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * kTX + lane;
+  const int j = blockIdx.y % g.ny, ks = blockIdx.y / g.ny;
+  const bool act = i < g.nxpp;
+  for (int k = w; k < N; k += kTW) {
+    const int kk = ks * N + k;
+    T x = 0;
+    if (act) {
+      x = proj ? proj_val<T>(g, F, i, j, kk) : F[fidx<T>(g, i, j, kk)];
       if (q == 2 && j == 0 && i < 2) x = (T)0;  // wc(1,1,:) = 0, solver.f:66-69
-      v[k] = x;
       O[fidx<T>(g, i, j, kk)] = x;
     }
+    tile[k * kTX + lane] = x;
+  }
+  __syncthreads();
+  if (!act) return;
   const T fac = (T)g.hfac[ks];
-#pragma unroll
-  for (int k1 = 0; k1 < NM; ++k1)
-    if (k1 < N) {
-      T s = 0;
-#pragma unroll
-      for (int k2 = 0; k2 < NM; ++k2)
-        if (k2 < N) s += (T)sD[k1 * N + k2] * v[k2];
-      Z[fidx<T>(g, i, j, ks * N + k1)] = s * fac;
-    }
+  for (int k1 = w; k1 < N; k1 += kTW) {
+    const T* dr = sD + k1 * N;
+    T s = 0;
+#pragma unroll 4
+    for (int k2 = 0; k2 < N; ++k2) s += dr[k2] * tile[k2 * kTX + lane];
+    Z[fidx<T>(g, i, j, ks * N + k1)] = s * fac;
+  }
 }
 
 // ===========================================================================
@@ -424,72 +429,70 @@ struct EArgs {
   int filter;
 };
 
-template <typename T, int NM>
-__global__ void k_stageE(Geo g, EArgs<T> a, Coefs c) {
-  __shared__ double sD[NM * NM];
-  __shared__ double sL[NM * NM];
-  for (int t = threadIdx.x; t < g.N * g.N; t += blockDim.x) {
-    sD[t] = g.D[t];
-    sL[t] = g.Lfil[t];
-  }
-  __syncthreads();
-  const int q = blockIdx.z;
-  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long total = (long)g.nxpp * g.ny * g.ns;
-  if (gid >= total) return;
-  int i = gid % g.nxpp;
-  long r = gid / g.nxpp;
-  int j = r % g.ny;
-  int ks = r / g.ny;
+template <typename T>
+__global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   const int N = g.N;
-  T z[NM], fs[NM];
-#pragma unroll
-  for (int k = 0; k < NM; ++k)
-    if (k < N) z[k] = a.Z[q][fidx<T>(g, i, j, ks * N + k)];
+  T* sD = (T*)smraw;       // N*N
+  T* sL = sD + N * N;      // N*N
+  T* tz = sL + N * N;      // N*kTX: Z tile
+  T* tf = tz + N * kTX;    // N*kTX: F* tile
+  for (int t = threadIdx.x; t < N * N; t += blockDim.x) {
+    sD[t] = (T)g.D[t];
+    sL[t] = (T)g.Lfil[t];
+  }
+  const int q = blockIdx.z;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * kTX + lane;
+  const int j = blockIdx.y % g.ny, ks = blockIdx.y / g.ny;
+  const bool act = i < g.nxpp;
+  for (int k = w; k < N; k += kTW) tz[k * kTX + lane] = act ? a.Z[q][fidx<T>(g, i, j, ks * N + k)] : (T)0;
+  __syncthreads();
   const T fac = (T)g.hfac[ks];
   const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
-#pragma unroll
-  for (int k1 = 0; k1 < NM; ++k1)
-    if (k1 < N) {
+  for (int k1 = w; k1 < N; k1 += kTW) {
+    T fsv = 0;
+    if (act) {
       const int kk = ks * N + k1;
       const size_t p = fidx<T>(g, i, j, kk);
+      const T* dr = sD + k1 * N;
       T s = 0;
-#pragma unroll
-      for (int k2 = 0; k2 < NM; ++k2)
-        if (k2 < N) s += (T)sD[k1 * N + k2] * z[k2];
-      T S = a.B[q][p] + s * fac;
-      T sn = a.Snold[q][p];
-      T snm = a.Snm_w[q][p];
+#pragma unroll 4
+      for (int k2 = 0; k2 < N; ++k2) s += dr[k2] * tz[k2 * kTX + lane];
+      const T S = a.B[q][p] + s * fac;
+      const T sn = a.Snold[q][p];
+      const T snm = a.Snm_w[q][p];
       if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
-        int side = kk == 0 ? 0 : 1;
+        const int side = kk == 0 ? 0 : 1;
         a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] =
             (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
       }
-      T se = f1 * S + f2 * sn + f3 * snm;
-      T F2 = proj_val<T>(g, a.F1[q], i, j, kk);
-      T fn = a.Fn[q][p];
-      T fnm = a.Fnm_w[q][p];
-      fs[k1] = (T)c.dt * se + (T)c.bdf1 * F2 + (T)c.bdf2 * fn + (T)c.bdf3 * fnm;
+      const T se = f1 * S + f2 * sn + f3 * snm;
+      const T F2 = proj_val<T>(g, a.F1[q], i, j, kk);
+      const T fn = a.Fn[q][p];
+      const T fnm = a.Fnm_w[q][p];
+      fsv = (T)c.dt * se + (T)c.bdf1 * F2 + (T)c.bdf2 * fn + (T)c.bdf3 * fnm;
       a.Snm_w[q][p] = S;
       a.Fnm_w[q][p] = F2;
     }
-  const int ii = i >> 1;
-  const T cf = a.filter ? (T)g.cfour[(size_t)j * g.nxhp + ii] : (T)1;
-#pragma unroll
-  for (int k1 = 0; k1 < NM; ++k1)
-    if (k1 < N) {
-      T o;
-      if (a.filter) {
-        T s = 0;
-#pragma unroll
-        for (int k2 = 0; k2 < NM; ++k2)
-          if (k2 < N) s += (T)sL[k1 * N + k2] * fs[k2];
-        o = cf * s;
-      } else {
-        o = fs[k1];
-      }
-      a.F[q][fidx<T>(g, i, j, ks * N + k1)] = o;
+    tf[k1 * kTX + lane] = fsv;
+  }
+  __syncthreads();
+  if (!act) return;
+  const T cf = a.filter ? (T)g.cfour[(size_t)j * g.nxhp + (i >> 1)] : (T)1;
+  for (int k1 = w; k1 < N; k1 += kTW) {
+    T o;
+    if (a.filter) {
+      const T* lr = sL + k1 * N;
+      T s = 0;
+#pragma unroll 4
+      for (int k2 = 0; k2 < N; ++k2) s += lr[k2] * tf[k2 * kTX + lane];
+      o = cf * s;
+    } else {
+      o = tf[k1 * kTX + lane];
     }
+    a.F[q][fidx<T>(g, i, j, ks * N + k1)] = o;
+  }
 }
 
 // rotational viscous term at the walls (solver.f:318-394, rotvisc 1210-1253):
@@ -586,6 +589,7 @@ struct FactorArgs {
   const double* D2;
   const double* zh;  // ns
   int assemble;      // 0: ab already holds the packed matrix (bandlu_solve_)
+  int factor = 1;    // 0: assemble only (block-inverse systems)
 };
 
 __device__ __forceinline__ double& ABr(double* ab, int ldab, int r, int c) {
@@ -675,6 +679,7 @@ __global__ void k_factor(Geo g, FactorArgs fa) {
   }
 #undef AEL
   }
+  if (!fa.factor) return;
   // SGBTF2
   const int kv = ku + kl;
   int info = 0;
@@ -1078,6 +1083,728 @@ __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ 
       if (role == 0 && r < 2 && lzero && meanu) x = rmul(tb.meang[k], x);
       F[fidx<T>(g, 2 * ii + part, j, k)] = (T)x;
     }
+  }
+}
+
+// ===========================================================================
+// Block-inverse solve of the viscous / diffusive penalty systems.
+// The penalty matrix A is block diagonal in N x N subdomain blocks A_ks, plus
+// coupling in the first row of block ks to all of block ks-1 (vector c_ks)
+// and in its last row to all of block ks+1 (vector d_ks).  With
+// y = A_ks^-1 b_ks, p_ks = A_ks^-1 e_0, q_ks = A_ks^-1 e_{N-1}:
+//     x_ks = y_ks - p_ks sigma_ks - q_ks tau_ks,
+//     sigma_ks = c_ks . x_{ks-1},  tau_ks = d_ks . x_{ks+1},
+// and the 2(ns-1) interface scalars solve a small dense system M z = r.
+// A_ks^-1 is formed once per system (FP64 Gauss-Jordan, partial pivoting),
+// stored column major per block in TI (float for the mixed path).
+// ===========================================================================
+struct BlockInv {
+  const void* ainv;     // per system: ns blocks of N*N, [ks][col][row]
+  const double* cvec;   // per system: ns*N (c_ks, ks>=1)
+  const double* dvec;   // per system: ns*N (d_ks, ks<=ns-2)
+  const double* minv;   // per system: m*m, m = 2(ns-1), row major
+  const double* pen;    // per system: 6*ns penalty parameters
+  const SysDesc* sys;
+  const int* col_sys;
+  const int* col_order;
+  const double* lvec;   // per system: m*N left vectors (see k_solve_cta)
+};
+
+// warp per (system, block): invert A_ks from the assembled band
+__global__ void k_block_invert(Geo g, const double* __restrict__ ab, int nsys, double* __restrict__ ainv64,
+                               double* __restrict__ cvec, double* __restrict__ dvec) {
+  extern __shared__ __align__(16) double smi[];
+  const int warps = blockDim.x / 32, wid = threadIdx.x / 32, lane = threadIdx.x & 31;
+  const int task = blockIdx.x * warps + wid;
+  const int N = g.N, ns = g.ns, n = g.nz, ldab = 3 * N + 1;
+  if (task >= nsys * ns) return;
+  const int s = task / ns, ks = task % ns, km = ks * N;
+  const double* a = ab + (size_t)s * ldab * n;
+  double* M = smi + (size_t)wid * N * 2 * N;  // row major N x 2N
+  auto AB = [&](int r, int c) -> double {     // 0-based global (r, c)
+    int br = 2 * N + r - c;                    // 0-based band row
+    if (br < 0 || br >= ldab) return 0.0;
+    return a[(size_t)br + (size_t)ldab * c];
+  };
+  for (int t = lane; t < N * 2 * N; t += 32) {
+    int r = t / (2 * N), c = t % (2 * N);
+    M[t] = c < N ? AB(km + r, km + c) : (c - N == r ? 1.0 : 0.0);
+  }
+  for (int k = lane; k < N; k += 32) {
+    cvec[((size_t)s * ns + ks) * N + k] = ks > 0 ? AB(km, km - N + k) : 0.0;
+    dvec[((size_t)s * ns + ks) * N + k] = ks < ns - 1 ? AB(km + N - 1, km + N + k) : 0.0;
+  }
+  __syncwarp();
+  for (int col = 0; col < N; ++col) {
+    // pivot: largest |M[r][col]|, r >= col
+    double best = -1.0;
+    int bi = col;
+    for (int r = col + lane; r < N; r += 32) {
+      double v = fabs(M[r * 2 * N + col]);
+      if (v > best) {
+        best = v;
+        bi = r;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (bi != col)
+      for (int c = lane; c < 2 * N; c += 32) {
+        double t = M[col * 2 * N + c];
+        M[col * 2 * N + c] = M[bi * 2 * N + c];
+        M[bi * 2 * N + c] = t;
+      }
+    __syncwarp();
+    const double inv = 1.0 / M[col * 2 * N + col];
+    for (int c = lane; c < 2 * N; c += 32) M[col * 2 * N + c] *= inv;
+    __syncwarp();
+    for (int r = 0; r < N; ++r) {
+      if (r == col) continue;
+      const double f = M[r * 2 * N + col];
+      if (f != 0.0)
+        for (int c = lane; c < 2 * N; c += 32) M[r * 2 * N + c] -= f * M[col * 2 * N + c];
+    }
+    __syncwarp();
+  }
+  double* out = ainv64 + ((size_t)s * ns + ks) * N * N;
+  for (int t = lane; t < N * N; t += 32) {
+    int c = t / N, r = t % N;  // column major
+    out[t] = M[r * 2 * N + N + c];
+  }
+}
+
+// thread per system: interface matrix M (m = 2(ns-1)) and its inverse
+__global__ void k_iface_matrix(Geo g, int nsys, const double* __restrict__ ainv64, const double* __restrict__ cvec,
+                               const double* __restrict__ dvec, double* __restrict__ minv, double* __restrict__ work) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = g.N, ns = g.ns, m = 2 * (ns - 1);
+  if (s >= nsys || m == 0) return;
+  double* A = work + (size_t)s * 2 * m * m;  // m x 2m
+  for (int t = 0; t < 2 * m * m; ++t) A[t] = 0.0;
+  // unknown index: sigma_ks (ks=1..ns-1) -> ks-1 ; tau_ks (ks=0..ns-2) -> ns-1+ks
+  auto inv = [&](int ks, int r, int c) { return ainv64[(((size_t)s * ns + ks) * N + c) * N + r]; };
+  for (int ks = 0; ks < ns; ++ks) {
+    if (ks + 1 <= ns - 1) {  // row for sigma_{ks+1}
+      int row = ks;          // sigma_{ks+1} index
+      const double* c = cvec + ((size_t)s * ns + ks + 1) * N;
+      double cp = 0, cq = 0;
+      for (int k = 0; k < N; ++k) {
+        cp += c[k] * inv(ks, k, 0);
+        cq += c[k] * inv(ks, k, N - 1);
+      }
+      A[row * 2 * m + row] += 1.0;
+      if (ks >= 1) A[row * 2 * m + (ks - 1)] += cp;
+      if (ks <= ns - 2) A[row * 2 * m + (ns - 1 + ks)] += cq;
+    }
+    if (ks - 1 >= 0) {  // row for tau_{ks-1}
+      int row = ns - 1 + ks - 1;
+      const double* d = dvec + ((size_t)s * ns + ks - 1) * N;
+      double dp = 0, dq = 0;
+      for (int k = 0; k < N; ++k) {
+        dp += d[k] * inv(ks, k, 0);
+        dq += d[k] * inv(ks, k, N - 1);
+      }
+      A[row * 2 * m + row] += 1.0;
+      if (ks >= 1) A[row * 2 * m + (ks - 1)] += dp;
+      if (ks <= ns - 2) A[row * 2 * m + (ns - 1 + ks)] += dq;
+    }
+  }
+  for (int r = 0; r < m; ++r) A[r * 2 * m + m + r] = 1.0;
+  for (int col = 0; col < m; ++col) {
+    int bi = col;
+    for (int r = col + 1; r < m; ++r)
+      if (fabs(A[r * 2 * m + col]) > fabs(A[bi * 2 * m + col])) bi = r;
+    if (bi != col)
+      for (int c = 0; c < 2 * m; ++c) {
+        double t = A[col * 2 * m + c];
+        A[col * 2 * m + c] = A[bi * 2 * m + c];
+        A[bi * 2 * m + c] = t;
+      }
+    double iv = 1.0 / A[col * 2 * m + col];
+    for (int c = 0; c < 2 * m; ++c) A[col * 2 * m + c] *= iv;
+    for (int r = 0; r < m; ++r)
+      if (r != col) {
+        double f = A[r * 2 * m + col];
+        if (f != 0.0)
+          for (int c = 0; c < 2 * m; ++c) A[r * 2 * m + c] -= f * A[col * 2 * m + c];
+      }
+  }
+  for (int r = 0; r < m; ++r)
+    for (int c = 0; c < m; ++c) minv[(size_t)s * m * m + r * m + c] = A[r * 2 * m + m + c];
+}
+
+// ===========================================================================
+// Grouped solves: one warp per task = up to G columns that share one system
+// (same kx^2+ky^2, adjacent in the sorted column order).  All right-hand
+// sides of the task advance together through each elimination step, so the
+// factor column is fetched once per step for all of them.
+// ===========================================================================
+struct Task {
+  int sys;    // system index (-1: no system, e.g. pressure of the (0,0) mode)
+  int first;  // index into the sorted column order
+  int count;  // columns in the task (<= G)
+};
+
+// SGBTRS + STBSV arithmetic for R <= RM right-hand sides b[r*n + row]
+template <int RM>
+__device__ void band_solve_multi(const double* __restrict__ ab, const int* __restrict__ ipiv, double* b, int R, int n,
+                                 int kl, int ku, int lane) {
+  constexpr int PF = 4;
+  const int ldab = 2 * kl + ku + 1, kd = ku + kl + 1;
+  const int i0 = lane + 1, i1 = lane + 33;
+  int rl[PF];
+  double rm0[PF], rm1[PF];
+#pragma unroll
+  for (int d = 0; d < PF; ++d) {
+    const int j = 1 + d;
+    rl[d] = 0;
+    rm0[d] = rm1[d] = 0.0;
+    if (j <= n - 1) {
+      const int lm = min(kl, n - j);
+      const double* col = ab + (size_t)ldab * (j - 1);
+      rl[d] = __ldg(ipiv + j - 1);
+      if (i0 <= lm) rm0[d] = __ldg(col + kd + i0 - 1);
+      if (i1 <= lm) rm1[d] = __ldg(col + kd + i1 - 1);
+    }
+  }
+  for (int jb = 1; jb <= n - 1; jb += PF) {
+#pragma unroll
+    for (int d = 0; d < PF; ++d) {
+      const int j = jb + d;
+      if (j <= n - 1) {
+        const int lm = min(kl, n - j);
+        const int l = rl[d];
+        const double m0 = rm0[d], m1 = rm1[d];
+        const int jn = j + PF;
+        if (jn <= n - 1) {
+          const int lmn = min(kl, n - jn);
+          const double* coln = ab + (size_t)ldab * (jn - 1);
+          rl[d] = __ldg(ipiv + jn - 1);
+          rm0[d] = (i0 <= lmn) ? __ldg(coln + kd + i0 - 1) : 0.0;
+          rm1[d] = (i1 <= lmn) ? __ldg(coln + kd + i1 - 1) : 0.0;
+        }
+        double y[RM], nv0[RM], nv1[RM];
+        const int row0 = j + i0, row1 = j + i1;
+#pragma unroll
+        for (int r = 0; r < RM; ++r)
+          if (r < R) {
+            const double* br = b + (size_t)r * n;
+            const double bj = br[j - 1], bl = br[l - 1];
+            y[r] = (l != j) ? bl : bj;
+            if (i0 <= lm) {
+              const double old = (row0 == l) ? bj : br[row0 - 1];
+              nv0[r] = (y[r] != 0.0) ? radd(old, rmul(m0, -y[r])) : old;
+            }
+            if (i1 <= lm) {
+              const double old = (row1 == l) ? bj : br[row1 - 1];
+              nv1[r] = (y[r] != 0.0) ? radd(old, rmul(m1, -y[r])) : old;
+            }
+          }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < RM; ++r)
+          if (r < R) {
+            double* br = b + (size_t)r * n;
+            if (i0 <= lm) br[row0 - 1] = nv0[r];
+            if (i1 <= lm) br[row1 - 1] = nv1[r];
+            if (lane == 0) br[j - 1] = y[r];
+          }
+        __syncwarp();
+      }
+    }
+  }
+  const int k = kl + ku, kplus1 = k + 1;
+  double rdg[PF], rv0[PF], rv1[PF], rv2[PF];
+  const int o0 = k - 1 - lane, o1 = k - 1 - lane - 32, o2 = k - 1 - lane - 64;
+#pragma unroll
+  for (int d = 0; d < PF; ++d) {
+    const int j = n - d;
+    rdg[d] = rv0[d] = rv1[d] = rv2[d] = 0.0;
+    if (j >= 1) {
+      const double* col = ab + (size_t)ldab * (j - 1);
+      rdg[d] = __ldg(col + kplus1 - 1);
+      if (o0 >= 0) rv0[d] = __ldg(col + o0);
+      if (o1 >= 0) rv1[d] = __ldg(col + o1);
+      if (o2 >= 0) rv2[d] = __ldg(col + o2);
+    }
+  }
+  for (int jb = n; jb >= 1; jb -= PF) {
+#pragma unroll
+    for (int d = 0; d < PF; ++d) {
+      const int j = jb - d;
+      if (j >= 1) {
+        const double dg = rdg[d];
+        const double v0 = rv0[d], v1 = rv1[d], v2 = rv2[d];
+        const int jn = j - PF;
+        if (jn >= 1) {
+          const double* coln = ab + (size_t)ldab * (jn - 1);
+          rdg[d] = __ldg(coln + kplus1 - 1);
+          rv0[d] = (o0 >= 0) ? __ldg(coln + o0) : 0.0;
+          rv1[d] = (o1 >= 0) ? __ldg(coln + o1) : 0.0;
+          rv2[d] = (o2 >= 0) ? __ldg(coln + o2) : 0.0;
+        }
+        const int lo = max(1, j - k);
+        const int ia = j - 1 - lane, ib = ia - 32, ic = ia - 64;
+        double xj[RM], n0[RM], n1[RM], n2[RM];
+#pragma unroll
+        for (int r = 0; r < RM; ++r)
+          if (r < R) {
+            const double* br = b + (size_t)r * n;
+            xj[r] = br[j - 1];
+            if (xj[r] != 0.0) {
+              xj[r] = __ddiv_rn(xj[r], dg);
+              if (ia >= lo) n0[r] = rsub(br[ia - 1], rmul(xj[r], v0));
+              if (ib >= lo) n1[r] = rsub(br[ib - 1], rmul(xj[r], v1));
+              if (ic >= lo) n2[r] = rsub(br[ic - 1], rmul(xj[r], v2));
+            }
+          }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < RM; ++r)
+          if (r < R && xj[r] != 0.0) {
+            double* br = b + (size_t)r * n;
+            if (ia >= lo) br[ia - 1] = n0[r];
+            if (ib >= lo) br[ib - 1] = n1[r];
+            if (ic >= lo) br[ic - 1] = n2[r];
+            if (lane == 0) br[j - 1] = xj[r];
+          }
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// K_F grouped: pressure for the columns of one task (calcuvwt.f:87-229)
+template <typename T, int G>
+__global__ void k_press_g(Geo g, SolveTabs tb, const Task* __restrict__ tasks, int ntask, T* __restrict__ U,
+                          T* __restrict__ V, T* __restrict__ W, const double* __restrict__ wnl,
+                          const double* __restrict__ wvr, int cpen, int kstart) {
+  extern __shared__ __align__(16) double sm[];
+  const int warps = blockDim.x / 32, wid = threadIdx.x / 32, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * warps + wid;
+  if (t >= ntask) return;
+  const Task tk = tasks[t];
+  const int n = g.nz, N = g.N;
+  double* B = sm + (size_t)wid * 2 * G * n;
+  const int R = 2 * tk.count;
+  const double dt = g.dt;
+  const int s = tk.sys;
+  if (s >= 0) {
+    const SysDesc sd = tb.sys[s];
+    const double eps = sd.eps;
+    for (int ci = 0; ci < tk.count; ++ci) {
+      const int c = tb.col_order[tk.first + ci];
+      const int j = c / g.nxhp, ii = c % g.nxhp;
+      const double xw = g.xw[ii], yw = g.yw[j];
+      double* rr = B + (size_t)(2 * ci) * n;
+      double* ri = rr + n;
+      for (int k = lane; k < n; k += 32) {
+        const int ks = k / N, k1 = k % N;
+        double sr = 0.0, si = 0.0;
+        for (int k2 = 0; k2 < N; ++k2) {
+          const double dd = g.D[k1 * N + k2];
+          sr = radd(sr, rmul(dd, (double)W[fidx<T>(g, 2 * ii, j, ks * N + k2)]));
+          si = radd(si, rmul(dd, (double)W[fidx<T>(g, 2 * ii + 1, j, ks * N + k2)]));
+        }
+        const double fac = g.hfac[ks];
+        const double dwr = rmul(sr, fac), dwi = rmul(si, fac);
+        const double ur = (double)U[fidx<T>(g, 2 * ii, j, k)], ui = (double)U[fidx<T>(g, 2 * ii + 1, j, k)];
+        const double vr = (double)V[fidx<T>(g, 2 * ii, j, k)], vi = (double)V[fidx<T>(g, 2 * ii + 1, j, k)];
+        double dr = radd(radd(0.0, -rmul(xw, ui)), -rmul(yw, vi));
+        double di = radd(radd(0.0, rmul(xw, ur)), rmul(yw, vr));
+        dr = radd(dr, dwr);
+        di = radd(di, dwi);
+        rr[k] = -rmul(__ddiv_rn(dr, dt), eps);
+        ri[k] = -rmul(__ddiv_rn(di, dt), eps);
+      }
+      __syncwarp();
+      if (lane == 0) {
+        const size_t p1 = (size_t)g.nxpp * j + 2 * ii, p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii;
+        const double bcrbot = radd(wnl[p1], wvr[p1]), bcibot = radd(wnl[p1 + 1], wvr[p1 + 1]);
+        const double bcrtop = radd(wnl[p2], wvr[p2]), bcitop = radd(wnl[p2 + 1], wvr[p2 + 1]);
+        rr[0] = rsub(rr[0], rmul(rmul(sd.tau1_bot, bcrbot), eps));
+        ri[0] = rsub(ri[0], rmul(rmul(sd.tau1_bot, bcibot), eps));
+        rr[n - 1] = radd(rr[n - 1], rmul(rmul(sd.tau2_top, bcrtop), eps));
+        ri[n - 1] = radd(ri[n - 1], rmul(rmul(sd.tau2_top, bcitop), eps));
+      }
+      __syncwarp();
+    }
+    const int ldab = 3 * N + 1;
+    band_solve_multi<2 * G>(tb.ab + (size_t)s * ldab * n, tb.ipiv + (size_t)s * n, B, R, n, N, N, lane);
+    if (cpen) {
+      legen_filter_cols(B, R, n, N, g.ns, tb.wg, tb.alpol, tb.sigma, lane);
+      __syncwarp();
+    }
+  } else {
+    for (int q = lane; q < R * n; q += 32) B[q] = 0.0;
+    __syncwarp();
+  }
+  for (int ci = 0; ci < tk.count; ++ci) {
+    const int c = tb.col_order[tk.first + ci];
+    const int j = c / g.nxhp, ii = c % g.nxhp;
+    const bool lzero = (ii == 0 && j == 0);
+    const double dtx = rmul(dt, g.xw[ii]), dty = rmul(dt, g.yw[j]);
+    const double* rr = B + (size_t)(2 * ci) * n;
+    const double* ri = rr + n;
+    for (int k = lane; k < n; k += 32) {
+      const size_t pr = fidx<T>(g, 2 * ii, j, k), pi = pr + 1;
+      if (k < kstart) {
+        U[pr] = 0;
+        U[pi] = 0;
+        V[pr] = 0;
+        V[pi] = 0;
+        W[pr] = 0;
+        W[pi] = 0;
+        continue;
+      }
+      const double phr = rr[k], phi = ri[k];
+      const double ur = (double)U[pr], ui = (double)U[pi], vr = (double)V[pr], vi = (double)V[pi];
+      double wbr = 0, wbi = 0;
+      if (!lzero) {
+        const int ks = k / N, k1 = k % N;
+        double sr = 0.0, si = 0.0;
+        for (int k2 = 0; k2 < N; ++k2) {
+          const double dd = g.D[k1 * N + k2];
+          sr = radd(sr, rmul(dd, rr[ks * N + k2]));
+          si = radd(si, rmul(dd, ri[ks * N + k2]));
+        }
+        const double fac = g.hfac[ks];
+        wbr = rsub((double)W[pr], rmul(dt, rmul(sr, fac)));
+        wbi = rsub((double)W[pi], rmul(dt, rmul(si, fac)));
+      }
+      U[pr] = (T)rsub(ur, rsub(rmul(0.0, phr), rmul(dtx, phi)));
+      U[pi] = (T)rsub(ui, radd(rmul(0.0, phi), rmul(dtx, phr)));
+      V[pr] = (T)rsub(vr, rsub(rmul(0.0, phr), rmul(dty, phi)));
+      V[pi] = (T)rsub(vi, radd(rmul(0.0, phi), rmul(dty, phr)));
+      W[pr] = (T)wbr;
+      W[pi] = (T)wbi;
+    }
+  }
+}
+
+// ===========================================================================
+// Block-inverse solve, one CTA per task (row parallel).
+//
+// A = blockdiag(A_0..A_{ns-1}) + interface couplings (first row of block ks
+// couples to the last row of ks-1 through c_ks, last row of ks to the first
+// row of ks+1 through d_ks).  With y = blockdiag^-1 b the interface unknowns
+// solve M z = r, r_e = <c_{e+1}, y_e> (e < ns-1), <d_t, y_{t+1}> (e = ns-1+t),
+// and x = y - A_ks^-1 e_0 z_{ks-1} - A_ks^-1 e_{N-1} z_{ns-1+ks}.
+// Because <c, A^-1 b> = <A^-T c, b>, the left vectors lvec = A^-T c, A^-T d
+// are precomputed per system, so r comes straight from b and x from one sweep
+// in which every inverse entry is read once (coalesced) and used for all R
+// right-hand sides.  Each thread owns whole rows.
+// ===========================================================================
+constexpr int kSolveThreads = 128;
+
+// dst = (accum ? dst : 0) + A^-1 src for R right-hand sides of length n.
+// rz, zz: R*m doubles of shared scratch.  Ends synchronised.
+template <int R>
+__device__ void bi_apply_cta(const Geo& g, const double* __restrict__ ainv, const double* __restrict__ lvec,
+                             const double* __restrict__ minv, const double* src, double* dst, double* rz, double* zz,
+                             bool accum) {
+  const int N = g.N, ns = g.ns, n = g.nz, m = 2 * (ns - 1);
+  const int tid = threadIdx.x;
+  if (m > 0) {
+    for (int q = tid; q < m * R; q += kSolveThreads) {
+      const int r = q / m, e = q - r * m;
+      const int blk = e < ns - 1 ? e : e - (ns - 1) + 1;
+      const double* lv = lvec + (size_t)e * N;
+      const double* sv = src + (size_t)r * n + blk * N;
+      double acc = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < N; ++k) acc += lv[k] * sv[k];
+      rz[q] = acc;
+    }
+    __syncthreads();
+    for (int q = tid; q < m * R; q += kSolveThreads) {
+      const int r = q / m, e = q - r * m;
+      const double* mr = minv + (size_t)e * m;
+      const double* rr = rz + r * m;
+      double z = 0.0;
+#pragma unroll 4
+      for (int c = 0; c < m; ++c) z += mr[c] * rr[c];
+      zz[q] = z;
+    }
+    __syncthreads();
+  }
+  for (int row = tid; row < n; row += kSolveThreads) {
+    const int ks = row / N, kk = row - ks * N;
+    const double* ai = ainv + (size_t)ks * N * N + kk;
+    const double* sv = src + ks * N;
+    double acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] = 0.0;
+#pragma unroll 8
+    for (int c = 0; c < N; ++c) {
+      const double a = __ldg(ai + (size_t)c * N);
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] += a * sv[(size_t)r * n + c];
+    }
+    const double p = ks >= 1 ? __ldg(ai) : 0.0;
+    const double q = ks <= ns - 2 ? __ldg(ai + (size_t)(N - 1) * N) : 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      double x = acc[r];
+      if (ks >= 1) x -= p * zz[r * m + ks - 1];
+      if (ks <= ns - 2) x -= q * zz[r * m + ns - 1 + ks];
+      double* d = dst + (size_t)r * n + row;
+      *d = accum ? *d + x : x;
+    }
+  }
+  __syncthreads();
+}
+
+// b -= A x for R right-hand sides (matrix free, FP64).  D2t/Dt: transposed
+// differentiation matrices (Dt[k*N + k1] = D[k1][k]).
+template <int R>
+__device__ void sub_A_cta(const Geo& g, const double* __restrict__ D2t, const double* __restrict__ zh, double eps,
+                          const double* __restrict__ pen, const double* x, double* b) {
+  const int N = g.N, ns = g.ns, n = g.nz;
+  for (int row = threadIdx.x; row < n; row += kSolveThreads) {
+    const int ks = row / N, k1 = row - ks * N, km = ks * N;
+    const double h2 = 2.0 / zh[ks];
+    double s2[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) s2[r] = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < N; ++k) {
+      const double d = __ldg(D2t + k * N + k1);
+#pragma unroll
+      for (int r = 0; r < R; ++r) s2[r] += d * x[(size_t)r * n + km + k];
+    }
+    const double ee = eps * (h2 * h2);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const double* xr = x + (size_t)r * n;
+      double v = xr[row] - ee * s2[r];
+      if (k1 == 0) {
+        const double pa = pen[ks], pb = pen[ns + ks], t1 = pen[4 * ns + ks];
+        double s0 = 0;
+        for (int k = 0; k < N; ++k) s0 += g.D[k] * xr[km + k];
+        v += t1 * pa * xr[km] - t1 * pb * eps * h2 * s0;
+        if (ks > 0) {
+          const double hl = 2.0 / zh[ks - 1];
+          double sl = 0;
+          for (int k = 0; k < N; ++k) sl += g.D[(N - 1) * N + k] * xr[km - N + k];
+          v += -0.5 * t1 * pa * xr[km] + 0.5 * t1 * pb * eps * h2 * s0 - 0.5 * t1 * pa * xr[km - 1] +
+               0.5 * t1 * pb * eps * hl * sl;
+        }
+      }
+      if (k1 == N - 1) {
+        const double pg = pen[2 * ns + ks], pd = pen[3 * ns + ks], t2 = pen[5 * ns + ks];
+        double s1 = 0;
+        for (int k = 0; k < N; ++k) s1 += g.D[(N - 1) * N + k] * xr[km + k];
+        v += t2 * pg * xr[km + N - 1] + t2 * pd * eps * h2 * s1;
+        if (ks < ns - 1) {
+          const double hr = 2.0 / zh[ks + 1];
+          double sr = 0;
+          for (int k = 0; k < N; ++k) sr += g.D[k] * xr[km + N + k];
+          v += -0.5 * t2 * pg * xr[km + N - 1] - 0.5 * t2 * pd * eps * h2 * s1 - 0.5 * t2 * pg * xr[km + N] -
+               0.5 * t2 * pd * eps * hr * sr;
+        }
+      }
+      b[(size_t)r * n + row] -= v;
+    }
+  }
+  __syncthreads();
+}
+
+// Solve of one task: <= R/per columns sharing system tk.sys, per = 4 right-hand
+// sides per column for role 0 (u, v re/im), 2 otherwise; unused ones are zero.
+// role 0: u/v (F0, F1), 1: w (F0), 2: rho (F0), 3: pressure from u*,v*,w*
+// (F0, F1, F2) followed by the projection (calcuvwt.f:87-229, 826-901).
+// refine: one FP64 residual sweep x += A^-1 (b - A x).
+template <typename T, int R>
+__global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
+    Geo g, BlockInv bi, SolveTabs tb, const Task* __restrict__ tasks, T* __restrict__ F0, T* __restrict__ F1,
+    T* __restrict__ F2, double rdiv, int role, int cpen, int meanu, int refine, const double* __restrict__ Dt,
+    const double* __restrict__ D2t, const double* __restrict__ zh, const double* __restrict__ wnl,
+    const double* __restrict__ wvr, int kstart) {
+  extern __shared__ __align__(16) double sm[];
+  const Task tk = tasks[blockIdx.x];
+  const int n = g.nz, N = g.N, ns = g.ns, m = 2 * (ns - 1);
+  const int tid = threadIdx.x;
+  double* b = sm;
+  double* x = b + (size_t)R * n;
+  double* rz = x + (size_t)R * n;
+  double* zz = rz + (size_t)R * (m > 0 ? m : 1);
+  const int per = role == 0 ? 4 : 2;
+  const int s = tk.sys;
+  const int ncolt = tk.count;
+  const double dt = g.dt;
+  if (s < 0 && role != 3) {  // w of the (0,0) mode is zero
+    for (int ci = 0; ci < ncolt; ++ci) {
+      const int c = tb.col_order[tk.first + ci];
+      const int j = c / g.nxhp, ii = c % g.nxhp;
+      for (int k = tid; k < n; k += kSolveThreads) {
+        F0[fidx<T>(g, 2 * ii, j, k)] = 0;
+        F0[fidx<T>(g, 2 * ii + 1, j, k)] = 0;
+      }
+    }
+    return;
+  }
+  if (s < 0) {  // pressure of the (0,0) mode: phi = 0
+    for (int q = tid; q < R * n; q += kSolveThreads) x[q] = 0.0;
+    __syncthreads();
+  } else {
+    const SysDesc sd = bi.sys[s];
+    const double eps = sd.eps;
+    // right-hand sides
+    if (role == 3) {
+      for (int q = tid; q < R * n; q += kSolveThreads) {  // w* columns into x (scratch)
+        const int r = q / n, k = q - r * n, ci = r >> 1;
+        double v = 0.0;
+        if (ci < ncolt) {
+          const int c = tb.col_order[tk.first + ci];
+          const int j = c / g.nxhp, ii = c % g.nxhp;
+          v = (double)F2[fidx<T>(g, 2 * ii + (r & 1), j, k)];
+        }
+        x[q] = v;
+      }
+      __syncthreads();
+      for (int q = tid; q < R * n; q += kSolveThreads) {
+        const int r = q / n, k = q - r * n, ci = r >> 1, part = r & 1;
+        double v = 0.0;
+        if (ci < ncolt) {
+          const int c = tb.col_order[tk.first + ci];
+          const int j = c / g.nxhp, ii = c % g.nxhp;
+          const int ks = k / N, k1 = k - ks * N;
+          const double* wc = x + (size_t)r * n + ks * N;
+          double sr = 0.0;
+          for (int k2 = 0; k2 < N; ++k2) sr += __ldg(Dt + k2 * N + k1) * wc[k2];
+          const double dw = sr * g.hfac[ks];
+          const double xw = g.xw[ii], yw = g.yw[j];
+          double d;
+          if (part == 0)
+            d = -(xw * (double)F0[fidx<T>(g, 2 * ii + 1, j, k)]) - (yw * (double)F1[fidx<T>(g, 2 * ii + 1, j, k)]) + dw;
+          else
+            d = (xw * (double)F0[fidx<T>(g, 2 * ii, j, k)]) + (yw * (double)F1[fidx<T>(g, 2 * ii, j, k)]) + dw;
+          v = -((d / dt) * eps);
+          if (k == 0) {
+            const size_t p1 = (size_t)g.nxpp * j + 2 * ii + part;
+            v -= (sd.tau1_bot * (wnl[p1] + wvr[p1])) * eps;
+          }
+          if (k == n - 1) {
+            const size_t p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii + part;
+            v += (sd.tau2_top * (wnl[p2] + wvr[p2])) * eps;
+          }
+        }
+        b[q] = v;
+      }
+    } else {
+      for (int q = tid; q < R * n; q += kSolveThreads) {
+        const int r = q / n, k = q - r * n, ci = r / per, rr = r - ci * per;
+        double v = 0.0;
+        if (ci < ncolt) {
+          const int c = tb.col_order[tk.first + ci];
+          const int j = c / g.nxhp, ii = c % g.nxhp;
+          const T* F = (role == 0 && rr >= 2) ? F1 : F0;
+          v = -(-((double)F[fidx<T>(g, 2 * ii + (rr & 1), j, k)] / rdiv) * eps);
+        }
+        b[q] = v;
+      }
+    }
+    __syncthreads();
+    const double* ainv = (const double*)bi.ainv + (size_t)s * ns * N * N;
+    const double* lv = bi.lvec + (size_t)s * (m > 0 ? m : 1) * N;
+    const double* mi = bi.minv + (size_t)s * (m > 0 ? m * m : 1);
+    bi_apply_cta<R>(g, ainv, lv, mi, b, x, rz, zz, false);
+    if (refine) {
+      sub_A_cta<R>(g, D2t, zh, eps, bi.pen + (size_t)s * 6 * ns, x, b);
+      bi_apply_cta<R>(g, ainv, lv, mi, b, x, rz, zz, true);
+    }
+    if (cpen) {
+      const int w = tid >> 5, lane = tid & 31;
+      for (int r = w; r < R; r += kSolveThreads / 32)
+        legen_filter_cols(x + (size_t)r * n, 1, n, N, ns, tb.wg, tb.alpol, tb.sigma, lane);
+      __syncthreads();
+    }
+  }
+  // write back
+  if (role == 3) {
+    for (int q = tid; q < (R / 2) * n; q += kSolveThreads) {
+      const int ci = q / n, k = q - ci * n;
+      if (ci >= ncolt) continue;
+      const int c = tb.col_order[tk.first + ci];
+      const int j = c / g.nxhp, ii = c % g.nxhp;
+      const size_t pr = fidx<T>(g, 2 * ii, j, k), pi = pr + 1;
+      if (k < kstart) {
+        F0[pr] = 0;
+        F0[pi] = 0;
+        F1[pr] = 0;
+        F1[pi] = 0;
+        F2[pr] = 0;
+        F2[pi] = 0;
+        continue;
+      }
+      const double* rr = x + (size_t)(2 * ci) * n;
+      const double* ri = rr + n;
+      const double phr = rr[k], phi = ri[k];
+      double wbr = 0, wbi = 0;
+      if (!(ii == 0 && j == 0)) {
+        const int ks = k / N, k1 = k - ks * N;
+        double sr = 0.0, si = 0.0;
+        for (int k2 = 0; k2 < N; ++k2) {
+          const double dd = __ldg(Dt + k2 * N + k1);
+          sr += dd * rr[ks * N + k2];
+          si += dd * ri[ks * N + k2];
+        }
+        const double fac = g.hfac[ks];
+        wbr = (double)F2[pr] - dt * (sr * fac);
+        wbi = (double)F2[pi] - dt * (si * fac);
+      }
+      const double dtx = dt * g.xw[ii], dty = dt * g.yw[j];
+      F0[pr] = (T)((double)F0[pr] + dtx * phi);
+      F0[pi] = (T)((double)F0[pi] - dtx * phr);
+      F1[pr] = (T)((double)F1[pr] + dty * phi);
+      F1[pi] = (T)((double)F1[pi] - dty * phr);
+      F2[pr] = (T)wbr;
+      F2[pi] = (T)wbi;
+    }
+  } else {
+    for (int q = tid; q < R * n; q += kSolveThreads) {
+      const int r = q / n, k = q - r * n, ci = r / per, rr = r - ci * per;
+      if (ci >= ncolt) continue;
+      const int c = tb.col_order[tk.first + ci];
+      const int j = c / g.nxhp, ii = c % g.nxhp;
+      T* F = (role == 0 && rr >= 2) ? F1 : F0;
+      double v = x[q];
+      if (role == 0 && rr < 2 && meanu && ii == 0 && j == 0) v = tb.meang[k] * v;
+      F[fidx<T>(g, 2 * ii + (rr & 1), j, k)] = (T)v;
+    }
+  }
+}
+
+// lvec[s][e][c] = sum_k A_blk^-1[k][c] v_e[k]: v_e = c_{e+1} on block e (e < ns-1),
+// d_t on block t+1 (e = ns-1+t).  One thread per (system, e, c).
+__global__ void k_left_vecs(Geo g, int nsys, const double* __restrict__ ainv, const double* __restrict__ cvec,
+                            const double* __restrict__ dvec, double* __restrict__ lvec) {
+  const int N = g.N, ns = g.ns, m = 2 * (ns - 1);
+  const size_t tot = (size_t)nsys * m * N;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(q % N);
+    const int e = (int)((q / N) % m);
+    const size_t s = q / ((size_t)N * m);
+    int blk;
+    const double* v;
+    if (e < ns - 1) {
+      blk = e;
+      v = cvec + (s * ns + e + 1) * N;
+    } else {
+      blk = e - (ns - 1) + 1;
+      v = dvec + (s * ns + blk - 1) * N;
+    }
+    const double* ai = ainv + (s * ns + blk) * (size_t)N * N + (size_t)c * N;
+    double acc = 0.0;
+    for (int k = 0; k < N; ++k) acc += ai[k] * v[k];
+    lvec[q] = acc;
   }
 }
 

