@@ -300,7 +300,7 @@ struct iw_handle {
   bool mixed = false;
   Tables tab;
   // device tables
-  double *dDt = 0, *dD2t = 0;  // transposed D, D2 (t[k*N + k1] = D[k1][k])
+  double *dDt = 0, *dD2t = 0, *dLt = 0;  // transposed D, D2, Legendre filter (t[k*N + k1] = D[k1][k])
   double *dD = 0, *dD2 = 0, *dL = 0, *dh = 0, *dxw = 0, *dyw = 0, *dcf = 0, *dzg = 0, *dzh = 0;
   double *dwg = 0, *dal = 0, *dsig = 0, *dmeang = 0;
   double *dwnl = 0, *dwvr = 0, *dred = 0;
@@ -1008,7 +1008,7 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   if (h->ntask[kind] > 0)
     k_solve_cta<T, R><<<h->ntask[kind], kSolveThreads, sm, h->st>>>(
         geo(h), bi, solve_tabs(h, kind), h->dtasks[kind], F0, F1, F2, rd, role, cpen, meanu, refine, h->dDt, h->dD2t,
-        h->dzh, h->dwnl, h->dwvr, kstart);
+        h->dLt, h->dzh, h->dwnl, h->dwvr, kstart);
 }
 
 // calcuvwt (calcuvwt_noslip.f / calcuvwt.f) on u*,v*,w*,rho* held in F.
@@ -1202,14 +1202,15 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
         cf[(size_t)j * h->nxhp + ii] = std::exp(-prm->amp * std::pow(theta, 2. * prm->pf));
       }
   }
-  std::vector<double> Dt(h->N * h->N), D2t(h->N * h->N);
+  std::vector<double> Dt(h->N * h->N), D2t(h->N * h->N), Lt(h->N * h->N);
   for (int k1 = 0; k1 < h->N; ++k1)
     for (int k = 0; k < h->N; ++k) {
       Dt[(size_t)k * h->N + k1] = h->tab.D[(size_t)k1 * h->N + k];
       D2t[(size_t)k * h->N + k1] = h->tab.D2[(size_t)k1 * h->N + k];
+      Lt[(size_t)k * h->N + k1] = h->tab.Lfil[(size_t)k1 * h->N + k];
     }
   int r = 0;
-  r |= up(h, &h->dDt, Dt) || up(h, &h->dD2t, D2t);
+  r |= up(h, &h->dDt, Dt) || up(h, &h->dD2t, D2t) || up(h, &h->dLt, Lt);
   r |= up(h, &h->dD, h->tab.D) || up(h, &h->dD2, h->tab.D2) || up(h, &h->dL, h->tab.Lfil) || up(h, &h->dh, hf) ||
        up(h, &h->dxw, xw) || up(h, &h->dyw, yw) || up(h, &h->dcf, cf) || up(h, &h->dzg, zg) || up(h, &h->dzh, zh) ||
        up(h, &h->dwg, h->tab.wg) || up(h, &h->dal, h->tab.alpol) || up(h, &h->dsig, h->tab.sigma) ||
@@ -1238,7 +1239,7 @@ int iw_destroy(iw_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   free_fields(h->f64);
   free_fields(h->f32);
-  for (double* p : {h->dDt, h->dD2t, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
+  for (double* p : {h->dDt, h->dD2t, h->dLt, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
                     h->dmeang, h->dwnl, h->dwvr, h->dred})
     cudaFree(p);
   cudaFree(h->dcnt);

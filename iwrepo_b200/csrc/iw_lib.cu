@@ -1616,6 +1616,29 @@ __device__ void sub_A_cta(const Geo& g, const double* __restrict__ D2t, const do
   __syncthreads();
 }
 
+// dst[r][row] = sum_j L[kk][j] src[r][ks*N + j]: the Legendre filter of every
+// subdomain (filtering.f:1225-1243 with the precombined matrix; Lt = L^T).
+template <int R>
+__device__ void legen_filter_cta(const Geo& g, const double* __restrict__ Lt, const double* src, double* dst) {
+  const int N = g.N, n = g.nz;
+  for (int row = threadIdx.x; row < n; row += kSolveThreads) {
+    const int ks = row / N, kk = row - ks * N;
+    const double* sv = src + ks * N;
+    double acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] = 0.0;
+#pragma unroll 8
+    for (int j = 0; j < N; ++j) {
+      const double l = __ldg(Lt + j * N + kk);
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] += l * sv[(size_t)r * n + j];
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[(size_t)r * n + row] = acc[r];
+  }
+  __syncthreads();
+}
+
 // Solve of one task: <= R/per columns sharing system tk.sys, per = 4 right-hand
 // sides per column for role 0 (u, v re/im), 2 otherwise; unused ones are zero.
 // role 0: u/v (F0, F1), 1: w (F0), 2: rho (F0), 3: pressure from u*,v*,w*
@@ -1625,9 +1648,10 @@ template <typename T, int R>
 __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
     Geo g, BlockInv bi, SolveTabs tb, const Task* __restrict__ tasks, T* __restrict__ F0, T* __restrict__ F1,
     T* __restrict__ F2, double rdiv, int role, int cpen, int meanu, int refine, const double* __restrict__ Dt,
-    const double* __restrict__ D2t, const double* __restrict__ zh, const double* __restrict__ wnl,
-    const double* __restrict__ wvr, int kstart) {
+    const double* __restrict__ D2t, const double* __restrict__ Lt, const double* __restrict__ zh,
+    const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart) {
   extern __shared__ __align__(16) double sm[];
+  __shared__ int cj[R], cii[R];
   const Task tk = tasks[blockIdx.x];
   const int n = g.nz, N = g.N, ns = g.ns, m = 2 * (ns - 1);
   const int tid = threadIdx.x;
@@ -1636,79 +1660,93 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
   double* rz = x + (size_t)R * n;
   double* zz = rz + (size_t)R * (m > 0 ? m : 1);
   const int per = role == 0 ? 4 : 2;
+  const int ncols = R / per;  // column slots per task
   const int s = tk.sys;
   const int ncolt = tk.count;
   const double dt = g.dt;
+  if (tid < ncols) {
+    const int c = tid < ncolt ? tb.col_order[tk.first + tid] : -1;
+    cj[tid] = c < 0 ? -1 : c / g.nxhp;
+    cii[tid] = c < 0 ? -1 : c % g.nxhp;
+  }
+  __syncthreads();
   if (s < 0 && role != 3) {  // w of the (0,0) mode is zero
-    for (int ci = 0; ci < ncolt; ++ci) {
-      const int c = tb.col_order[tk.first + ci];
-      const int j = c / g.nxhp, ii = c % g.nxhp;
+    for (int ci = 0; ci < ncolt; ++ci)
       for (int k = tid; k < n; k += kSolveThreads) {
-        F0[fidx<T>(g, 2 * ii, j, k)] = 0;
-        F0[fidx<T>(g, 2 * ii + 1, j, k)] = 0;
+        F0[fidx<T>(g, 2 * cii[ci], cj[ci], k)] = 0;
+        F0[fidx<T>(g, 2 * cii[ci] + 1, cj[ci], k)] = 0;
       }
-    }
     return;
   }
+  const double* res = x;
   if (s < 0) {  // pressure of the (0,0) mode: phi = 0
     for (int q = tid; q < R * n; q += kSolveThreads) x[q] = 0.0;
     __syncthreads();
   } else {
     const SysDesc sd = bi.sys[s];
     const double eps = sd.eps;
-    // right-hand sides
     if (role == 3) {
-      for (int q = tid; q < R * n; q += kSolveThreads) {  // w* columns into x (scratch)
-        const int r = q / n, k = q - r * n, ci = r >> 1;
-        double v = 0.0;
-        if (ci < ncolt) {
-          const int c = tb.col_order[tk.first + ci];
-          const int j = c / g.nxhp, ii = c % g.nxhp;
-          v = (double)F2[fidx<T>(g, 2 * ii + (r & 1), j, k)];
+      for (int k = tid; k < n; k += kSolveThreads) {  // w* columns into x (scratch)
+        double v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int ci = r >> 1;
+          v[r] = cj[ci] >= 0 ? (double)F2[fidx<T>(g, 2 * cii[ci] + (r & 1), cj[ci], k)] : 0.0;
         }
-        x[q] = v;
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[(size_t)r * n + k] = v[r];
       }
       __syncthreads();
-      for (int q = tid; q < R * n; q += kSolveThreads) {
-        const int r = q / n, k = q - r * n, ci = r >> 1, part = r & 1;
-        double v = 0.0;
-        if (ci < ncolt) {
-          const int c = tb.col_order[tk.first + ci];
-          const int j = c / g.nxhp, ii = c % g.nxhp;
-          const int ks = k / N, k1 = k - ks * N;
-          const double* wc = x + (size_t)r * n + ks * N;
-          double sr = 0.0;
-          for (int k2 = 0; k2 < N; ++k2) sr += __ldg(Dt + k2 * N + k1) * wc[k2];
-          const double dw = sr * g.hfac[ks];
-          const double xw = g.xw[ii], yw = g.yw[j];
-          double d;
-          if (part == 0)
-            d = -(xw * (double)F0[fidx<T>(g, 2 * ii + 1, j, k)]) - (yw * (double)F1[fidx<T>(g, 2 * ii + 1, j, k)]) + dw;
-          else
-            d = (xw * (double)F0[fidx<T>(g, 2 * ii, j, k)]) + (yw * (double)F1[fidx<T>(g, 2 * ii, j, k)]) + dw;
-          v = -((d / dt) * eps);
-          if (k == 0) {
-            const size_t p1 = (size_t)g.nxpp * j + 2 * ii + part;
-            v -= (sd.tau1_bot * (wnl[p1] + wvr[p1])) * eps;
-          }
-          if (k == n - 1) {
-            const size_t p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii + part;
-            v += (sd.tau2_top * (wnl[p2] + wvr[p2])) * eps;
-          }
+      for (int k = tid; k < n; k += kSolveThreads) {
+        const int ks = k / N, k1 = k - ks * N;
+        double dw[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) dw[r] = 0.0;
+        for (int k2 = 0; k2 < N; ++k2) {
+          const double dd = __ldg(Dt + k2 * N + k1);
+#pragma unroll
+          for (int r = 0; r < R; ++r) dw[r] += dd * x[(size_t)r * n + ks * N + k2];
         }
-        b[q] = v;
+        const double fac = g.hfac[ks];
+#pragma unroll
+        for (int ci = 0; ci < R / 2; ++ci) {
+          double vr = 0.0, vi = 0.0;
+          if (cj[ci] >= 0) {
+            const int j = cj[ci], ii = cii[ci];
+            const size_t pr = fidx<T>(g, 2 * ii, j, k);
+            const double ur = (double)F0[pr], ui = (double)F0[pr + 1];
+            const double wr = (double)F1[pr], wi = (double)F1[pr + 1];
+            const double xw = g.xw[ii], yw = g.yw[j];
+            const double dr = -(xw * ui) - (yw * wi) + dw[2 * ci] * fac;
+            const double di = (xw * ur) + (yw * wr) + dw[2 * ci + 1] * fac;
+            vr = -((dr / dt) * eps);
+            vi = -((di / dt) * eps);
+            if (k == 0) {
+              const size_t p1 = (size_t)g.nxpp * j + 2 * ii;
+              vr -= (sd.tau1_bot * (wnl[p1] + wvr[p1])) * eps;
+              vi -= (sd.tau1_bot * (wnl[p1 + 1] + wvr[p1 + 1])) * eps;
+            }
+            if (k == n - 1) {
+              const size_t p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii;
+              vr += (sd.tau2_top * (wnl[p2] + wvr[p2])) * eps;
+              vi += (sd.tau2_top * (wnl[p2 + 1] + wvr[p2 + 1])) * eps;
+            }
+          }
+          b[(size_t)(2 * ci) * n + k] = vr;
+          b[(size_t)(2 * ci + 1) * n + k] = vi;
+        }
       }
     } else {
-      for (int q = tid; q < R * n; q += kSolveThreads) {
-        const int r = q / n, k = q - r * n, ci = r / per, rr = r - ci * per;
-        double v = 0.0;
-        if (ci < ncolt) {
-          const int c = tb.col_order[tk.first + ci];
-          const int j = c / g.nxhp, ii = c % g.nxhp;
+      for (int k = tid; k < n; k += kSolveThreads) {
+        double v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int ci = r / per, rr = r - ci * per;
           const T* F = (role == 0 && rr >= 2) ? F1 : F0;
-          v = -(-((double)F[fidx<T>(g, 2 * ii + (rr & 1), j, k)] / rdiv) * eps);
+          v[r] = cj[ci] >= 0 ? (double)F[fidx<T>(g, 2 * cii[ci] + (rr & 1), cj[ci], k)] : 0.0;
         }
-        b[q] = v;
+#pragma unroll
+        for (int r = 0; r < R; ++r) b[(size_t)r * n + k] = -(-(v[r] / rdiv) * eps);
       }
     }
     __syncthreads();
@@ -1721,63 +1759,64 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
       bi_apply_cta<R>(g, ainv, lv, mi, b, x, rz, zz, true);
     }
     if (cpen) {
-      const int w = tid >> 5, lane = tid & 31;
-      for (int r = w; r < R; r += kSolveThreads / 32)
-        legen_filter_cols(x + (size_t)r * n, 1, n, N, ns, tb.wg, tb.alpol, tb.sigma, lane);
-      __syncthreads();
+      legen_filter_cta<R>(g, Lt, x, b);
+      res = b;
     }
   }
   // write back
   if (role == 3) {
-    for (int q = tid; q < (R / 2) * n; q += kSolveThreads) {
-      const int ci = q / n, k = q - ci * n;
-      if (ci >= ncolt) continue;
-      const int c = tb.col_order[tk.first + ci];
-      const int j = c / g.nxhp, ii = c % g.nxhp;
-      const size_t pr = fidx<T>(g, 2 * ii, j, k), pi = pr + 1;
-      if (k < kstart) {
-        F0[pr] = 0;
-        F0[pi] = 0;
-        F1[pr] = 0;
-        F1[pi] = 0;
-        F2[pr] = 0;
-        F2[pi] = 0;
-        continue;
+    for (int k = tid; k < n; k += kSolveThreads) {
+      const int ks = k / N, k1 = k - ks * N;
+      double dz[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) dz[r] = 0.0;
+      for (int k2 = 0; k2 < N; ++k2) {
+        const double dd = __ldg(Dt + k2 * N + k1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) dz[r] += dd * res[(size_t)r * n + ks * N + k2];
       }
-      const double* rr = x + (size_t)(2 * ci) * n;
-      const double* ri = rr + n;
-      const double phr = rr[k], phi = ri[k];
-      double wbr = 0, wbi = 0;
-      if (!(ii == 0 && j == 0)) {
-        const int ks = k / N, k1 = k - ks * N;
-        double sr = 0.0, si = 0.0;
-        for (int k2 = 0; k2 < N; ++k2) {
-          const double dd = __ldg(Dt + k2 * N + k1);
-          sr += dd * rr[ks * N + k2];
-          si += dd * ri[ks * N + k2];
+      const double fac = g.hfac[ks];
+#pragma unroll
+      for (int ci = 0; ci < R / 2; ++ci) {
+        if (cj[ci] < 0) continue;
+        const int j = cj[ci], ii = cii[ci];
+        const size_t pr = fidx<T>(g, 2 * ii, j, k), pi = pr + 1;
+        if (k < kstart) {
+          F0[pr] = 0;
+          F0[pi] = 0;
+          F1[pr] = 0;
+          F1[pi] = 0;
+          F2[pr] = 0;
+          F2[pi] = 0;
+          continue;
         }
-        const double fac = g.hfac[ks];
-        wbr = (double)F2[pr] - dt * (sr * fac);
-        wbi = (double)F2[pi] - dt * (si * fac);
+        const double phr = res[(size_t)(2 * ci) * n + k], phi = res[(size_t)(2 * ci + 1) * n + k];
+        double wbr = 0, wbi = 0;
+        if (!(ii == 0 && j == 0)) {
+          wbr = (double)F2[pr] - dt * (dz[2 * ci] * fac);
+          wbi = (double)F2[pi] - dt * (dz[2 * ci + 1] * fac);
+        }
+        const double dtx = dt * g.xw[ii], dty = dt * g.yw[j];
+        const double ur = (double)F0[pr], ui = (double)F0[pi], vr = (double)F1[pr], vi = (double)F1[pi];
+        F0[pr] = (T)(ur + dtx * phi);
+        F0[pi] = (T)(ui - dtx * phr);
+        F1[pr] = (T)(vr + dty * phi);
+        F1[pi] = (T)(vi - dty * phr);
+        F2[pr] = (T)wbr;
+        F2[pi] = (T)wbi;
       }
-      const double dtx = dt * g.xw[ii], dty = dt * g.yw[j];
-      F0[pr] = (T)((double)F0[pr] + dtx * phi);
-      F0[pi] = (T)((double)F0[pi] - dtx * phr);
-      F1[pr] = (T)((double)F1[pr] + dty * phi);
-      F1[pi] = (T)((double)F1[pi] - dty * phr);
-      F2[pr] = (T)wbr;
-      F2[pi] = (T)wbi;
     }
   } else {
-    for (int q = tid; q < R * n; q += kSolveThreads) {
-      const int r = q / n, k = q - r * n, ci = r / per, rr = r - ci * per;
-      if (ci >= ncolt) continue;
-      const int c = tb.col_order[tk.first + ci];
-      const int j = c / g.nxhp, ii = c % g.nxhp;
-      T* F = (role == 0 && rr >= 2) ? F1 : F0;
-      double v = x[q];
-      if (role == 0 && rr < 2 && meanu && ii == 0 && j == 0) v = tb.meang[k] * v;
-      F[fidx<T>(g, 2 * ii + (rr & 1), j, k)] = (T)v;
+    for (int k = tid; k < n; k += kSolveThreads) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int ci = r / per, rr = r - ci * per;
+        if (cj[ci] < 0) continue;
+        T* F = (role == 0 && rr >= 2) ? F1 : F0;
+        double v = res[(size_t)r * n + k];
+        if (role == 0 && rr < 2 && meanu && cii[ci] == 0 && cj[ci] == 0) v = tb.meang[k] * v;
+        F[fidx<T>(g, 2 * cii[ci] + (rr & 1), cj[ci], k)] = (T)v;
+      }
     }
   }
 }
