@@ -1,7 +1,8 @@
 // Shared-memory FFT building blocks for sm_100a.
 //
 // Complex FFTs of length M (M = 2^a 3^b 5^c) are done as Stockham autosort
-// passes (radix 4, 2, 3, 5) on data held in shared memory; a thread block
+// passes (radix 16, 8, 4, 2, 3, 5; the power-of-two radices are
+// in-register DFTs) on data held in shared memory; a thread block
 // works on a batch of independent transforms at once, one butterfly per
 // thread per pass.  Real transforms of length N = 2M use the half-length
 // complex transform plus the usual even/odd split.  Twiddles come from tables
@@ -52,6 +53,21 @@ __device__ __forceinline__ C cmul_mi(C a, bool inv) {
   return inv ? cmk<C>(-a.y, a.x) : cmk<C>(a.y, -a.x);
 }
 
+// Asynchronous global -> shared copy of one complex value (8 or 16 bytes,
+// naturally aligned), so that a CTA can put all of its loads in flight before
+// waiting once.
+template <typename C>
+__device__ __forceinline__ void cp_async_c(C* smem, const C* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if (sizeof(C) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // Plan of one complex length; radices in pass order.
 struct FftPlan {
   int M;
@@ -62,12 +78,86 @@ struct FftPlan {
   int nssh[12];     // log2(ns) if a power of two, else -1
 };
 
-// One Stockham pass over `nb` batched transforms stored contiguously
-// (stride M) in src, written to dst.  W[e] = exp(-2 pi i e / M).
+// v * w with w = c - i s (forward) or c + i s (inverse)
 template <typename C>
-__device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restrict__ dst, int M, int R,
-                                         int Ns, int nbatch, const C* __restrict__ W, bool inv, int tid,
-                                         int nthr, int nbsh, int nssh) {
+__device__ __forceinline__ C crot(C v, decltype(C().x) c, decltype(C().x) s, bool inv) {
+  const decltype(C().x) t = inv ? s : -s;
+  return cmk<C>(v.x * c - v.y * t, v.x * t + v.y * c);
+}
+
+// In-register DFT of v[0..R-1] (natural order in and out) for R = 2, 4, 8, 16.
+// R = 8 and 16 are split 2x4 and 4x4 (n = a + q b, k = c + p d).  The
+// constants are cos/sin of multiples of pi/8.
+template <typename C>
+__device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3, bool inv) {
+  C t0 = cadd(a0, a2), t1 = csub(a0, a2);
+  C t2 = cadd(a1, a3), t3 = cmul_mi(csub(a1, a3), inv);
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+template <typename C, int R>
+__device__ __forceinline__ void dft_reg(C* v, bool inv) {
+  typedef decltype(C().x) T;
+  const T h = (T)0.70710678118654752440;   // cos(pi/4)
+  const T c8 = (T)0.92387953251128675613;  // cos(pi/8)
+  const T s8 = (T)0.38268343236508977173;  // sin(pi/8)
+  if (R == 2) {
+    C t = v[0];
+    v[0] = cadd(t, v[1]);
+    v[1] = csub(t, v[1]);
+  } else if (R == 4) {
+    dft4(v[0], v[1], v[2], v[3], inv);
+  } else if (R == 8) {
+    // a in {0,1}: DFT4 over v[a + 2b]
+    dft4(v[0], v[2], v[4], v[6], inv);
+    dft4(v[1], v[3], v[5], v[7], inv);
+    // twiddle w8^c on the a = 1 half (c = 1..3 sit at v[3], v[5], v[7])
+    v[3] = crot(v[3], h, h, inv);
+    v[5] = cmul_mi(v[5], inv);
+    v[7] = crot(v[7], -h, h, inv);
+    C o[8];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      o[c] = cadd(v[2 * c], v[2 * c + 1]);
+      o[c + 4] = csub(v[2 * c], v[2 * c + 1]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = o[i];
+  } else if (R == 16) {
+    // a = 0..3: DFT4 over v[a + 4b] -> T[a][c] stored at v[a + 4c]
+#pragma unroll
+    for (int a = 0; a < 4; ++a) dft4(v[a], v[a + 4], v[a + 8], v[a + 12], inv);
+    // twiddles w16^(a c)
+    v[5] = crot(v[5], c8, s8, inv);      // a1 c1: e1
+    v[9] = crot(v[9], h, h, inv);        // a1 c2: e2
+    v[13] = crot(v[13], s8, c8, inv);    // a1 c3: e3
+    v[6] = crot(v[6], h, h, inv);        // a2 c1: e2
+    v[10] = cmul_mi(v[10], inv);         // a2 c2: e4
+    v[14] = crot(v[14], -h, h, inv);     // a2 c3: e6
+    v[7] = crot(v[7], s8, c8, inv);      // a3 c1: e3
+    v[11] = crot(v[11], -h, h, inv);     // a3 c2: e6
+    v[15] = crot(v[15], -c8, -s8, inv);  // a3 c3: e9
+    // c = 0..3: DFT4 over a of v[a + 4c] -> X[c + 4d]
+#pragma unroll
+    for (int c = 0; c < 4; ++c) dft4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3], inv);
+    C o[16];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int d = 0; d < 4; ++d) o[c + 4 * d] = v[4 * c + d];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = o[i];
+  }
+}
+
+// One Stockham pass of radix R over `nbatch` transforms stored contiguously
+// (stride M) in src, written to dst.  W[e] = exp(-2 pi i e / M).
+template <typename C, int R>
+__device__ __forceinline__ void fft_pass_r(const C* __restrict__ src, C* __restrict__ dst, int M, int Ns, int nbatch,
+                                           const C* __restrict__ W, bool inv, int tid, int nthr, int nbsh, int nssh) {
   const int nb = M / R;
   const int total = nb * nbatch;
   const int step = M / (Ns * R);
@@ -76,52 +166,42 @@ __device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restric
     const int j = w - b * nb;
     const C* s = src + (size_t)b * M;
     C* d = dst + (size_t)b * M;
-    C v[5];
+    C v[R];
     const int jq = nssh >= 0 ? (j >> nssh) : (j / Ns);
     const int jm = j - jq * Ns;
 #pragma unroll
-    for (int r = 0; r < 5; ++r)
-      if (r < R) v[r] = s[j + r * nb];
+    for (int r = 0; r < R; ++r) v[r] = s[j + r * nb];
     if (Ns > 1) {
+      const int e = jm * step;
 #pragma unroll
-      for (int r = 1; r < 5; ++r)
-        if (r < R) {
-          C tw = W[r * jm * step];  // r*jm*step < R*Ns*step = M
-          if (inv) tw.y = -tw.y;
-          v[r] = cmul(v[r], tw);
-        }
+      for (int r = 1; r < R; ++r) {
+        C tw = W[r * e];  // r*jm*step < R*Ns*step = M
+        if (inv) tw.y = -tw.y;
+        v[r] = cmul(v[r], tw);
+      }
     }
-    C o[5];
-    if (R == 4) {
-      C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-      C t2 = cadd(v[1], v[3]), t3 = cmul_mi(csub(v[1], v[3]), inv);
-      o[0] = cadd(t0, t2);
-      o[2] = csub(t0, t2);
-      o[1] = cadd(t1, t3);
-      o[3] = csub(t1, t3);
-    } else if (R == 2) {
-      o[0] = cadd(v[0], v[1]);
-      o[1] = csub(v[0], v[1]);
-    } else {
+    if (R == 3 || R == 5) {
       const int q0 = M / R;
+      C o[R];
 #pragma unroll
-      for (int q = 0; q < 5; ++q)
-        if (q < R) {
-          C acc = v[0];
+      for (int q = 0; q < R; ++q) {
+        C acc = v[0];
 #pragma unroll
-          for (int p = 1; p < 5; ++p)
-            if (p < R) {
-              C tw = W[((p * q) % R) * q0];
-              if (inv) tw.y = -tw.y;
-              acc = cadd(acc, cmul(v[p], tw));
-            }
-          o[q] = acc;
+        for (int p = 1; p < R; ++p) {
+          C tw = W[((p * q) % R) * q0];
+          if (inv) tw.y = -tw.y;
+          acc = cadd(acc, cmul(v[p], tw));
         }
+        o[q] = acc;
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = o[r];
+    } else {
+      dft_reg<C, R>(v, inv);
     }
     const int base = jq * Ns * R + jm;
 #pragma unroll
-    for (int r = 0; r < 5; ++r)
-      if (r < R) d[base + r * Ns] = o[r];
+    for (int r = 0; r < R; ++r) d[base + r * Ns] = v[r];
   }
 }
 
@@ -132,7 +212,15 @@ __device__ C* fft_run(C* a, C* b, const FftPlan& pl, int nbatch, const C* W, boo
   C* src = a;
   C* dst = b;
   for (int p = 0; p < pl.npass; ++p) {
-    fft_pass<C>(src, dst, pl.M, pl.rad[p], pl.ns[p], nbatch, W, inv, tid, nthr, pl.nbsh[p], pl.nssh[p]);
+    const int R = pl.rad[p], Ns = pl.ns[p], bs = pl.nbsh[p], ss = pl.nssh[p];
+    switch (R) {
+      case 16: fft_pass_r<C, 16>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
+      case 8: fft_pass_r<C, 8>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
+      case 4: fft_pass_r<C, 4>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
+      case 2: fft_pass_r<C, 2>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
+      case 3: fft_pass_r<C, 3>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
+      default: fft_pass_r<C, 5>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
+    }
     __syncthreads();
     C* t = src;
     src = dst;

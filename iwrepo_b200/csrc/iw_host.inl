@@ -237,13 +237,18 @@ FftPlan make_plan(int M) {
     ns *= r;
     p.npass++;
   };
-  while (m % 4 == 0) {
-    push(4);
-    m /= 4;
-  }
+  // powers of two: ceil(a/4) passes, bits spread evenly (512 -> 8*8*8, 256 -> 16*16)
+  int a2 = 0;
   while (m % 2 == 0) {
-    push(2);
     m /= 2;
+    ++a2;
+  }
+  if (a2 > 0) {
+    const int np = (a2 + 3) / 4;
+    for (int q = 0; q < np; ++q) {
+      const int bits = a2 / np + (q < a2 % np ? 1 : 0);
+      push(1 << bits);
+    }
   }
   while (m % 3 == 0) {
     push(3);
@@ -915,7 +920,7 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
       a.f_amp_r = (xa * um) * (-(1 / om)) * bz * bz * (h->p.rho0 / h->p.grav) * (um / zdim) * ph;
     }
     a.dx = (pi2_of(h) / (pi2_of(h) / h->p.xlen)) / h->nx;
-    size_t smem = 2 * 20 * (size_t)M * sizeof(C);
+    size_t smem = 2 * 20 * (size_t)(M + 1) * sizeof(C);
     cudaFuncSetAttribute(k_xrow_nl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid(h->ny, h->nz);
     k_xrow_nl<T><<<grid, 256, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);
@@ -1127,7 +1132,7 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
     return set_err(IW_ERR_CONFIG, "ny: need 1 or even with radices 2,3,5");
   if (d.nzloc < 3 || d.nzloc > 48) return set_err(IW_ERR_CONFIG, "nzloc outside [3,48]");
   if (d.nsubd < 1 || d.nsubd > IW_MAX_SUBD) return set_err(IW_ERR_CONFIG, "nsubd outside [1,64]");
-  if ((size_t)d.nx / 2 * 20 * 2 * 16 > 220 * 1024 && prm->precision == IW_PREC_FP64)
+  if (((size_t)d.nx / 2 + 1) * 20 * 2 * 16 > 227 * 1024 && prm->precision == IW_PREC_FP64)
     return set_err(IW_ERR_CONFIG, "nx too large for the FP64 row kernel");
   double zsum = 0;
   for (int k = 0; k < d.nsubd; ++k) {

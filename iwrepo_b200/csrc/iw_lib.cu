@@ -171,25 +171,27 @@ __global__ void k_yfft(Geo g, YJobs<T> jobs, int nplanes, FftPlan pl, const type
   const bool two = jb.mode == 3;
   (void)ntile;
   (void)nplanes;
-  // load: A[b*ny + j] = column (ii0+b), row j
+  // load: A[b*ny + j] = column (ii0+b), row j (all copies in flight at once)
   for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
     int b = t % TX, j = t / TX;
     int ii = ii0 + b;
-    C v = cmk<C>(0, 0), v2 = cmk<C>(0, 0);
     if (ii < g.nxhp) {
-      const T* p = jb.src + fidx<T>(g, 2 * ii, j, k);
-      v = cmk<C>(p[0], p[1]);
-      if (two) {
-        const T* p2 = jb.src2 + fidx<T>(g, 2 * ii, j, k);
-        v2 = cmk<C>(p2[0], p2[1]);
-      }
-      if (jb.mode == 1) {
-        T ky = (T)g.yw[j];
-        v = cmk<C>(-(ky * v.y), ky * v.x);
-      }
+      cp_async_c<C>(A + b * ny + j, (const C*)(jb.src + fidx<T>(g, 2 * ii, j, k)));
+      if (two) cp_async_c<C>(A2 + b * ny + j, (const C*)(jb.src2 + fidx<T>(g, 2 * ii, j, k)));
+    } else {
+      A[b * ny + j] = cmk<C>(0, 0);
+      if (two) A2[b * ny + j] = cmk<C>(0, 0);
     }
-    A[b * ny + j] = v;
-    if (two) A2[b * ny + j] = v2;
+  }
+  cp_async_wait_all();
+  if (jb.mode == 1) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
+      int b = t % TX, j = t / TX;
+      T ky = (T)g.yw[j];
+      C v = A[b * ny + j];
+      A[b * ny + j] = cmk<C>(-(ky * v.y), ky * v.x);
+    }
   }
   __syncthreads();
   C* res = A;
@@ -215,9 +217,7 @@ __global__ void k_yfft(Geo g, YJobs<T> jobs, int nplanes, FftPlan pl, const type
       T ky = (T)g.yw[j];
       o = cmk<C>(o.x - ky * w2.y, o.y + ky * w2.x);
     }
-    T* p = jb.dst + fidx<T>(g, 2 * ii, j, k);
-    p[0] = o.x;
-    p[1] = o.y;
+    *(C*)(jb.dst + fidx<T>(g, 2 * ii, j, k)) = o;
   }
 }
 
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(256) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl,
   extern __shared__ __align__(16) unsigned char smraw[];
   const int M = g.nx / 2;
   C* A = (C*)smraw;
-  C* B = A + 20 * M;
+  C* B = A + 20 * (M + 1);  // both buffers hold 20 rows of M+1 values
   const int j = blockIdx.x, k = blockIdx.y;
   const int N = g.N;
   const int kl = k % N, ks = k / N;
@@ -294,27 +294,20 @@ __global__ void __launch_bounds__(256) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl,
   const int knb = nb_lo ? k - 1 : k + 1;
   const int nrow = 16 + ((nb_lo || nb_hi) ? 4 : 0);
   const T kxs = (T)g.xw[1];
-  // rows 0..3 u v w t, 4..7 dx, 8..11 dy, 12..15 dz, 16..19 neighbour u v w t
-  for (int r = 0; r < nrow; ++r) {
-    const T* src;
-    int mk = 0;
-    size_t off;
-    if (r < 4) {
-      src = a.in[r];
-      off = fidx<T>(g, 0, j, k);
-    } else if (r < 8) {
-      src = a.in[r - 4];
-      mk = 1;
-      off = fidx<T>(g, 0, j, k);
-    } else if (r < 16) {
-      src = a.in[r - 4];
-      off = fidx<T>(g, 0, j, k);
-    } else {
-      src = a.in[r - 16];
-      off = fidx<T>(g, 0, j, knb);
-    }
-    xinv_prep<C, T>(src + off, A + r * M, M, Wn, mk, kxs, threadIdx.x, blockDim.x);
+  // rows 0..3 u v w t, 4..7 dx, 8..11 dy, 12..15 dz, 16..19 neighbour u v w t.
+  // Raw half-complex rows (M+1 values) are staged in B, all copies in flight.
+  const int nxhp = M + 1;
+  C* raw = B;
+  for (int q = threadIdx.x; q < nrow * nxhp; q += blockDim.x) {
+    const int r = q / nxhp, kk = q - r * nxhp;
+    const T* src = r < 4 ? a.in[r] : r < 8 ? a.in[r - 4] : r < 16 ? a.in[r - 4] : a.in[r - 16];
+    const int kr = r < 16 ? k : knb;
+    cp_async_c<C>(raw + q, (const C*)(src + fidx<T>(g, 2 * kk, j, kr)));
   }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int r = 0; r < nrow; ++r)
+    xinv_prep<C, T>((const T*)(raw + r * nxhp), A + r * M, M, Wn, r >= 4 && r < 8, kxs, threadIdx.x, blockDim.x);
   __syncthreads();
   C* ph = fft_run<C>(A, B, pl, nrow, Wm, true, threadIdx.x, blockDim.x);
   C* pr = (ph == A) ? B : A;  // products go to the other buffer
@@ -396,9 +389,7 @@ __global__ void __launch_bounds__(256) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl,
       const int src_row[7] = {5, 8, 9, 10, 6, 11, 12};
       val = xfwd_post<C>(sp + src_row[o - 4] * M, kk, M, Wn, invN);
     }
-    T* p = a.out[o] + fidx<T>(g, 2 * kk, j, k);
-    p[0] = val.x;
-    p[1] = val.y;
+    *(C*)(a.out[o] + fidx<T>(g, 2 * kk, j, k)) = val;
   }
 }
 
