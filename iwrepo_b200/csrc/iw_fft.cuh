@@ -1,7 +1,7 @@
 // Shared-memory FFT building blocks for sm_100a.
 //
 // Complex FFTs of length M (M = 2^a 3^b 5^c) are done as Stockham autosort
-// passes (radix 16, 8, 4, 2, 3, 5; the power-of-two radices are
+// passes (radix 8, 4, 2, 3, 5; the power-of-two radices are
 // in-register DFTs) on data held in shared memory; a thread block
 // works on a batch of independent transforms at once, one butterfly per
 // thread per pass.  Real transforms of length N = 2M use the half-length
@@ -85,9 +85,8 @@ __device__ __forceinline__ C crot(C v, decltype(C().x) c, decltype(C().x) s, boo
   return cmk<C>(v.x * c - v.y * t, v.x * t + v.y * c);
 }
 
-// In-register DFT of v[0..R-1] (natural order in and out) for R = 2, 4, 8, 16.
-// R = 8 and 16 are split 2x4 and 4x4 (n = a + q b, k = c + p d).  The
-// constants are cos/sin of multiples of pi/8.
+// In-register DFT of v[0..R-1] (natural order in and out) for R = 2, 4, 8.
+// R = 8 is split 2x4 (n = a + 2b, k = c + 4d); h = cos(pi/4).
 template <typename C>
 __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3, bool inv) {
   C t0 = cadd(a0, a2), t1 = csub(a0, a2);
@@ -102,8 +101,6 @@ template <typename C, int R>
 __device__ __forceinline__ void dft_reg(C* v, bool inv) {
   typedef decltype(C().x) T;
   const T h = (T)0.70710678118654752440;   // cos(pi/4)
-  const T c8 = (T)0.92387953251128675613;  // cos(pi/8)
-  const T s8 = (T)0.38268343236508977173;  // sin(pi/8)
   if (R == 2) {
     C t = v[0];
     v[0] = cadd(t, v[1]);
@@ -126,30 +123,6 @@ __device__ __forceinline__ void dft_reg(C* v, bool inv) {
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i) v[i] = o[i];
-  } else if (R == 16) {
-    // a = 0..3: DFT4 over v[a + 4b] -> T[a][c] stored at v[a + 4c]
-#pragma unroll
-    for (int a = 0; a < 4; ++a) dft4(v[a], v[a + 4], v[a + 8], v[a + 12], inv);
-    // twiddles w16^(a c)
-    v[5] = crot(v[5], c8, s8, inv);      // a1 c1: e1
-    v[9] = crot(v[9], h, h, inv);        // a1 c2: e2
-    v[13] = crot(v[13], s8, c8, inv);    // a1 c3: e3
-    v[6] = crot(v[6], h, h, inv);        // a2 c1: e2
-    v[10] = cmul_mi(v[10], inv);         // a2 c2: e4
-    v[14] = crot(v[14], -h, h, inv);     // a2 c3: e6
-    v[7] = crot(v[7], s8, c8, inv);      // a3 c1: e3
-    v[11] = crot(v[11], -h, h, inv);     // a3 c2: e6
-    v[15] = crot(v[15], -c8, -s8, inv);  // a3 c3: e9
-    // c = 0..3: DFT4 over a of v[a + 4c] -> X[c + 4d]
-#pragma unroll
-    for (int c = 0; c < 4; ++c) dft4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3], inv);
-    C o[16];
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-      for (int d = 0; d < 4; ++d) o[c + 4 * d] = v[4 * c + d];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = o[i];
   }
 }
 
@@ -214,7 +187,6 @@ __device__ C* fft_run(C* a, C* b, const FftPlan& pl, int nbatch, const C* W, boo
   for (int p = 0; p < pl.npass; ++p) {
     const int R = pl.rad[p], Ns = pl.ns[p], bs = pl.nbsh[p], ss = pl.nssh[p];
     switch (R) {
-      case 16: fft_pass_r<C, 16>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
       case 8: fft_pass_r<C, 8>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
       case 4: fft_pass_r<C, 4>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
       case 2: fft_pass_r<C, 2>(src, dst, pl.M, Ns, nbatch, W, inv, tid, nthr, bs, ss); break;
@@ -228,5 +200,105 @@ __device__ C* fft_run(C* a, C* b, const FftPlan& pl, int nbatch, const C* W, boo
   }
   return src;
 }
+
+
+// ---------------------------------------------------------------------------
+// Warp-synchronous in-place transforms.  One warp owns one transform of length
+// M held in shared memory with one pad slot after every 16 values (index
+// fpad(i)), which keeps the strided Stockham stores free of bank conflicts.
+// Every pass loads all of its butterflies into registers, then stores them:
+// no second buffer and no CTA-wide barrier.  DPT >= M/32 values per lane.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
+// slots needed for L padded values
+__host__ __device__ __forceinline__ int fpadlen(int L) { return L > 0 ? fpad(L - 1) + 1 : 0; }
+
+template <typename C, int R, int NB>
+__device__ __forceinline__ void fft_pass_w(C* row, int M, int Ns, const C* __restrict__ W, bool inv, int lane,
+                                           int nssh) {
+  const int nb = M / R;
+  const int step = M / (Ns * R);
+  C v[NB][R];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int j = lane + 32 * q;
+    if (j < nb) {
+      const int jq = nssh >= 0 ? (j >> nssh) : (j / Ns);
+      const int jm = j - jq * Ns;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q][r] = row[fpad(j + r * nb)];
+      if (Ns > 1) {
+        const int e = jm * step;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C tw = W[r * e];
+          if (inv) tw.y = -tw.y;
+          v[q][r] = cmul(v[q][r], tw);
+        }
+      }
+      if (R == 3 || R == 5) {
+        const int q0 = M / R;
+        C o[R];
+#pragma unroll
+        for (int qq = 0; qq < R; ++qq) {
+          C acc = v[q][0];
+#pragma unroll
+          for (int p = 1; p < R; ++p) {
+            C tw = W[((p * qq) % R) * q0];
+            if (inv) tw.y = -tw.y;
+            acc = cadd(acc, cmul(v[q][p], tw));
+          }
+          o[qq] = acc;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[q][r] = o[r];
+      } else {
+        dft_reg<C, R>(v[q], inv);
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int j = lane + 32 * q;
+    if (j < nb) {
+      const int jq = nssh >= 0 ? (j >> nssh) : (j / Ns);
+      const int jm = j - jq * Ns;
+      const int base = jq * Ns * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) row[fpad(base + r * Ns)] = v[q][r];
+    }
+  }
+  __syncwarp();
+}
+
+// In-place transform of one padded row by one warp (all lanes call it).
+// POW2: the length is a power of two, so only radix 8, 4, 2 passes are
+// compiled (every compiled radix raises the register count of the kernel).
+template <typename C, int DPT, bool POW2>
+__device__ __forceinline__ void fft_warp(C* row, const FftPlan& pl, const C* __restrict__ W, bool inv, int lane) {
+  for (int p = 0; p < pl.npass; ++p) {
+    const int Ns = pl.ns[p], ss = pl.nssh[p];
+    switch (pl.rad[p]) {
+      case 8: fft_pass_w<C, 8, (DPT + 7) / 8>(row, pl.M, Ns, W, inv, lane, ss); break;
+      case 4: fft_pass_w<C, 4, (DPT + 3) / 4>(row, pl.M, Ns, W, inv, lane, ss); break;
+      case 2: fft_pass_w<C, 2, (DPT + 1) / 2>(row, pl.M, Ns, W, inv, lane, ss); break;
+      default:
+        if (!POW2) {
+          if (pl.rad[p] == 3)
+            fft_pass_w<C, 3, (DPT + 2) / 3>(row, pl.M, Ns, W, inv, lane, ss);
+          else
+            fft_pass_w<C, 5, (DPT + 4) / 5>(row, pl.M, Ns, W, inv, lane, ss);
+        }
+        break;
+    }
+  }
+}
+
+// minimum resident CTAs of 256 threads for a warp-transform kernel
+template <typename T, int DPT>
+struct FftOcc {
+  static constexpr int v = sizeof(T) == 4 ? (DPT <= 8 ? 4 : DPT <= 16 ? 2 : 1) : (DPT <= 4 ? 4 : DPT <= 8 ? 2 : 1);
+};
 
 }  // namespace iw

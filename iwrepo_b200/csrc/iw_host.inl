@@ -237,14 +237,16 @@ FftPlan make_plan(int M) {
     ns *= r;
     p.npass++;
   };
-  // powers of two: ceil(a/4) passes, bits spread evenly (512 -> 8*8*8, 256 -> 16*16)
+  // powers of two: ceil(a/3) passes of radix <= 8, bits spread evenly
+  // (512 -> 8*8*8, 256 -> 8*8*4); larger radices cost more registers than
+  // they save in passes
   int a2 = 0;
   while (m % 2 == 0) {
     m /= 2;
     ++a2;
   }
   if (a2 > 0) {
-    const int np = (a2 + 3) / 4;
+    const int np = (a2 + 2) / 3;
     for (int q = 0; q < np; ++q) {
       const int bits = a2 / np + (q < a2 % np ? 1 : 0);
       push(1 << bits);
@@ -817,39 +819,55 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   k_stageE<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c);
 }
 
+// values per lane of a warp transform of length M
+static int fft_dpt(int M) {
+  const int d = (M + 31) / 32;
+  return d <= 4 ? 4 : d <= 8 ? 8 : d <= 16 ? 16 : 32;
+}
+
 template <typename T>
-static int ytx(const iw_handle* h) {  // y-FFT tile width
-  size_t cs = 2 * sizeof(T);
+static int ytx(const iw_handle* h, bool two) {  // y-FFT tile width
+  const size_t cs = 2 * sizeof(T);
   int tx = 8;
-  while (tx > 1 && 4 * (size_t)tx * h->ny * cs > 200 * 1024) tx /= 2;
+  while (tx > 1 && (two ? 2 : 1) * (size_t)tx * ystride(h->ny) * cs > 110 * 1024) tx /= 2;
   return tx;
+}
+
+template <typename T, int TX>
+static void launch_y_tx(iw_handle* h, YJobs<T>& jobs, dim3 grid, size_t smem, int nplanes,
+                        const typename cplx_t<T>::type* Wy) {
+  Geo g = geo(h);
+  const bool p2 = (h->ny & (h->ny - 1)) == 0;
+  switch (fft_dpt(h->ny) * (p2 ? 1 : -1)) {
+#define IW_YCASE(D, P)                                                                                       \
+  case (P ? D : -D):                                                                                         \
+    cudaFuncSetAttribute(k_yfft<T, TX, D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+    k_yfft<T, TX, D, P><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, Wy);                          \
+    break;
+    IW_YCASE(4, true)
+    IW_YCASE(8, true)
+    IW_YCASE(16, true)
+    IW_YCASE(32, true)
+    IW_YCASE(4, false)
+    IW_YCASE(8, false)
+    IW_YCASE(16, false)
+    IW_YCASE(32, false)
+#undef IW_YCASE
+  }
 }
 
 template <typename T>
 static void launch_y(iw_handle* h, FieldSet<T>& fs, YJobs<T>& jobs, int njobs, int nplanes, bool four) {
   typedef typename cplx_t<T>::type C;
-  int tx = ytx<T>(h);
-  int ntile = (h->nxhp + tx - 1) / tx;
+  const int tx = ytx<T>(h, four);
+  const int ntile = (h->nxhp + tx - 1) / tx;
   dim3 grid(ntile, nplanes, njobs);
-  size_t smem = (four ? 4 : 2) * (size_t)tx * h->ny * sizeof(C);
-  Geo g = geo(h);
+  const size_t smem = (four ? 2 : 1) * (size_t)tx * ystride(h->ny) * sizeof(C);
   switch (tx) {
-    case 8:
-      cudaFuncSetAttribute(k_yfft<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_yfft<T, 8><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
-      break;
-    case 4:
-      cudaFuncSetAttribute(k_yfft<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_yfft<T, 4><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
-      break;
-    case 2:
-      cudaFuncSetAttribute(k_yfft<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_yfft<T, 2><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
-      break;
-    default:
-      cudaFuncSetAttribute(k_yfft<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_yfft<T, 1><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, fs.Wy);
-      break;
+    case 8: launch_y_tx<T, 8>(h, jobs, grid, smem, nplanes, fs.Wy); break;
+    case 4: launch_y_tx<T, 4>(h, jobs, grid, smem, nplanes, fs.Wy); break;
+    case 2: launch_y_tx<T, 2>(h, jobs, grid, smem, nplanes, fs.Wy); break;
+    default: launch_y_tx<T, 1>(h, jobs, grid, smem, nplanes, fs.Wy); break;
   }
 }
 
@@ -920,10 +938,25 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
       a.f_amp_r = (xa * um) * (-(1 / om)) * bz * bz * (h->p.rho0 / h->p.grav) * (um / zdim) * ph;
     }
     a.dx = (pi2_of(h) / (pi2_of(h) / h->p.xlen)) / h->nx;
-    size_t smem = 2 * 20 * (size_t)(M + 1) * sizeof(C);
-    cudaFuncSetAttribute(k_xrow_nl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = 20 * (size_t)xstride(M) * sizeof(C);
     dim3 grid(h->ny, h->nz);
-    k_xrow_nl<T><<<grid, 256, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);
+    const bool p2 = (M & (M - 1)) == 0;
+    switch (fft_dpt(M) * (p2 ? 1 : -1)) {
+#define IW_XCASE(D, P)                                                                                   \
+  case (P ? D : -D):                                                                                     \
+    cudaFuncSetAttribute(k_xrow_nl<T, D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+    k_xrow_nl<T, D, P><<<grid, 256, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);                        \
+    break;
+      IW_XCASE(4, true)
+      IW_XCASE(8, true)
+      IW_XCASE(16, true)
+      IW_XCASE(32, true)
+      IW_XCASE(4, false)
+      IW_XCASE(8, false)
+      IW_XCASE(16, false)
+      IW_XCASE(32, false)
+#undef IW_XCASE
+    }
   }
   mark(h, 2);
   // K_D: y-forward; B_q = Y(A_q) + i ky Y(P_q), Z_q = Y(P_zq)
@@ -1132,8 +1165,13 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
     return set_err(IW_ERR_CONFIG, "ny: need 1 or even with radices 2,3,5");
   if (d.nzloc < 3 || d.nzloc > 48) return set_err(IW_ERR_CONFIG, "nzloc outside [3,48]");
   if (d.nsubd < 1 || d.nsubd > IW_MAX_SUBD) return set_err(IW_ERR_CONFIG, "nsubd outside [1,64]");
-  if (((size_t)d.nx / 2 + 1) * 20 * 2 * 16 > 227 * 1024 && prm->precision == IW_PREC_FP64)
-    return set_err(IW_ERR_CONFIG, "nx too large for the FP64 row kernel");
+  {
+    const size_t cs = prm->precision == IW_PREC_FP64 ? 16 : 8;
+    if (20 * (size_t)xstride(d.nx / 2) * cs > 227 * 1024 || d.nx / 2 > 1024)
+      return set_err(IW_ERR_CONFIG, "nx too large for the row kernel (20 rows of nx/2+1 values in shared memory)");
+    if ((size_t)ystride(d.ny) * cs > 110 * 1024 || d.ny > 1024)
+      return set_err(IW_ERR_CONFIG, "ny too large for the y-transform kernel");
+  }
   double zsum = 0;
   for (int k = 0; k < d.nsubd; ++k) {
     if (!(prm->zh[k] > 0)) return set_err(IW_ERR_CONFIG, "subdomain height must be positive");

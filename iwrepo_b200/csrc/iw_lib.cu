@@ -154,67 +154,73 @@ struct YJobs {
   YJob<T> j[16];
 };
 
-template <typename T, int TX>
-__global__ void k_yfft(Geo g, YJobs<T> jobs, int nplanes, FftPlan pl, const typename cplx_t<T>::type* __restrict__ Wy) {
+// slots per padded y column: >= fpadlen(ny) and = 2 (mod 16), so that the
+// TX columns of a tile sit in different banks
+__host__ __device__ __forceinline__ int ystride(int ny) {
+  int s = fpadlen(ny);
+  return s + ((2 - s) % 16 + 16) % 16;
+}
+
+template <typename T, int TX, int DPT, bool POW2>
+__global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<T> jobs, int nplanes, FftPlan pl,
+                                              const typename cplx_t<T>::type* __restrict__ Wy) {
   typedef typename cplx_t<T>::type C;
   extern __shared__ __align__(16) unsigned char smraw[];
+  const int ny = g.ny;
+  const int RSY = ystride(ny);
   C* A = (C*)smraw;
-  C* B = A + (size_t)TX * g.ny;
-  C* A2 = B + (size_t)TX * g.ny;
-  C* B2 = A2 + (size_t)TX * g.ny;
+  C* A2 = A + (size_t)TX * RSY;
   const YJob<T> jb = jobs.j[blockIdx.z];
   const int k = blockIdx.y;
-  const int ntile = (g.nxhp + TX - 1) / TX;  // includes the Nyquist column
   const int ii0 = blockIdx.x * TX;
-  const int ny = g.ny;
   const bool fwd = jb.mode >= 2;
   const bool two = jb.mode == 3;
-  (void)ntile;
   (void)nplanes;
-  // load: A[b*ny + j] = column (ii0+b), row j (all copies in flight at once)
+  // load: column ii0+b, row j -> A[b*RSY + fpad(j)] (all copies in flight at once)
   for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
-    int b = t % TX, j = t / TX;
-    int ii = ii0 + b;
+    const int b = t % TX, j = t / TX;
+    const int ii = ii0 + b;
+    C* d = A + b * RSY + fpad(j);
     if (ii < g.nxhp) {
-      cp_async_c<C>(A + b * ny + j, (const C*)(jb.src + fidx<T>(g, 2 * ii, j, k)));
-      if (two) cp_async_c<C>(A2 + b * ny + j, (const C*)(jb.src2 + fidx<T>(g, 2 * ii, j, k)));
+      cp_async_c<C>(d, (const C*)(jb.src + fidx<T>(g, 2 * ii, j, k)));
+      if (two) cp_async_c<C>(d + TX * RSY, (const C*)(jb.src2 + fidx<T>(g, 2 * ii, j, k)));
     } else {
-      A[b * ny + j] = cmk<C>(0, 0);
-      if (two) A2[b * ny + j] = cmk<C>(0, 0);
+      *d = cmk<C>(0, 0);
+      if (two) d[TX * RSY] = cmk<C>(0, 0);
     }
   }
   cp_async_wait_all();
+  __syncthreads();
   if (jb.mode == 1) {
-    __syncthreads();
     for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
-      int b = t % TX, j = t / TX;
-      T ky = (T)g.yw[j];
-      C v = A[b * ny + j];
-      A[b * ny + j] = cmk<C>(-(ky * v.y), ky * v.x);
+      const int b = t % TX, j = t / TX;
+      const T ky = (T)g.yw[j];
+      C* d = A + b * RSY + fpad(j);
+      const C v = *d;
+      *d = cmk<C>(-(ky * v.y), ky * v.x);
     }
+    __syncthreads();
+  }
+  // the x-Nyquist column (ii = nxh) is not transformed
+  const int nb = ny > 1 ? max(0, min(TX, g.nxh - ii0)) : 0;
+  const int nrow = two ? 2 * nb : nb;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = threadIdx.x >> 5; r < nrow; r += nw) {
+    C* row = r < nb ? A + r * RSY : A2 + (r - nb) * RSY;
+    fft_warp<C, DPT, POW2>(row, pl, Wy, !fwd, lane);
   }
   __syncthreads();
-  C* res = A;
-  C* res2 = A2;
-  int nb = min(TX, g.nxh - ii0);  // transformed columns in this tile
-  if (nb > 0 && ny > 1) {
-    res = fft_run<C>(A, B, pl, nb, Wy, !fwd, threadIdx.x, blockDim.x);
-    if (two) res2 = fft_run<C>(A2, B2, pl, nb, Wy, !fwd, threadIdx.x, blockDim.x);
-  }
-  // the Nyquist column (ii = nxh) stays where it was: copy it if the
-  // transform wrote the result to the other buffer
   const T sc = fwd ? (T)g.scaley : (T)1;
   for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
-    int b = t % TX, j = t / TX;
-    int ii = ii0 + b;
+    const int b = t % TX, j = t / TX;
+    const int ii = ii0 + b;
     if (ii >= g.nxhp) continue;
-    bool tr = (ii < g.nxh) && ny > 1;
-    C v = tr ? res[b * ny + j] : A[b * ny + j];
+    const C v = A[b * RSY + fpad(j)];
     C o = cmk<C>(v.x * sc, v.y * sc);
     if (two) {
-      C v2 = tr ? res2[b * ny + j] : A2[b * ny + j];
-      C w2 = cmk<C>(v2.x * sc, v2.y * sc);
-      T ky = (T)g.yw[j];
+      const C v2 = A2[b * RSY + fpad(j)];
+      const C w2 = cmk<C>(v2.x * sc, v2.y * sc);
+      const T ky = (T)g.yw[j];
       o = cmk<C>(o.x - ky * w2.y, o.y + ky * w2.x);
     }
     *(C*)(jb.dst + fidx<T>(g, 2 * ii, j, k)) = o;
@@ -277,15 +283,64 @@ struct NLArgs {
   double dx;
 };
 
-// K_C: CTA per (j,k) row.  smem: two buffers of 20 rows of M complex.
-template <typename T>
-__global__ void __launch_bounds__(256) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl, const typename cplx_t<T>::type* __restrict__ Wm,
+// In-place pre-pass of the inverse real transform for the pair (kk, M-kk) of a
+// padded row holding X_0..X_M: Z_k = (X_k + conj X_{M-k}) + i conj(W_k) (X_k - conj X_{M-k}),
+// after the optional multiplication by i kx.  0 <= kk <= M/2.
+template <typename C, typename T>
+__device__ __forceinline__ void xprep_pair(C* row, int kk, int M, const C* __restrict__ Wn, bool mulkx, T kxstep) {
+  const int km = M - kk;
+  const C X0 = row[fpad(kk)], X1 = row[fpad(km)];
+  auto zk = [&](C Xk, C Xm, int k) {
+    if (mulkx) {
+      const T a = kxstep * (T)k, b = kxstep * (T)(M - k);
+      Xk = cmk<C>(-(a * Xk.y), a * Xk.x);
+      Xm = cmk<C>(-(b * Xm.y), b * Xm.x);
+    }
+    if (k == 0) {
+      Xk.y = 0;
+      Xm.y = 0;
+    }
+    const C s = cadd(Xk, cconj(Xm));
+    const C d = csub(Xk, cconj(Xm));
+    const C t = cmul(cconj(Wn[k]), d);
+    return cmk<C>(s.x - t.y, s.y + t.x);
+  };
+  const C z0 = zk(X0, X1, kk);
+  if (kk > 0 && kk < km) row[fpad(km)] = zk(X1, X0, km);
+  row[fpad(kk)] = z0;
+}
+
+// forward post on a padded row: Z = FFT_M(z) -> X_k, k = 0..M (scaled by 1/N)
+template <typename C>
+__device__ __forceinline__ C xfwd_post_p(const C* row, int k, int M, const C* __restrict__ Wn,
+                                         decltype(C().x) invN) {
+  typedef decltype(C().x) T;
+  if (k == 0 || k == M) {
+    const C z = row[0];
+    return k == 0 ? cmk<C>((z.x + z.y) * invN, (T)0) : cmk<C>((z.x - z.y) * invN, (T)0);
+  }
+  const C a = row[fpad(k)], b = cconj(row[fpad(M - k)]);
+  const C e = cmk<C>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y + b.y));
+  const C dd = csub(a, b);
+  const C o = cmk<C>((T)0.5 * dd.y, (T)-0.5 * dd.x);  // (a-b)/(2i)
+  const C wo = cmul(Wn[k], o);
+  return cmk<C>((e.x + wo.x) * invN, (e.y + wo.y) * invN);
+}
+
+// slots per padded x row (M+1 half-complex values)
+__host__ __device__ __forceinline__ int xstride(int M) { return fpadlen(M + 1); }
+
+// K_C: CTA per (j,k) row; 20 padded rows of M+1 values in shared memory; each
+// warp transforms whole rows in place.
+template <typename T, int DPT, bool POW2>
+__global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl,
+                                                 const typename cplx_t<T>::type* __restrict__ Wm,
                                                  const typename cplx_t<T>::type* __restrict__ Wn) {
   typedef typename cplx_t<T>::type C;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int M = g.nx / 2;
-  C* A = (C*)smraw;
-  C* B = A + 20 * (M + 1);  // both buffers hold 20 rows of M+1 values
+  const int RS = xstride(M);
+  C* buf = (C*)smraw;
   const int j = blockIdx.x, k = blockIdx.y;
   const int N = g.N;
   const int kl = k % N, ks = k / N;
@@ -294,57 +349,52 @@ __global__ void __launch_bounds__(256) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl,
   const int knb = nb_lo ? k - 1 : k + 1;
   const int nrow = 16 + ((nb_lo || nb_hi) ? 4 : 0);
   const T kxs = (T)g.xw[1];
-  // rows 0..3 u v w t, 4..7 dx, 8..11 dy, 12..15 dz, 16..19 neighbour u v w t.
-  // Raw half-complex rows (M+1 values) are staged in B, all copies in flight.
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
+  // rows 0..3 u v w t, 4..7 dx, 8..11 dy, 12..15 dz, 16..19 neighbour u v w t:
+  // half-complex rows (M+1 values), all copies in flight at once
   const int nxhp = M + 1;
-  C* raw = B;
-  for (int q = threadIdx.x; q < nrow * nxhp; q += blockDim.x) {
+  for (int q = tid; q < nrow * nxhp; q += nthr) {
     const int r = q / nxhp, kk = q - r * nxhp;
     const T* src = r < 4 ? a.in[r] : r < 8 ? a.in[r - 4] : r < 16 ? a.in[r - 4] : a.in[r - 16];
     const int kr = r < 16 ? k : knb;
-    cp_async_c<C>(raw + q, (const C*)(src + fidx<T>(g, 2 * kk, j, kr)));
+    cp_async_c<C>(buf + r * RS + fpad(kk), (const C*)(src + fidx<T>(g, 2 * kk, j, kr)));
   }
   cp_async_wait_all();
   __syncthreads();
-  for (int r = 0; r < nrow; ++r)
-    xinv_prep<C, T>((const T*)(raw + r * nxhp), A + r * M, M, Wn, r >= 4 && r < 8, kxs, threadIdx.x, blockDim.x);
+  const int nh = M / 2 + 1;
+  for (int q = tid; q < nrow * nh; q += nthr) {
+    const int r = q / nh, kk = q - r * nh;
+    xprep_pair<C, T>(buf + r * RS, kk, M, Wn, r >= 4 && r < 8, kxs);
+  }
   __syncthreads();
-  C* ph = fft_run<C>(A, B, pl, nrow, Wm, true, threadIdx.x, blockDim.x);
-  C* pr = (ph == A) ? B : A;  // products go to the other buffer
-  const T* P = (const T*)ph;   // physical row r: P[r*2M + i]
-  T* Q = (T*)pr;
+  for (int r = wid; r < nrow; r += nw) fft_warp<C, DPT, POW2>(buf + r * RS, pl, Wm, true, lane);
+  __syncthreads();
+  // physical value i of row r
+  auto P = [&](int r, int i) -> T& { return ((T*)(buf + r * RS))[2 * fpad(i >> 1) + (i & 1)]; };
   const int nx = g.nx;
-  // upwind interface penalty (solver.f:700-839)
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    T u = P[0 * nx + i], v = P[1 * nx + i], w = P[2 * nx + i], t = P[3 * nx + i];
-    T ux = P[4 * nx + i], vx = P[5 * nx + i], wx = P[6 * nx + i], tx = P[7 * nx + i];
-    T uy = P[8 * nx + i], vy = P[9 * nx + i], wy = P[10 * nx + i];
-    T uz = P[12 * nx + i], vz = P[13 * nx + i], wz = P[14 * nx + i];
-    (void)tx;
+  // upwind interface penalty (solver.f:700-839); products overwrite rows 0..12
+  for (int i = tid; i < nx; i += nthr) {
+    const T u = P(0, i), v = P(1, i), w = P(2, i), t = P(3, i);
+    const T ux = P(4, i), vx = P(5, i), wx = P(6, i);
+    const T uy = P(8, i), vy = P(9, i), wy = P(10, i);
+    const T uz = P(12, i), vz = P(13, i), wz = P(14, i);
     T qu = (T)-0.5 * (u * ux + v * uy + w * uz);
     T qv = (T)-0.5 * (u * vx + v * vy + w * vz);
     T qw = (T)-0.5 * (u * wx + v * wy + w * wz) + (T)a.coef_buoy * t;
     T qt = -(w * (T)a.rg);
-    if (kl == 0 && k > 0) {
-      // bottom point of subdomain ks: inflow from below when w > 0
-      if (w > (T)0) {
-        T tau = (T)a.tau_pen[ks];
-        T al = w;
-        qu -= tau * (al * u - al * P[16 * nx + i]);
-        qv -= tau * (al * v - al * P[17 * nx + i]);
-        qw -= tau * (al * w - al * P[18 * nx + i]);
-        qt -= tau * (al * t - al * P[19 * nx + i]);
-      }
+    if (nb_lo && w > (T)0) {  // bottom point of subdomain ks: inflow from below
+      const T tau = (T)a.tau_pen[ks], al = w;
+      qu -= tau * (al * u - al * P(16, i));
+      qv -= tau * (al * v - al * P(17, i));
+      qw -= tau * (al * w - al * P(18, i));
+      qt -= tau * (al * t - al * P(19, i));
     }
-    if (kl == N - 1 && k < g.nz - 1) {
-      if (w < (T)0) {
-        T tau = (T)a.tau_pen[ks];
-        T ga = -w;
-        qu -= tau * (ga * u - ga * P[16 * nx + i]);
-        qv -= tau * (ga * v - ga * P[17 * nx + i]);
-        qw -= tau * (ga * w - ga * P[18 * nx + i]);
-        qt -= tau * (ga * t - ga * P[19 * nx + i]);
-      }
+    if (nb_hi && w < (T)0) {
+      const T tau = (T)a.tau_pen[ks], ga = -w;
+      qu -= tau * (ga * u - ga * P(16, i));
+      qv -= tau * (ga * v - ga * P(17, i));
+      qw -= tau * (ga * w - ga * P(18, i));
+      qt -= tau * (ga * t - ga * P(19, i));
     }
     if (a.forcing) {
       double xx = (double)i * a.dx, zz = g.zg[k];
@@ -357,37 +407,38 @@ __global__ void __launch_bounds__(256) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl,
       qt += (T)(a.f_amp_r * szm * sf);
     }
     // 13 rows to transform: Qu Qv Qw Qt | uu uv uw ut | vv vw vt | ww wt
-    Q[0 * nx + i] = qu;
-    Q[1 * nx + i] = qv;
-    Q[2 * nx + i] = qw;
-    Q[3 * nx + i] = qt;
-    Q[4 * nx + i] = (T)-0.5 * u * u;
-    Q[5 * nx + i] = (T)-0.5 * u * v;
-    Q[6 * nx + i] = (T)-0.5 * u * w;
-    Q[7 * nx + i] = -(u * t);
-    Q[8 * nx + i] = (T)-0.5 * v * v;
-    Q[9 * nx + i] = (T)-0.5 * v * w;
-    Q[10 * nx + i] = -(v * t);
-    Q[11 * nx + i] = (T)-0.5 * w * w;
-    Q[12 * nx + i] = -(w * t);
+    P(0, i) = qu;
+    P(1, i) = qv;
+    P(2, i) = qw;
+    P(3, i) = qt;
+    P(4, i) = (T)-0.5 * u * u;
+    P(5, i) = (T)-0.5 * u * v;
+    P(6, i) = (T)-0.5 * u * w;
+    P(7, i) = -(u * t);
+    P(8, i) = (T)-0.5 * v * v;
+    P(9, i) = (T)-0.5 * v * w;
+    P(10, i) = -(v * t);
+    P(11, i) = (T)-0.5 * w * w;
+    P(12, i) = -(w * t);
   }
   __syncthreads();
-  C* sp = fft_run<C>(pr, ph, pl, 13, Wm, false, threadIdx.x, blockDim.x);
+  for (int r = wid; r < 13; r += nw) fft_warp<C, DPT, POW2>(buf + r * RS, pl, Wm, false, lane);
+  __syncthreads();
   const T invN = (T)1 / (T)nx;
   // outputs: A_q = X(Q_q) + i kx X(P_uq) for q = u v w t ; then uv vv vw vt uw ww wt
   const int nout = M + 1;
-  for (int t = threadIdx.x; t < 11 * nout; t += blockDim.x) {
-    int o = t / nout, kk = t % nout;
+  for (int t = tid; t < 11 * nout; t += nthr) {
+    const int o = t / nout, kk = t - o * nout;
     C val;
     if (o < 4) {
-      C x1 = xfwd_post<C>(sp + o * M, kk, M, Wn, invN);
-      C x2 = xfwd_post<C>(sp + (4 + o) * M, kk, M, Wn, invN);
-      T kx = kxs * (T)kk;
+      const C x1 = xfwd_post_p<C>(buf + o * RS, kk, M, Wn, invN);
+      const C x2 = xfwd_post_p<C>(buf + (4 + o) * RS, kk, M, Wn, invN);
+      const T kx = kxs * (T)kk;
       val = cmk<C>(x1.x - kx * x2.y, x1.y + kx * x2.x);
     } else {
       // map: 4->uv(5) 5->vv(8) 6->vw(9) 7->vt(10) 8->uw(6) 9->ww(11) 10->wt(12)
-      const int src_row[7] = {5, 8, 9, 10, 6, 11, 12};
-      val = xfwd_post<C>(sp + src_row[o - 4] * M, kk, M, Wn, invN);
+      const int sr = o == 4 ? 5 : o == 5 ? 8 : o == 6 ? 9 : o == 7 ? 10 : o == 8 ? 6 : o == 9 ? 11 : 12;
+      val = xfwd_post_p<C>(buf + sr * RS, kk, M, Wn, invN);
     }
     *(C*)(a.out[o] + fidx<T>(g, 2 * kk, j, k)) = val;
   }
