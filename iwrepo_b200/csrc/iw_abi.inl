@@ -173,8 +173,8 @@ void calcuvwt_(const int* izmode, const int* ispecfilter, const int* irelax, con
   (void)irelax;
   iw_handle* h = bound();
   if (!h) return;
-  if (ensure_factors(h)) return;
   int cpen = cpenspecfilter ? (*cpenspecfilter != 0) : 1;
+  if (ensure_factors(h, cpen)) return;
   if (h->mixed)
     calcuvwt_impl<float>(h, h->f32, cpen);
   else

@@ -331,6 +331,8 @@ struct iw_handle {
   struct BI {
     void* ainv = 0;
     double *cvec = 0, *dvec = 0, *minv = 0, *pen = 0, *lvec = 0;
+    double* ainv_raw = 0;  // unfiltered inverses of systems [0, nsys_raw) when ainv has the filter folded in
+    int nsys_raw = 0;
     SysDesc* sys = 0;
     int* colsys = 0;
     int nsys = 0;
@@ -339,8 +341,13 @@ struct iw_handle {
   // grouped solve tasks per kind (columns sharing a system, <= G per task)
   Task* dtasks[SYS_KINDS] = {0, 0, 0, 0};
   int ntask[SYS_KINDS] = {0, 0, 0, 0};
+  std::vector<Task> htasks[SYS_KINDS];
+  // tasks [0, nrefine) get one FP64 residual sweep: their systems have an
+  // estimated condition number above kRefineCond (small kx^2+ky^2 pressure)
+  int nrefine[SYS_KINDS] = {0, 0, 0, 0};
   double bi_bdfv[SYS_KINDS] = {-1, -1, -1, -1};
   bool bi_f32[SYS_KINDS] = {false, false, false, false};
+  bool bi_fold[SYS_KINDS] = {false, false, false, false};  // Legendre filter folded into ainv
   double bi_dt[SYS_KINDS] = {-1, -1, -1, -1};
   double fac_bdfv[SYS_KINDS] = {-1, -1, -1, -1};  // bdfv the factors were built for
   double fac_dt[SYS_KINDS] = {-1, -1, -1, -1};
@@ -522,6 +529,9 @@ static int kind_bcs(const iw_handle* h, int kind, int& bot, int& top) {
 
 // tasks: runs of the sorted column order that share one system, split into
 // pieces of at most G columns
+// systems above this estimated condition number get a residual sweep
+constexpr double kRefineCond = 1e5;
+
 static int build_tasks(iw_handle* h, int kind, const std::vector<int>& colsys, int G) {
   std::vector<int> order(h->ncol);
   for (int c = 0; c < h->ncol; ++c) order[c] = c;
@@ -539,6 +549,7 @@ static int build_tasks(iw_handle* h, int kind, const std::vector<int>& colsys, i
   h->dtasks[kind] = nullptr;
   if (up(h, &h->dtasks[kind], tasks)) return IW_ERR_NOMEM;
   h->ntask[kind] = (int)tasks.size();
+  h->htasks[kind] = tasks;
   return 0;
 }
 
@@ -663,7 +674,7 @@ static void enumerate_systems(iw_handle* h, int kind, std::vector<SysDesc>& sys,
 }
 
 // block inverses (FP32 for the mixed path, FP64 otherwise) of one kind
-static int build_blockinv(iw_handle* h, int kind) {
+static int build_blockinv(iw_handle* h, int kind, bool fold) {
   const int ns = h->ns, N = h->N, n = h->nz, ldab = 3 * N + 1, m = 2 * (ns - 1);
   const bool f32 = false;  // the solves run in FP64 in both precisions
   const size_t tib = f32 ? sizeof(float) : sizeof(double);
@@ -680,6 +691,7 @@ static int build_blockinv(iw_handle* h, int kind) {
     cudaFree(B.minv);
     cudaFree(B.pen);
     cudaFree(B.lvec);
+    cudaFree(B.ainv_raw);
     cudaFree(B.sys);
     cudaFree(B.colsys);
     B = iw_handle::BI();
@@ -701,6 +713,30 @@ static int build_blockinv(iw_handle* h, int kind) {
   CK(scopy(h, B.colsys, colsys.data(), colsys.size() * sizeof(int), cudaMemcpyHostToDevice));
   if (build_tasks(h, kind, colsys, kind == SYS_U ? 1 : 2)) return IW_ERR_NOMEM;
   h->bi_f32[kind] = f32;
+  {
+    // cond(I - eps (2/h)^2 D2 + penalty) <~ 1 + eps max_ks (2/h_ks)^2 |D2|_inf
+    double d2n = 0;
+    for (int k1 = 0; k1 < N; ++k1) {
+      double rs = 0;
+      for (int k = 0; k < N; ++k) rs += std::fabs(h->tab.D2[(size_t)k1 * N + k]);
+      d2n = std::max(d2n, rs);
+    }
+    double hmin = 1e300;
+    for (int ks = 0; ks < ns; ++ks) hmin = std::min(hmin, h->p.zh[ks]);
+    const double rho = d2n * (2.0 / hmin) * (2.0 / hmin);
+    int last = -1;
+    const auto& tk = h->htasks[kind];
+    for (int t = 0; t < (int)tk.size(); ++t)
+      if (tk[t].sys >= 0 && 1.0 + sys[tk[t].sys].eps * rho > kRefineCond) last = t;
+    h->nrefine[kind] = last + 1;
+    int nraw = 0;
+    if (fold)
+      for (int t = 0; t <= last; ++t) nraw = std::max(nraw, tk[t].sys + 1);
+    cudaFree(B.ainv_raw);
+    B.ainv_raw = nullptr;
+    B.nsys_raw = nraw;
+    if (nraw > 0 && dalloc(h, &B.ainv_raw, (size_t)nraw * ns * N * N)) return IW_ERR_NOMEM;
+  }
   // chunked: assemble -> invert blocks -> interface matrix -> store
   const int CH = std::max(1, std::min(nsys, (int)(1200000000ull / ((size_t)ldab * n * 8 + (size_t)ns * N * N * 8 + 1))));
   double *tab = nullptr, *tinv = nullptr, *twork = nullptr;
@@ -738,8 +774,14 @@ static int build_blockinv(iw_handle* h, int kind) {
       k_left_vecs<<<1184, 256, 0, h->st>>>(g, cn, tinv, B.cvec + (size_t)s0 * ns * N, B.dvec + (size_t)s0 * ns * N,
                                          B.lvec + (size_t)s0 * m * N);
     const size_t cnt = (size_t)cn * ns * N * N;
+    if (fold && s0 < B.nsys_raw)
+      CK(cudaMemcpyAsync(B.ainv_raw + (size_t)s0 * ns * N * N, tinv,
+                         (size_t)(std::min(B.nsys_raw, s0 + cn) - s0) * ns * N * N * sizeof(double),
+                         cudaMemcpyDeviceToDevice, h->st));
     if (f32)
       k_convert<double, float><<<2048, 256, 0, h->st>>>(tinv, (float*)B.ainv + (size_t)s0 * ns * N * N, cnt);
+    else if (fold)
+      k_fold_filter<<<2368, 256, 0, h->st>>>(N, (size_t)cn * ns, h->dL, tinv, (double*)B.ainv + (size_t)s0 * ns * N * N);
     else
       CK(cudaMemcpyAsync((double*)B.ainv + (size_t)s0 * ns * N * N, tinv, cnt * sizeof(double),
                          cudaMemcpyDeviceToDevice, h->st));
@@ -752,14 +794,19 @@ static int build_blockinv(iw_handle* h, int kind) {
   cudaFree(tinfo);
   h->bi_bdfv[kind] = h->c.bdfv;
   h->bi_dt[kind] = h->p.dt;
+  h->bi_fold[kind] = fold;
   return 0;
 }
 
-static int ensure_factors(iw_handle* h) {
+// cpen: whether the coming solves filter their solutions.  The filter is
+// folded into the block inverses only when it runs every step.
+static int ensure_factors(iw_handle* h, int cpen) {
   if (h->use_bi) {
+    const bool fold = cpen && h->p.ispecfilterexp == 1 && h->p.nspecfilterexp == 1;
     for (int k = SYS_P; k <= SYS_T; ++k)
-      if (h->bi_dt[k] != h->p.dt || (k != SYS_P && h->bi_bdfv[k] != h->c.bdfv) || h->bi_dt[k] < 0) {
-        int r = build_blockinv(h, k);
+      if (h->bi_dt[k] != h->p.dt || (k != SYS_P && h->bi_bdfv[k] != h->c.bdfv) || h->bi_dt[k] < 0 ||
+          h->bi_fold[k] != fold) {
+        int r = build_blockinv(h, k, fold);
         if (r) return r;
       }
   }
@@ -1016,7 +1063,6 @@ template <typename T>
 static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, int kstart) {
   constexpr int R = 4;
   const int kind = role == 0 ? SYS_U : role == 1 ? SYS_W : role == 2 ? SYS_T : SYS_P;
-  const int refine = kind == SYS_P ? 1 : 0;  // the pressure can be ill conditioned (eps = 1/k^2)
   BlockInv bi;
   bi.ainv = h->bi[kind].ainv;
   bi.cvec = h->bi[kind].cvec;
@@ -1043,10 +1089,26 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   const double rd = role == 2 ? h->p.dt * h->p.xkappa : h->p.xnu * h->p.dt;
   const int meanu = role == 0 ? h->p.meanu_damping : 0;
   if (sm > 48 * 1024) cudaFuncSetAttribute(k_solve_cta<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (h->ntask[kind] > 0)
-    k_solve_cta<T, R><<<h->ntask[kind], kSolveThreads, sm, h->st>>>(
-        geo(h), bi, solve_tabs(h, kind), h->dtasks[kind], F0, F1, F2, rd, role, cpen, meanu, refine, h->dDt, h->dD2t,
-        h->dLt, h->dzh, h->dwnl, h->dwvr, kstart);
+  // refined prefix, then the rest
+  // With the filter folded into ainv, the refined prefix uses the unfiltered
+  // copy and the filter pass; the rest needs no filter pass.
+  const int nref = h->nrefine[kind], nt = h->ntask[kind];
+  const bool fold = h->bi_fold[kind] && cpen;
+  for (int part = 0; part < 2; ++part) {
+    const int t0 = part == 0 ? 0 : nref, cnt = part == 0 ? nref : nt - nref;
+    if (cnt <= 0) continue;
+    BlockInv b2 = bi;
+    int cp = cpen;
+    if (fold) {
+      if (part == 0)
+        b2.ainv = h->bi[kind].ainv_raw;
+      else
+        cp = 0;
+    }
+    k_solve_cta<T, R><<<cnt, kSolveThreads, sm, h->st>>>(geo(h), b2, solve_tabs(h, kind), h->dtasks[kind] + t0, F0, F1,
+                                                          F2, rd, role, cp, meanu, part == 0 ? 1 : 0, h->dDt, h->dD2t,
+                                                          h->dLt, h->dzh, h->dwnl, h->dwvr, kstart);
+  }
 }
 
 // calcuvwt (calcuvwt_noslip.f / calcuvwt.f) on u*,v*,w*,rho* held in F.
@@ -1132,11 +1194,11 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
 template <typename T>
 static int full_step(iw_handle* h, FieldSet<T>& fs) {
   h->istep += 1;
-  int r = ensure_factors(h);
+  const int cpen = (h->p.ispecfilterexp == 1) && (h->istep % h->p.nspecfilterexp == 0);
+  int r = ensure_factors(h, cpen);
   if (r) return r;
   convec_impl<T>(h, fs, 1);
   schedule_after_convec(h);
-  const int cpen = (h->p.ispecfilterexp == 1) && (h->istep % h->p.nspecfilterexp == 0);
   calcuvwt_impl<T>(h, fs, cpen);
   h->c.bdfv = (h->istep < 2) ? 1.5 : 11. / 6.;
   h->t = h->t + h->p.dt;
@@ -1296,6 +1358,7 @@ int iw_destroy(iw_handle* h) {
     cudaFree(h->bi[k].minv);
     cudaFree(h->bi[k].pen);
     cudaFree(h->bi[k].lvec);
+    cudaFree(h->bi[k].ainv_raw);
     cudaFree(h->bi[k].sys);
     cudaFree(h->bi[k].colsys);
     cudaFree(h->dab[k]);

@@ -1863,6 +1863,21 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
   }
 }
 
+// out[blk][c][kk] = sum_j L[kk][j] in[blk][c][j]: the per-subdomain Legendre
+// filter folded into stored block inverses (L row major, N*N).
+__global__ void k_fold_filter(int N, size_t nblk, const double* __restrict__ L, const double* __restrict__ in,
+                              double* __restrict__ out) {
+  const size_t tot = nblk * N * N;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    const int kk = (int)(q % N);
+    const double* col = in + (q - kk);
+    const double* lr = L + (size_t)kk * N;
+    double acc = 0.0;
+    for (int j = 0; j < N; ++j) acc += lr[j] * col[j];
+    out[q] = acc;
+  }
+}
+
 // lvec[s][e][c] = sum_k A_blk^-1[k][c] v_e[k]: v_e = c_{e+1} on block e (e < ns-1),
 // d_t on block t+1 (e = ns-1+t).  One thread per (system, e, c).
 __global__ void k_left_vecs(Geo g, int nsys, const double* __restrict__ ainv, const double* __restrict__ cvec,
