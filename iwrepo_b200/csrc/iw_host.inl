@@ -839,13 +839,49 @@ static SolveTabs solve_tabs(iw_handle* h, int kind) {
 // ---------------------------------------------------------------------------
 // the step
 // ---------------------------------------------------------------------------
+// operator bucket of the register-column kernels (0: use the tiled kernels)
+static int zop_bucket(int N) {
+  for (int nm : {9, 17, 21, 25, 29, 33})
+    if (N <= nm) return nm;
+  return 0;
+}
+
+template <typename T, int NM>
+static ZOp<T, NM> make_zop(const iw_handle* h) {
+  ZOp<T, NM> op;
+  memset(&op, 0, sizeof op);
+  for (int k1 = 0; k1 < h->N; ++k1)
+    for (int k2 = 0; k2 < h->N; ++k2) {
+      op.D[k1 * NM + k2] = (T)h->tab.D[(size_t)k1 * h->N + k2];
+      op.L[k1 * NM + k2] = (T)h->tab.Lfil[(size_t)k1 * h->N + k2];
+    }
+  return op;
+}
+
+template <typename T, int NM>
+static void launch_stageA_r(iw_handle* h, FieldSet<T>& fs, int proj) {
+  dim3 grid((unsigned)((h->plane + 127) / 128), (unsigned)h->ns, 4);
+  k_stageA_r<T, NM><<<grid, 128, 0, h->st>>>(geo(h), make_zop<T, NM>(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.F1[0],
+                                             fs.F1[1], fs.F1[2], fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj);
+}
+
 template <typename T>
 static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
+  switch (zop_bucket(h->N)) {
+    case 9: launch_stageA_r<T, 9>(h, fs, proj); return;
+    case 17: launch_stageA_r<T, 17>(h, fs, proj); return;
+    case 21: launch_stageA_r<T, 21>(h, fs, proj); return;
+    case 25: launch_stageA_r<T, 25>(h, fs, proj); return;
+    case 29: launch_stageA_r<T, 29>(h, fs, proj); return;
+    case 33: launch_stageA_r<T, 33>(h, fs, proj); return;
+    default: break;
+  }
   dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
   size_t smem = (size_t)(h->N * h->N + h->N * kTX) * sizeof(T);
   k_stageA<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.F1[0], fs.F1[1],
                                                 fs.F1[2], fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj);
 }
+
 template <typename T>
 static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   EArgs<T> a;
@@ -861,6 +897,24 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   }
   a.wnl = h->dwnl;
   a.filter = h->p.ispecfilternl == 1;
+  const dim3 rgrid((unsigned)((h->plane + 127) / 128), (unsigned)h->ns, 4);
+  // The register-column stage E holds two columns per thread; past these sizes
+  // its register count costs more occupancy than the tiled kernel loses.
+  const int emax = sizeof(T) == 4 ? 25 : 17;
+  switch (h->N <= emax ? zop_bucket(h->N) : 0) {
+#define IW_ECASE(NM)                                                                          \
+  case NM:                                                                                    \
+    k_stageE_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, make_zop<T, NM>(h));         \
+    return;
+    IW_ECASE(9)
+    IW_ECASE(17)
+    IW_ECASE(21)
+    IW_ECASE(25)
+    IW_ECASE(29)
+    IW_ECASE(33)
+#undef IW_ECASE
+    default: break;
+  }
   dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
   size_t smem = (size_t)(2 * h->N * h->N + 2 * h->N * kTX) * sizeof(T);
   k_stageE<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c);

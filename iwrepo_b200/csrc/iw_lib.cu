@@ -537,6 +537,145 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-column variants of K_A and K_E for N <= 33.  A thread owns one
+// (x, y) point of one subdomain and keeps its N values of the column in
+// registers; thread t addresses element t of every z-plane, so each warp
+// reads and writes 128-byte contiguous runs.  The N x N operators (D and the
+// precombined filter, zero-padded to NM x NM) are kernel parameters, i.e. they
+// sit in the constant bank, and the fully unrolled products take them as
+// immediate operands: about one instruction per multiply-add.
+// ---------------------------------------------------------------------------
+template <typename T, int NM>
+struct ZOp {
+  T D[NM * NM];  // D[k1*NM + k2], zero outside N x N
+  T L[NM * NM];  // precombined Legendre filter, same layout
+};
+
+template <typename T, int NM>
+__global__ void __launch_bounds__(128) k_stageA_r(Geo g, const __grid_constant__ ZOp<T, NM> op,
+                                                   const T* __restrict__ F0, const T* __restrict__ F1_,
+                                                   const T* __restrict__ F2_, const T* __restrict__ F3_,
+                                                   T* __restrict__ O0, T* __restrict__ O1, T* __restrict__ O2,
+                                                   T* __restrict__ O3, T* __restrict__ Z0, T* __restrict__ Z1,
+                                                   T* __restrict__ Z2, T* __restrict__ Z3, int proj) {
+  const int q = blockIdx.z, ks = blockIdx.y, N = g.N;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.plane) return;
+  const int i = (int)(t % g.nxpp), j = (int)(t / g.nxpp);
+  const T* F = q == 0 ? F0 : q == 1 ? F1_ : q == 2 ? F2_ : F3_;
+  T* O = q == 0 ? O0 : q == 1 ? O1 : q == 2 ? O2 : O3;
+  T* Z = q == 0 ? Z0 : q == 1 ? Z1 : q == 2 ? Z2 : Z3;
+  const bool wzero = q == 2 && j == 0 && i < 2;  // wc(1,1,:) = 0, solver.f:66-69
+  T col[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k) {
+    T x = 0;
+    if (k < N) {
+      const int kk = ks * N + k;
+      x = proj ? proj_val<T>(g, F, i, j, kk) : F[(size_t)kk * g.plane + t];
+      if (wzero) x = (T)0;
+      O[(size_t)kk * g.plane + t] = x;
+    }
+    col[k] = x;
+  }
+  const T fac = (T)g.hfac[ks];
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1) {
+    if (k1 < N) {
+      T s = 0;
+#pragma unroll
+      for (int k2 = 0; k2 < NM; ++k2) s += op.D[k1 * NM + k2] * col[k2];
+      Z[(size_t)(ks * N + k1) * g.plane + t] = s * fac;
+    }
+  }
+}
+
+template <typename T, int NM>
+__global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, const __grid_constant__ ZOp<T, NM> op) {
+  const int q = blockIdx.z, ks = blockIdx.y, N = g.N;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.plane) return;
+  const int i = (int)(t % g.nxpp), j = (int)(t / g.nxpp);
+  T zc[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k) zc[k] = k < N ? a.Z[q][(size_t)(ks * N + k) * g.plane + t] : (T)0;
+  const T fac = (T)g.hfac[ks];
+  const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
+  const T* Bq = a.B[q];
+  const T* Snq = a.Snold[q];
+  const T* F1q = a.F1[q];
+  const T* Fnq = a.Fn[q];
+  T* Snmq = a.Snm_w[q];
+  T* Fnmq = a.Fnm_w[q];
+  // Rolling window: the inputs of row k1+PF are loaded before the stores of
+  // row k1, so the loads of several rows are in flight at once (the pointers
+  // are not known to be distinct, so the compiler would not hoist them).
+  constexpr int PF = 4;
+  T wb[PF], wsn[PF], wsnm[PF], wf2[PF], wfn[PF], wfnm[PF];
+#pragma unroll
+  for (int k1 = 0; k1 < PF; ++k1) {
+    if (k1 < N) {
+      const int kk = ks * N + k1;
+      const size_t p = (size_t)kk * g.plane + t;
+      wb[k1] = Bq[p];
+      wsn[k1] = Snq[p];
+      wsnm[k1] = Snmq[p];
+      wf2[k1] = proj_val<T>(g, F1q, i, j, kk);
+      wfn[k1] = Fnq[p];
+      wfnm[k1] = Fnmq[p];
+    }
+  }
+  T fs[NM];
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1) {
+    T fsv = 0;
+    if (k1 < N) {
+      const int sl = k1 % PF;
+      const T b = wb[sl], sn = wsn[sl], snm = wsnm[sl], F2 = wf2[sl], fn = wfn[sl], fnm = wfnm[sl];
+      if (k1 + PF < NM && k1 + PF < N) {
+        const int kn = ks * N + k1 + PF;
+        const size_t pn = (size_t)kn * g.plane + t;
+        wb[sl] = Bq[pn];
+        wsn[sl] = Snq[pn];
+        wsnm[sl] = Snmq[pn];
+        wf2[sl] = proj_val<T>(g, F1q, i, j, kn);
+        wfn[sl] = Fnq[pn];
+        wfnm[sl] = Fnmq[pn];
+      }
+      const int kk = ks * N + k1;
+      const size_t p = (size_t)kk * g.plane + t;
+      T s = 0;
+#pragma unroll
+      for (int k2 = 0; k2 < NM; ++k2) s += op.D[k1 * NM + k2] * zc[k2];
+      const T S = b + s * fac;
+      if (q == 2 && ((kk == 0) || (kk == g.nz - 1)))
+        a.wnl[t + (kk == 0 ? 0 : g.plane)] = (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
+      const T se = f1 * S + f2 * sn + f3 * snm;
+      fsv = (T)c.dt * se + (T)c.bdf1 * F2 + (T)c.bdf2 * fn + (T)c.bdf3 * fnm;
+      Snmq[p] = S;
+      Fnmq[p] = F2;
+    }
+    fs[k1] = fsv;
+  }
+  const T cf = a.filter ? (T)g.cfour[(size_t)j * g.nxhp + (i >> 1)] : (T)1;
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1) {
+    if (k1 < N) {
+      T o;
+      if (a.filter) {
+        T s = 0;
+#pragma unroll
+        for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * fs[k2];
+        o = cf * s;
+      } else {
+        o = fs[k1];
+      }
+      a.F[q][(size_t)(ks * N + k1) * g.plane + t] = o;
+    }
+  }
+}
+
 // rotational viscous term at the walls (solver.f:318-394, rotvisc 1210-1253):
 // wviscrot = -nu * (fac1 rot(n) + fac2 rot(n-1) + fac3 rot(n-2)),
 // rot = (kx^2+ky^2) w + i kx du/dz + i ky dv/dz at k0.
