@@ -243,6 +243,32 @@ void penalty_main_(const double *epsilon, const int *ifuncreal,
 void bandlu_solve_(const double *ain, double *xr, double *xi,
                    const int *ifuncreal);
 
+/* No counterpart in the reference.  The work of bandlu_solve_ for callers that
+ * must not allocate device memory while they run: a program whose device memory
+ * belongs to its own pool sized at start-up (an extra cudaMalloc may fail or be
+ * forbidden there), or a timing-critical loop that cannot take the device-wide
+ * synchronisation of cudaFree.  It calls no cudaMalloc, cudaFree or other
+ * allocating routine.
+ *   ain_dev  device pointer, dense nz x nz matrix, column major, nz = nzloc*nsubd
+ *            (kl = ku = nzloc, as in band_lu.f)
+ *   x_dev    device pointer, nrhs (1 or 2) right-hand sides of nz values back to
+ *            back; overwritten by the solutions
+ *   stream   cudaStream_t to order the work on (NULL: the default stream); the
+ *            call returns once the work is enqueued
+ * Limits: nz <= 3072 and (3*nzloc+1)*nz <= 131072.  Larger systems are refused
+ * with IW_ERR_CONFIG and a message in iw_last_error().  No handle is needed;
+ * the current device is used.
+ * Band storage, pivots and status sit in one fixed device array of about 1.06 MB
+ * that each GPU loading this library holds until the process exits.  Every call
+ * on a device uses that same array; each call rewrites all of it that it reads.
+ * Calls that overlap on the GPU (other streams, other host threads) therefore
+ * corrupt each other: order them, for example on one stream.
+ * The first call on each device also does a one-time set-up (it looks up the
+ * device address of the array); make that first call before any stream capture
+ * begins.  As in bandlu_solve_ and the reference, a zero pivot is not reported. */
+int iw_bandlu_solve_noalloc(const double *ain_dev, double *x_dev, int nzloc,
+                            int nsubd, int nrhs, void *stream);
+
 /* penalty.f:9-53: interior-subdomain Robin parameters for epsilon (kept in
  * the bound handle, used by the next penalty_main_). */
 void penalty_setup_(const double *epsilon);

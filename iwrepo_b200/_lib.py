@@ -26,7 +26,7 @@ EXPORTS = [
     "iw_step", "iw_run", "iw_step_coefs", "iw_diag", "iw_sync", "iw_field_ptr", "iw_stream",
     "iw_device_bytes", "iw_helm_solve_batched", "iw_bind", "iw_profile", "iw_profile_read", "iw_mean_profiles",
     "horfft_", "dpdz_", "filter_3dlegenfourier_", "filter_legenpen_", "interface_avg3d_",
-    "penalty_main_", "bandlu_solve_", "penalty_setup_", "convec_", "calcuvwt_",
+    "penalty_main_", "bandlu_solve_", "iw_bandlu_solve_noalloc", "penalty_setup_", "convec_", "calcuvwt_",
     "abvar1_", "abvar2_", "abvar3_", "bdfvarv_", "bdfvar1_", "bdfvar2_", "bdfvar3_",
 ]
 
@@ -66,6 +66,7 @@ def lib():
     L.iw_stream.argtypes = [vp, C.POINTER(vp)]
     L.iw_device_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
     L.iw_helm_solve_batched.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int]
+    L.iw_bandlu_solve_noalloc.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, vp]
     L.iw_bind.argtypes = [vp]
     L.iw_profile.argtypes = [vp, C.c_int]
     L.iw_mean_profiles.argtypes = [vp, PD]

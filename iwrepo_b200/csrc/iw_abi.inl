@@ -518,3 +518,111 @@ int iw_helm_solve_batched(iw_handle* h, const double* lam_dev, int ncol, int ifb
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// bandlu_solve_ without device allocation.
+//
+// Some callers cannot allocate device memory while they run. Examples: a
+// program whose device memory is handed out by its own pool, sized at start-up
+// (a fresh cudaMalloc may fail or is not allowed), or a timing-critical loop
+// that cannot take the device-wide synchronisation implied by cudaFree.
+// iw_bandlu_solve_noalloc does the work of bandlu_solve_ (pack the dense matrix
+// into band storage, factor with partial pivoting, solve in place) with the
+// same kernels.  Its band storage, pivots and status live in one fixed
+// file-scope device array of kNoAllocDoubles doubles (about 1.06 MB), which
+// every GPU that loads this library keeps until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocBand = 131072;  // band storage: (3 nzloc + 1) * nz doubles at most
+constexpr int kNoAllocMaxN = 3072;       // nz at most (two right-hand sides stay within 48 KB of shared memory)
+constexpr size_t kNoAllocPivot = kNoAllocBand;                  // pivots: kNoAllocMaxN ints
+constexpr size_t kNoAllocInfo = kNoAllocPivot + kNoAllocMaxN / 2;  // status word
+constexpr size_t kNoAllocSys = kNoAllocInfo + 8;               // system descriptor
+constexpr size_t kNoAllocDoubles = kNoAllocSys + 56;
+static_assert(sizeof(SysDesc) <= 56 * sizeof(double), "SysDesc must fit its scratch slot");
+constexpr int kNoAllocMaxDev = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_base[kNoAllocMaxDev] = {};
+}  // namespace
+
+// Shared by every call on a device; see iw_bandlu_solve_noalloc for the rules.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// Column-major dense n x n -> band storage of band_lu.f:19-34 (row 2N + i - j
+// of column j holds a(i, j) for |i - j| <= N).  Every entry is written, the N
+// fill-in rows and everything outside the band as zero, so nothing left by an
+// earlier call survives.  Also resets the status word and the descriptor.
+__global__ void k_pack_band(const double* __restrict__ a, int n, int N, int ldab, double* __restrict__ ab,
+                            SysDesc* sd, int* info) {
+  const size_t tot = (size_t)ldab * n;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(q % ldab), j = (int)(q / ldab);
+    const int i = r - 2 * N + j;
+    ab[q] = (r >= N && i >= 0 && i < n) ? a[(size_t)i + (size_t)n * j] : 0.0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    SysDesc s;
+    memset(&s, 0, sizeof s);
+    s.eps = 1.0;
+    *sd = s;
+    *info = 0;
+  }
+}
+
+extern "C" {
+
+int iw_bandlu_solve_noalloc(const double* ain_dev, double* x_dev, int nzloc, int nsubd, int nrhs, void* stream) {
+  if (!ain_dev || !x_dev) return set_err(IW_ERR_STATE, "iw_bandlu_solve_noalloc: null matrix or right-hand side");
+  if (nzloc < 2 || nsubd < 1 || nzloc > IW_MAX_NZLOC || nsubd > IW_MAX_SUBD)
+    return set_err(IW_ERR_CONFIG, "iw_bandlu_solve_noalloc: nzloc must be in [2, 64] and nsubd in [1, 64]");
+  if (nrhs != 1 && nrhs != 2) return set_err(IW_ERR_CONFIG, "iw_bandlu_solve_noalloc: nrhs must be 1 or 2");
+  const int n = nzloc * nsubd, ldab = 3 * nzloc + 1;
+  if (n > kNoAllocMaxN || (size_t)ldab * n > kNoAllocBand)
+    return set_err(IW_ERR_CONFIG, "iw_bandlu_solve_noalloc: system exceeds the fixed scratch: need nzloc*nsubd <= 3072 and "
+                                  "(3*nzloc+1)*nzloc*nsubd <= 131072, got nz=" +
+                                      std::to_string(n) + ", band " + std::to_string((size_t)ldab * n));
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDev) return set_err(IW_ERR_CONFIG, "iw_bandlu_solve_noalloc: device index too large");
+  double* base = nullptr;
+  {
+    // one-time set-up per device, with that device current: the device
+    // address of the scratch array (its name in host code is not one)
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return set_err(IW_ERR_CUDA, std::string("iw_bandlu_solve_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      g_noalloc_base[dev] = (double*)p;
+    }
+    base = g_noalloc_base[dev];
+  }
+  double* ab = base;
+  int* ipiv = (int*)(base + kNoAllocPivot);
+  int* info = (int*)(base + kNoAllocInfo);
+  SysDesc* sd = (SysDesc*)(base + kNoAllocSys);
+  Geo g;
+  memset(&g, 0, sizeof g);
+  g.nz = n;
+  g.N = nzloc;
+  g.ns = nsubd;
+  FactorArgs fa;
+  memset(&fa, 0, sizeof fa);
+  fa.sys = sd;
+  fa.pen = base;  // not read without assembly
+  fa.ab = ab;
+  fa.ipiv = ipiv;
+  fa.info = info;
+  fa.nsys = 1;
+  fa.assemble = 0;
+  fa.factor = 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_pack_band<<<64, 256, 0, st>>>(ain_dev, n, nzloc, ldab, ab, sd, info);
+  k_factor<<<1, 32, 0, st>>>(g, fa);
+  k_solve_one<<<1, 32, (size_t)nrhs * n * sizeof(double), st>>>(g, ab, ipiv, x_dev, nrhs);
+  CK(cudaGetLastError());
+  return IW_OK;
+}
+
+}  // extern "C"
