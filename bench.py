@@ -46,24 +46,37 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    # smaller horizontal grid with the same vertical grid and physics, for
+    # profiling the same kernels on a case that fits a profiler's replay
+    ap.add_argument("--nx", type=int, default=None)
+    ap.add_argument("--ny", type=int, default=None)
     return ap.parse_args()
 
 
-def workload_cfg(name: str, precision: str):
+def workload_cfg(name: str, precision: str, nx=None, ny=None):
     prec = cf.IW_PREC_MIXED if precision == "mixed" else cf.IW_PREC_FP64
-    return cf.baseline(name, precision=prec)
+    kw = {k: v for k, v in (("nx", nx), ("ny", ny)) if v}
+    return cf.baseline(name, precision=prec, **kw)
+
+
+def _base_xy(name):
+    b = cf.baseline(name)
+    return (b.nx, b.ny)
 
 
 def describe(cfg, precision):
     amp, noise = cf.BASELINE_IC.get(cfg.name, (0.05, 1e-4))
     return {
-        "workload": f"{cfg.name}: {cfg.nx}x{cfg.ny}x({cfg.nsubd}x{cfg.nzloc}={cfg.nz}) Boussinesq step, "
+        "workload": f"{cfg.name}{'' if (cfg.nx, cfg.ny) == _base_xy(cfg.name) else ' vertical grid and physics'}: "
+                    f"{cfg.nx}x{cfg.ny}x({cfg.nsubd}x{cfg.nzloc}={cfg.nz}) Boussinesq step, "
                     f"Re={1 / cfg.xnu:.0f}, A={amp}, noise={noise}, dt={cfg.dt}, "
                     f"{'FP32 fields + FP64 solves' if precision == 'mixed' else 'plain FP64'}",
         "nx": cfg.nx, "ny": cfg.ny, "nz": cfg.nz, "nsubd": cfg.nsubd, "nzloc": cfg.nzloc,
         "grid_points": cfg.grid_points, "bc": "no-slip bottom / free-slip top",
         "filter": "exponential order 8, amp 36, every step",
-        "l2": "inputs larger than L2 (each field >= 105 MB); no flush needed",
+        "l2": (f"no flush: every launch streams more than the 126 MB L2 (one field is "
+               f"{cfg.ntot * (4 if precision == 'mixed' else 8) / 1e6:.0f} MB; the smallest launch moves "
+               f"2 fields plus its solver tables)"),
         "parallelism": "replicas (no sharding)",
     }
 
@@ -143,7 +156,7 @@ def cpu_rate(cfg, threads: int, warm: int, steps: int, faithful: bool):
 
 
 def run_reference(args, rank, world):
-    cfg = workload_cfg(args.config, args.precision)
+    cfg = workload_cfg(args.config, args.precision, args.nx, args.ny)
     if rank != 0:
         return
     import oracle
@@ -169,7 +182,24 @@ PHASE_FIELDS = {  # algorithmic fields moved per launch (reads + writes of ntot-
     "stageA": 12, "y_inverse": 20, "x_row_nl": 23, "y_forward": 19, "stageE": 40,
     "pressure": 6, "solve_uv": 4, "solve_w": 2, "solve_rho": 2,
 }
-LAUNCHES_PER_STEP = 18  # stageA, yinv, xrow, 2 yfwd, wallbc, stageE, press, 3 visc, 6 interface
+# kernels launched per step: stage A, y-inverse, x rows, 2 y-forward, wall BC,
+# stage E, pressure (2 when ill-conditioned systems get a residual sweep),
+# u/v, w, rho, interface averaging (2 gathers, 2 y transforms, rows, planes)
+LAUNCHES_PER_STEP = 18
+
+
+def dram_traffic(cfg, precision, phase):
+    """DRAM bytes per launch of `phase` from the committed ncu figures
+    (profiles/dram_traffic.json), scaled from the captured workload to this one
+    by grid points when they differ; None when no figure exists."""
+    try:
+        tab = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic.json")))
+    except Exception:
+        return None
+    ent = tab.get(precision, {}).get(phase)
+    if not ent:
+        return None
+    return ent["bytes_per_launch"] * cfg.ntot / ent["ntot"]
 
 
 def run_ours(args, rank, world):
@@ -184,7 +214,7 @@ def run_ours(args, rank, world):
         import datetime
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
-    cfg = workload_cfg(args.config, args.precision)
+    cfg = workload_cfg(args.config, args.precision, args.nx, args.ny)
     amp, noise = cf.BASELINE_IC.get(cfg.name, (0.05, 1e-4))
     seed = 1000 + rank
     s = iw.Solver(cfg, device=dev)
@@ -200,6 +230,9 @@ def run_ours(args, rank, world):
     barrier()
     clocks = Clocks(dev)
     clocks.start()
+    # per-phase CUDA events on the library's stream during the timed steps
+    # (one host wait per step to read them: a few microseconds per step)
+    s.profile(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(ext)
     s.step(args.steps)
@@ -207,18 +240,15 @@ def run_ours(args, rank, world):
     barrier()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
+    ph = s.profile_read()
+    s.profile(False)
     if dist:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * cfg.grid_points * args.steps / (ms / 1e3)
 
-    # per-phase device time (separate profiled steps) -> dominant kernel
-    s.profile(True)
-    s.step(max(2, min(args.steps, 5)))
-    s.sync()
-    ph = s.profile_read()
-    s.profile(False)
+    # per-phase device time of the timed steps -> dominant kernel
     elem = 4 if args.precision == "mixed" else 8
     fb = cfg.ntot * elem
     peaks = {}
@@ -236,7 +266,7 @@ def run_ours(args, rank, world):
     dom = max((k for k in phases if PHASE_FIELDS.get(k)), key=lambda k: phases[k]["ms"])
     dom_gbs = phases[dom]["gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_gbs, "peak": hbm, "unit": "GB/s",
-                "frac": dom_gbs / hbm, "traffic": None,
+                "frac": dom_gbs / hbm, "traffic": dram_traffic(cfg, args.precision, dom),
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_launch": PHASE_FIELDS[dom] * fb}
     b_alg = 28 * elem * (cfg.nx + 2) / cfg.nx
