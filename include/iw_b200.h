@@ -161,9 +161,22 @@ int iw_init_mode1(iw_handle *h, double amplitude, double noise_amp,
  * coefficient schedule, calcuvwt, t += dt, interface averaging.  The
  * coefficient schedule of main.f:700-856 is applied internally (fixed dt). */
 int iw_step(iw_handle *h);
-/* nsteps steps; with use_graph != 0 the steady-state step is captured once
- * into a CUDA graph and replayed. */
+/* nsteps steps of main.f:653-1066.  With use_graph != 0, once the step is
+ * invariant, steps are replayed from two captured CUDA graphs, one launch per
+ * step. "Invariant" means: from step 4 with a fixed dt; no paddle forcing;
+ * the filter every nspecfilterexp = 1 step; navgintrfc <= 1; profiling off.
+ * Two graphs are needed because the history buffers alternate between two
+ * arrangements.  Results are identical to the eager path.  Graphs are built
+ * per call and freed before it returns. */
 int iw_run(iw_handle *h, int nsteps, int use_graph);
+
+/* Not in the reference (its main.f advances one run).  Advances n independent
+ * runs of any sizes (separate handles on one device) by nsteps steps each.
+ * Steps run eagerly until every member is invariant as for iw_run.  After
+ * that, each step of the whole ensemble is one CUDA-graph launch, in which the
+ * members are independent branches.  Each member's results are identical to
+ * running it alone. */
+int iw_ensemble_run(iw_handle *const *members, int n, int nsteps);
 /* As iw_step but with caller-supplied coefficients (variable-dt restarts). */
 int iw_step_coefs(iw_handle *h, const iw_coefs *c);
 

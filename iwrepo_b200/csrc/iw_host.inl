@@ -615,6 +615,8 @@ static int build_factors(iw_handle* h, int kind) {
   CK(cudaMemcpyAsync(h->dcolsys[kind], colsys.data(), colsys.size() * sizeof(int), cudaMemcpyHostToDevice, h->st));
   if (nsys > 0) {
     FactorArgs fa;
+    fa.assemble = 1;
+    fa.factor = 1;
     fa.sys = h->dsys[kind];
     fa.pen = h->dpen[kind];
     fa.ab = h->dab[kind];
@@ -984,6 +986,17 @@ static void launch_y(iw_handle* h, FieldSet<T>& fs, YJobs<T>& jobs, int njobs, i
       FN<T, 48>(__VA_ARGS__);                     \
   } while (0)
 
+// History rotation by pointer swap (solver.f:447-478): the buffer written
+// with S (level n) becomes Sn, the one written with F2 becomes Fn.  The
+// arrangement repeats every 2 steps.
+template <typename T>
+static void rotate_levels(FieldSet<T>& fs) {
+  for (int q = 0; q < 4; ++q) {
+    std::swap(fs.Sn[q], fs.Snm[q]);
+    std::swap(fs.Fn[q], fs.Fnm[q]);
+  }
+}
+
 // convec (solver.f:6-514).  proj=1 also applies the maxcalc round trip that
 // precedes it in the main loop (main.f:657).
 template <typename T>
@@ -1087,10 +1100,7 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
   // K_E
   launch_stageE<T>(h, fs);
   mark(h, 5);
-  for (int q = 0; q < 4; ++q) {
-    std::swap(fs.Sn[q], fs.Snm[q]);  // Snm buffer now holds S (level n) -> becomes Sn
-    std::swap(fs.Fn[q], fs.Fnm[q]);
-  }
+  rotate_levels(fs);
   return 0;
 }
 
@@ -1263,6 +1273,114 @@ static int full_step(iw_handle* h, FieldSet<T>& fs) {
   prof_flush(h);
   CK(cudaGetLastError());
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA-graph replay of whole steps.
+//
+// From step 4 on, with a fixed dt, the SS3/BDF3 coefficients and the solver
+// tables no longer change.  The launches of a step and their arguments are
+// then the same from step to step, up to the history buffers, whose pointer
+// arrangement repeats every 2 steps.  Two captured graphs (one per
+// arrangement), launched alternately, therefore replay the step exactly.
+// Conditions that would make a step depend on its number keep the eager path:
+// paddle forcing (time in the arguments), a filter not applied every step,
+// interface averaging less often than every step, per-phase profiling.
+// ---------------------------------------------------------------------------
+static bool graph_ready(const iw_handle* h) {
+  return h->istep >= 3 && !h->prof && !h->p.forcing && (h->p.ispecfilterexp != 1 || h->p.nspecfilterexp == 1) &&
+         h->p.navgintrfc <= 1;
+}
+
+static int step_dispatch(iw_handle* h) { return h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64); }
+
+static void rotate_host(iw_handle* h) {
+  if (h->mixed)
+    rotate_levels(h->f32);
+  else
+    rotate_levels(h->f64);
+}
+
+// One step of every handle captured into one graph whose launch on s0 runs
+// the members as independent branches.  The host-side step counters are put
+// back after capture (they advance when the graph runs).
+static int capture_step(iw_handle* const* hs, int n, cudaStream_t s0, cudaGraphExec_t* out) {
+  *out = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join(n, nullptr);
+  CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  for (auto& e : join) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  int rc = IW_OK, stepped = 0;
+  CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  cudaEventRecord(fork, s0);
+  for (int i = 0; i < n; ++i) {
+    iw_handle* h = hs[i];
+    cudaStreamWaitEvent(h->st, fork, 0);
+    const int is = h->istep;
+    const double t = h->t;
+    rc = step_dispatch(h);
+    h->istep = is;
+    h->t = t;
+    ++stepped;
+    cudaEventRecord(join[i], h->st);
+    cudaStreamWaitEvent(s0, join[i], 0);
+    if (rc != IW_OK) break;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s0, &g);
+  if (rc == IW_OK && e != cudaSuccess)
+    rc = set_err(IW_ERR_CUDA, std::string("graph capture of the step failed: ") + cudaGetErrorString(e));
+  if (rc == IW_OK) {
+    const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+    if (ei != cudaSuccess) rc = set_err(IW_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(ei));
+  }
+  if (g) cudaGraphDestroy(g);
+  if (rc != IW_OK)
+    for (int i = 0; i < stepped; ++i) rotate_host(hs[i]);  // nothing ran: undo the host-side rotation
+  cudaEventDestroy(fork);
+  for (auto& ev : join) cudaEventDestroy(ev);
+  return rc;
+}
+
+// nsteps steps of every handle (all graph_ready, same device) as alternating
+// graph launches on a private stream, ordered after and before the handles'
+// own streams.
+static int run_graphs(iw_handle* const* hs, int n, int nsteps) {
+  if (nsteps <= 0) return IW_OK;
+  cudaStream_t s0 = nullptr;
+  CK(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+  cudaEvent_t ev = nullptr;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  for (int i = 0; i < n; ++i) {
+    CK(cudaEventRecord(ev, hs[i]->st));
+    CK(cudaStreamWaitEvent(s0, ev, 0));
+  }
+  cudaGraphExec_t gx[2] = {nullptr, nullptr};
+  int rc = capture_step(hs, n, s0, &gx[0]);  // arrangement p; host moves to p+1
+  if (rc == IW_OK) {
+    rc = capture_step(hs, n, s0, &gx[1]);  // arrangement p+1; host back to p
+    if (rc != IW_OK)
+      for (int i = 0; i < n; ++i) rotate_host(hs[i]);
+  }
+  if (rc == IW_OK) {
+    for (int k = 0; k < nsteps && rc == IW_OK; ++k) {
+      const cudaError_t e = cudaGraphLaunch(gx[k & 1], s0);
+      if (e != cudaSuccess) rc = set_err(IW_ERR_CUDA, std::string("graph launch failed: ") + cudaGetErrorString(e));
+      else
+        for (int i = 0; i < n; ++i) {  // host-side state follows each replayed step
+          hs[i]->istep += 1;
+          hs[i]->t += hs[i]->p.dt;
+          rotate_host(hs[i]);
+        }
+    }
+    cudaEventRecord(ev, s0);
+    for (int i = 0; i < n; ++i) cudaStreamWaitEvent(hs[i]->st, ev, 0);
+  }
+  for (auto& g : gx)
+    if (g) cudaGraphExecDestroy(g);
+  cudaEventDestroy(ev);
+  cudaStreamDestroy(s0);
+  return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -1503,12 +1621,49 @@ int iw_step(iw_handle* h) {
 }
 
 int iw_run(iw_handle* h, int nsteps, int use_graph) {
-  (void)use_graph;
-  for (int s = 0; s < nsteps; ++s) {
-    int r = iw_step(h);
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  cudaSetDevice(h->dev);
+  int s = 0;
+  for (; s < nsteps && !(use_graph && graph_ready(h)); ++s) {
+    int r = step_dispatch(h);
     if (r) return r;
   }
-  return IW_OK;
+  return run_graphs(&h, 1, nsteps - s);
+}
+
+int iw_ensemble_run(iw_handle* const* members, int n, int nsteps) {
+  if (!members || n <= 0 || nsteps < 0) return set_err(IW_ERR_STATE, "iw_ensemble_run: bad argument");
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) return set_err(IW_ERR_STATE, "iw_ensemble_run: null member");
+    if (members[i]->dev != members[0]->dev) return set_err(IW_ERR_CONFIG, "iw_ensemble_run: members on different devices");
+    for (int j = 0; j < i; ++j)
+      if (members[j] == members[i]) return set_err(IW_ERR_CONFIG, "iw_ensemble_run: a member is listed twice");
+  }
+  cudaSetDevice(members[0]->dev);
+  // eager steps (members overlap on their own streams) until every member can
+  // be replayed from a graph
+  int s = 0;
+  for (;; ++s) {
+    bool all = true;
+    for (int i = 0; i < n; ++i) all = all && graph_ready(members[i]);
+    if (all || s >= nsteps) break;
+    for (int i = 0; i < n; ++i) {
+      int r = step_dispatch(members[i]);
+      if (r) return r;
+    }
+  }
+  if (s >= nsteps) return IW_OK;
+  bool all = true;
+  for (int i = 0; i < n; ++i) all = all && graph_ready(members[i]);
+  if (!all) {  // a member that never qualifies (forcing, profiling, ...): eager
+    for (; s < nsteps; ++s)
+      for (int i = 0; i < n; ++i) {
+        int r = step_dispatch(members[i]);
+        if (r) return r;
+      }
+    return IW_OK;
+  }
+  return run_graphs(members, n, nsteps - s);
 }
 
 int iw_step_coefs(iw_handle* h, const iw_coefs* c) {

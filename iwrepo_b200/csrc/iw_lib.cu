@@ -760,17 +760,17 @@ struct SysDesc {
 };
 
 struct FactorArgs {
-  const SysDesc* sys;
-  const double* pen;  // per system: 6*ns (alpha,beta,gamma,delta,tau1,tau2)
-  double* ab;         // per system: ldab*nz
-  int* ipiv;          // per system: nz
-  int* info;          // per system
-  int nsys;
-  const double* D;
-  const double* D2;
-  const double* zh;  // ns
-  int assemble;      // 0: ab already holds the packed matrix (bandlu_solve_)
-  int factor = 1;    // 0: assemble only (block-inverse systems)
+  const SysDesc* sys = nullptr;
+  const double* pen = nullptr;  // per system: 6*ns (alpha,beta,gamma,delta,tau1,tau2)
+  double* ab = nullptr;         // per system: ldab*nz
+  int* ipiv = nullptr;          // per system: nz
+  int* info = nullptr;          // per system
+  int nsys = 0;
+  const double* D = nullptr;
+  const double* D2 = nullptr;
+  const double* zh = nullptr;  // ns
+  int assemble = 1;            // 0: ab already holds the packed matrix (bandlu_solve_)
+  int factor = 1;              // 0: assemble only (block-inverse systems)
 };
 
 __device__ __forceinline__ double& ABr(double* ab, int ldab, int r, int c) {

@@ -98,6 +98,11 @@ class Solver:
     def step(self, n: int = 1):
         _lib.check(_lib.lib().iw_run(self.h, n, 0))
 
+    def run(self, n: int, graph: bool = True):
+        """n steps; with graph=True the invariant steady-state step is replayed
+        from captured CUDA graphs (identical results, one launch per step)."""
+        _lib.check(_lib.lib().iw_run(self.h, n, 1 if graph else 0))
+
     def step_coefs(self, fac, bdf, bdfv, dt):
         c = IwCoefs(fac[0], fac[1], fac[2], bdf[0], bdf[1], bdf[2], bdfv, dt)
         _lib.check(_lib.lib().iw_step_coefs(self.h, C.byref(c)))
@@ -212,6 +217,14 @@ class Solver:
     def calcuvwt(self, cpenspecfilter: bool = True):
         self._bind()
         _lib.lib().calcuvwt_(_ri(0), _ri(0), _ri(0), _ri(1 if cpenspecfilter else 0))
+
+
+def ensemble_run(members, n: int):
+    """Advance independent runs of any sizes (Solver objects on one device) by
+    n steps each; once all are in steady state, each ensemble step is one
+    CUDA-graph launch.  Results equal running each member alone."""
+    arr = (C.c_void_p * len(members))(*[m.h for m in members])
+    _lib.check(_lib.lib().iw_ensemble_run(arr, len(members), n))
 
 
 def multistep(name: str, dt1: float, dt2: float, dt3: float) -> float:
