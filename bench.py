@@ -50,6 +50,9 @@ def parse():
     # profiling the same kernels on a case that fits a profiler's replay
     ap.add_argument("--nx", type=int, default=None)
     ap.add_argument("--ny", type=int, default=None)
+    # C3 mixed against C3 FP64 over this many steps: field, kinetic-energy and
+    # noise growth-rate errors (a report, not a bench line)
+    ap.add_argument("--error-report", type=int, default=0)
     return ap.parse_args()
 
 
@@ -433,10 +436,118 @@ def run_c4(args):
     print(json.dumps(line), flush=True)
 
 
+def run_c1(args):
+    """C1: 256 x 129 isolated penalty-Helmholtz columns over 8 x 25 GLL points,
+    lambda = kx^2 + ky^2 + 11/(6 dt), dt = 1e-3, seeded N(0,1) complex RHS.
+    FP64 factor + solve (first call), FP64 solve with cached factors, and FP32
+    solve + one FP64 residual sweep (iw_helm_solve_batched modes 0 and 1)."""
+    import torch
+    import iwrepo_b200 as iw
+
+    torch.cuda.set_device(0)
+    cfg = cf.Config(nx=256, ny=256, nzloc=25, nsubd=8, dt=1e-3, xnu=1.0, xkappa=1.0,
+                    precision=cf.IW_PREC_FP64, name="C1").validate()
+    s = iw.Solver(cfg, device=0)
+    kx = np.arange(cfg.nx // 2 + 1)
+    ky = np.fft.fftfreq(cfg.ny, 1.0 / cfg.ny)
+    lam = (kx[None, :] ** 2 + ky[:, None] ** 2).ravel() + 11.0 / (6 * cfg.dt)
+    ncol = lam.size
+    rng = np.random.default_rng(2024)
+    rhs = torch.tensor(rng.standard_normal((ncol, cfg.nz, 2)), dtype=torch.float64, device="cuda")
+    dl = torch.tensor(lam, dtype=torch.float64, device="cuda")
+    out = {m: torch.zeros_like(rhs) for m in (0, 1)}
+    ext = torch.cuda.ExternalStream(s.stream())
+
+    def timed(mode, reps):
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(ext)
+        for _ in range(reps):
+            iw.helm_solve_batched(s, dl.data_ptr(), ncol, 0, 1, rhs.data_ptr(), out[mode].data_ptr(), mode)
+        a1.record(ext)
+        torch.cuda.synchronize()
+        return a0.elapsed_time(a1) / reps
+
+    t_fact = timed(0, 1)  # builds and caches the factors of the distinct lambdas
+    for _ in range(args.warmup):
+        timed(0, 1)
+        timed(1, 1)
+    t64 = timed(0, max(args.steps, 1))
+    t32 = timed(1, max(args.steps, 1))
+    x0, x1 = out[0].cpu().numpy(), out[1].cpu().numpy()
+    per_col = np.linalg.norm((x1 - x0).reshape(ncol, -1), axis=1) / np.linalg.norm(x0.reshape(ncol, -1), axis=1)
+    b_alg = 2 * cfg.nz * 16  # complex RHS in + solution out
+    peak = 6553.0
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        pass
+    rates = {"fp64_factor_and_solve": ncol / (t_fact / 1e3), "fp64_solve": ncol / (t64 / 1e3),
+             "fp32_solve_fp64_refine": ncol / (t32 / 1e3)}
+    line = {
+        "metric": "solves/s", "value": rates["fp32_solve_fp64_refine"], "unit": "solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "data": "synthetic (seeded N(0,1) RHS)",
+        "config": {"workload": "C1: 33,024 penalty-Helmholtz systems (kx 0..128 x ky 256), nz = 8 x 25, "
+                               "lambda = k^2 + 11/(6 dt), dt = 1e-3, u-type BCs (Dirichlet bottom, Neumann top)",
+                   "distinct_systems": int(np.unique(lam).size)},
+        "rates_solves_per_s": rates,
+        "ms_per_batch": {"fp64_factor_and_solve": t_fact, "fp64_solve": t64, "fp32_solve_fp64_refine": t32},
+        "fp32_refined_vs_fp64_rel_l2": {"max_over_columns": float(per_col.max()), "median": float(np.median(per_col))},
+        "hbm_roofline_frac_rhs_and_solution": {k: v * b_alg / (peak * 1e9) for k, v in rates.items()},
+        "note": "relative residuals are checked in tests/test_gpu_parity.py::test_helm_batched_modes "
+                "(<1e-11 FP64, <1e-7 FP32 + refinement)",
+    }
+    print(json.dumps(line), flush=True)
+    s.close()
+
+
+def run_error_report(args):
+    """C3 mixed vs C3 FP64 from the same seeded state for args.error_report
+    steps: final relative L2 per field and for the velocity vector, the largest
+    relative KE difference over the run, and the growth rate of the rms of w
+    in the bottom 20 % of the depth (the seeded noise) in each precision."""
+    import iwrepo_b200 as iw
+
+    base = workload_cfg(args.config, "mixed", args.nx, args.ny)
+    amp, noise = cf.BASELINE_IC.get(base.name, (0.05, 1e-4))
+    runs = {"mixed": iw.Solver(base, device=0), "fp64": iw.Solver(base.replace(precision=cf.IW_PREC_FP64), device=0)}
+    hist = {k: [] for k in runs}
+    for r in runs.values():
+        r.init_mode1(amp, noise, 1000)
+    every = 10
+    for k in range(0, args.error_report, every):
+        for name, r in runs.items():
+            r.run(min(every, args.error_report - k), graph=True)
+            d = r.diag()
+            hist[name].append((d["t"], d["ke"], d["wrms_bottom"]))
+    a, b = runs["mixed"].state(0), runs["fp64"].state(0)
+    err = {f: float(np.linalg.norm(a[q] - b[q]) / np.linalg.norm(b[q])) for q, f in enumerate("uvwr")}
+    err["velocity"] = float(np.linalg.norm(a[:3] - b[:3]) / np.linalg.norm(b[:3]))
+    hm, hd = np.array(hist["mixed"]), np.array(hist["fp64"])
+    ke_err = float(np.max(np.abs(hm[:, 1] - hd[:, 1]) / np.abs(hd[:, 1])))
+
+    def rate(h):  # least-squares slope of log(w rms) over the second half of the run
+        n2 = len(h) // 2
+        return float(np.polyfit(h[n2:, 0], np.log(h[n2:, 2]), 1)[0])
+
+    gm, gd = rate(hm), rate(hd)
+    line = {"report": "mixed vs fp64", "workload": describe(base, "mixed")["workload"], "steps": args.error_report,
+            "field_rel_l2": err, "ke_max_rel_diff": ke_err,
+            "noise_growth_rate": {"mixed": gm, "fp64": gd, "rel_diff": abs(gm - gd) / abs(gd)},
+            "samples_every_steps": every}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.error_report > 0:
+        run_error_report(args)
+        return
     if args.config == "C4" and args.impl == "ours":
         run_c4(args)
+        return
+    if args.config == "C1" and args.impl == "ours":
+        run_c1(args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.impl == "ours" else 1)))

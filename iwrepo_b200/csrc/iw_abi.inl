@@ -465,9 +465,51 @@ static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
     }
   }
   double red[8];
+  // maxcalc statistics on the physical fields
+  {
+    const double dx = h->p.xlen / h->nx, dy = h->p.ylen / h->ny;
+    const double rg = -(h->p.rho0 * h->p.brunt * h->p.brunt) / h->p.grav;
+    for (int q = 0; q < 4; ++q) {
+      phys_of<T>(h, fs, fs.F[q], dst, tmp, 0);
+      const double cflh = q == 0 ? h->p.dt / dx : q == 1 ? h->p.dt / dy : 0.0;
+      k_phys_stats<T><<<296, 256, 0, h->st>>>(g, dst, q, h->dzg, h->ddzinv, cflh, rg, 0.2 * h->p.zlen,
+                                              h->dpart + (size_t)q * 296 * 5);
+    }
+  }
+  std::vector<double> part((size_t)4 * 296 * 5);
+  CK(cudaMemcpyAsync(part.data(), h->dpart, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(red, h->dred, sizeof red, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   memset(out, 0, sizeof *out);
+  {
+    double mm[4][2], cf[4] = {0, 0, 0, 0}, s2 = 0, cnt = 0;
+    for (int q = 0; q < 4; ++q) {
+      mm[q][0] = part[(size_t)q * 296 * 5];
+      mm[q][1] = part[(size_t)q * 296 * 5 + 1];
+      for (int b = 0; b < 296; ++b) {
+        const double* o = part.data() + ((size_t)q * 296 + b) * 5;
+        mm[q][0] = std::min(mm[q][0], o[0]);
+        mm[q][1] = std::max(mm[q][1], o[1]);
+        cf[q] = std::max(cf[q], o[2]);
+        if (q == 2) {
+          s2 += o[3];
+          cnt += o[4];
+        }
+      }
+    }
+    out->umin = mm[0][0];
+    out->umax = mm[0][1];
+    out->vmin = mm[1][0];
+    out->vmax = mm[1][1];
+    out->wmin = mm[2][0];
+    out->wmax = mm[2][1];
+    out->tmin = mm[3][0];
+    out->tmax = mm[3][1];
+    out->cflx = cf[0];
+    out->cfly = cf[1];
+    out->cflz = cf[2];
+    out->wrms_bottom = cnt > 0 ? std::sqrt(s2 / cnt) : 0.0;
+  }
   out->ke = 0.5 * red[0];
   out->eps = h->p.xnu * red[1];
   out->t = h->t;

@@ -307,6 +307,7 @@ struct iw_handle {
   bool mixed = false;
   Tables tab;
   // device tables
+  double *ddzinv = 0, *dpart = 0;  // diagnostics: dt-free CFL spacing per level, per-block partials
   double *dDt = 0, *dD2t = 0, *dLt = 0;  // transposed D, D2, Legendre filter (t[k*N + k1] = D[k1][k])
   double *dD = 0, *dD2 = 0, *dL = 0, *dh = 0, *dxw = 0, *dyw = 0, *dcf = 0, *dzg = 0, *dzh = 0;
   double *dwg = 0, *dal = 0, *dsig = 0, *dmeang = 0;
@@ -855,7 +856,7 @@ static ZOp<T, NM> make_zop(const iw_handle* h) {
   for (int k1 = 0; k1 < h->N; ++k1)
     for (int k2 = 0; k2 < h->N; ++k2) {
       op.D[k1 * NM + k2] = (T)h->tab.D[(size_t)k1 * h->N + k2];
-      op.L[k1 * NM + k2] = (T)h->tab.Lfil[(size_t)k1 * h->N + k2];
+      op.L[k1 * NM + k2] = (T)(h->tab.Lfil[(size_t)k1 * h->N + k2] - (k1 == k2 ? 1.0 : 0.0));
     }
   return op;
 }
@@ -1488,6 +1489,27 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
     }
   int r = 0;
   r |= up(h, &h->dDt, Dt) || up(h, &h->dD2t, D2t) || up(h, &h->dLt, Lt);
+  {
+    // 1/dz of the CFL in z (various.f:665-987): zf merges the duplicated
+    // interface points; the point below zf(1) is the word before it, z(nz);
+    // the top level has no CFL
+    const int N = h->N, ns = h->ns, nz = h->nz;
+    std::vector<double> zf((size_t)ns * (N - 1) + 2, 0.0), zgl(nz), dzi(nz, 0.0);
+    for (int ks = 0; ks < ns; ++ks)
+      for (int kl = 0; kl < N; ++kl) {
+        const double z = prm->z0[ks] + 0.5 * prm->zh[ks] * (h->tab.zpts[kl] + 1.0);
+        zgl[ks * N + kl] = z;
+        zf[(size_t)ks * (N - 1) + kl + 1] = z;
+      }
+    for (int ks = 0; ks < ns; ++ks)
+      for (int kl = 0; kl < N; ++kl) {
+        const int k = ks * N + kl, kg = ks * (N - 1) + kl + 1;
+        if (k == nz - 1) continue;
+        const double zm = kg - 1 >= 1 ? zf[kg - 1] : zgl[nz - 1];
+        dzi[k] = 1.0 / (zf[kg] - zm);
+      }
+    r |= up(h, &h->ddzinv, dzi) || dalloc(h, &h->dpart, (size_t)4 * 296 * 5);
+  }
   r |= up(h, &h->dD, h->tab.D) || up(h, &h->dD2, h->tab.D2) || up(h, &h->dL, h->tab.Lfil) || up(h, &h->dh, hf) ||
        up(h, &h->dxw, xw) || up(h, &h->dyw, yw) || up(h, &h->dcf, cf) || up(h, &h->dzg, zg) || up(h, &h->dzh, zh) ||
        up(h, &h->dwg, h->tab.wg) || up(h, &h->dal, h->tab.alpol) || up(h, &h->dsig, h->tab.sigma) ||
@@ -1516,7 +1538,7 @@ int iw_destroy(iw_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   free_fields(h->f64);
   free_fields(h->f32);
-  for (double* p : {h->dDt, h->dD2t, h->dLt, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
+  for (double* p : {h->ddzinv, h->dpart, h->dDt, h->dD2t, h->dLt, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
                     h->dmeang, h->dwnl, h->dwvr, h->dred})
     cudaFree(p);
   cudaFree(h->dcnt);

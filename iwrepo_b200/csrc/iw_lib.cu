@@ -457,6 +457,14 @@ struct Coefs {
   double fac1, fac2, fac3, bdf1, bdf2, bdf3, bdfv, dt;
 };
 
+// u* = dt (extrapolated NL) + bdf1 F2 + bdf2 Fn + bdf3 Fnm, combined in FP64
+// whatever the storage type: in FP32 the rounded coefficients (1/3) would
+// make bdf1 + bdf2 + bdf3 differ from bdfv and bias every step the same way.
+template <typename T>
+__device__ __forceinline__ T bdf_combine(const Coefs& c, T se, T F2, T fn, T fnm) {
+  return (T)(c.dt * (double)se + c.bdf1 * (double)F2 + c.bdf2 * (double)fn + c.bdf3 * (double)fnm);
+}
+
 template <typename T>
 struct EArgs {
   const T* B[4];
@@ -481,7 +489,7 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
   T* tf = tz + N * kTX;    // N*kTX: F* tile
   for (int t = threadIdx.x; t < N * N; t += blockDim.x) {
     sD[t] = (T)g.D[t];
-    sL[t] = (T)g.Lfil[t];
+    sL[t] = (T)(g.Lfil[t] - (t / N == t % N ? 1.0 : 0.0));  // L - I, formed before rounding
   }
   const int q = blockIdx.z;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -513,7 +521,7 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
       const T F2 = proj_val<T>(g, a.F1[q], i, j, kk);
       const T fn = a.Fn[q][p];
       const T fnm = a.Fnm_w[q][p];
-      fsv = (T)c.dt * se + (T)c.bdf1 * F2 + (T)c.bdf2 * fn + (T)c.bdf3 * fnm;
+      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
       a.Snm_w[q][p] = S;
       a.Fnm_w[q][p] = F2;
     }
@@ -521,7 +529,7 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
   }
   __syncthreads();
   if (!act) return;
-  const T cf = a.filter ? (T)g.cfour[(size_t)j * g.nxhp + (i >> 1)] : (T)1;
+  const T cfm1 = a.filter ? (T)(g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0) : (T)0;
   for (int k1 = w; k1 < N; k1 += kTW) {
     T o;
     if (a.filter) {
@@ -529,7 +537,8 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
       T s = 0;
 #pragma unroll 4
       for (int k2 = 0; k2 < N; ++k2) s += lr[k2] * tf[k2 * kTX + lane];
-      o = cf * s;
+      const T gv = tf[k1 * kTX + lane] + s;  // L f = f + (L - I) f
+      o = gv + cfm1 * gv;                    // cf g = g + (cf - 1) g
     } else {
       o = tf[k1 * kTX + lane];
     }
@@ -542,14 +551,16 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
 // (x, y) point of one subdomain and keeps its N values of the column in
 // registers; thread t addresses element t of every z-plane, so each warp
 // reads and writes 128-byte contiguous runs.  The N x N operators (D and the
-// precombined filter, zero-padded to NM x NM) are kernel parameters, i.e. they
+// precombined filter minus the identity, zero-padded to NM x NM; a filter
+// close to the identity is applied as f + (L - I) f so that rounding its
+// entries does not bias every step) are kernel parameters, i.e. they
 // sit in the constant bank, and the fully unrolled products take them as
 // immediate operands: about one instruction per multiply-add.
 // ---------------------------------------------------------------------------
 template <typename T, int NM>
 struct ZOp {
   T D[NM * NM];  // D[k1*NM + k2], zero outside N x N
-  T L[NM * NM];  // precombined Legendre filter, same layout
+  T L[NM * NM];  // precombined Legendre filter minus the identity, same layout
 };
 
 template <typename T, int NM>
@@ -652,13 +663,13 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
       if (q == 2 && ((kk == 0) || (kk == g.nz - 1)))
         a.wnl[t + (kk == 0 ? 0 : g.plane)] = (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
       const T se = f1 * S + f2 * sn + f3 * snm;
-      fsv = (T)c.dt * se + (T)c.bdf1 * F2 + (T)c.bdf2 * fn + (T)c.bdf3 * fnm;
+      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
       Snmq[p] = S;
       Fnmq[p] = F2;
     }
     fs[k1] = fsv;
   }
-  const T cf = a.filter ? (T)g.cfour[(size_t)j * g.nxhp + (i >> 1)] : (T)1;
+  const T cfm1 = a.filter ? (T)(g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0) : (T)0;
 #pragma unroll
   for (int k1 = 0; k1 < NM; ++k1) {
     if (k1 < N) {
@@ -666,8 +677,9 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
       if (a.filter) {
         T s = 0;
 #pragma unroll
-        for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * fs[k2];
-        o = cf * s;
+        for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * fs[k2];  // (L - I) f
+        const T gv = fs[k1] + s;
+        o = gv + cfm1 * gv;
       } else {
         o = fs[k1];
       }
@@ -2246,6 +2258,68 @@ __global__ void k_reduce_sq(Geo g, const T* __restrict__ a, int kmin, double* ou
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+// maxcalc statistics of one physical field (various.f:665-987 without the
+// adaptive step): extrema starting from the reference's initial values (0, or
+// 1 for rho whose background 1 + rhograd z is added), the CFL maximum
+// (x, y: |f| dt/dx; z: |w| dt/dz with the reference's merged-interface
+// spacing, dzinv), and for w the sum of squares and count below zlim.
+// Per-block partials: part[5*block + {min, max, cfl, sum w^2, count}].
+template <typename T>
+__global__ void k_phys_stats(Geo g, const T* __restrict__ a, int q, const double* __restrict__ zg,
+                             const double* __restrict__ dzinv, double cflh, double rg, double zlim, double* part) {
+  double mn = q == 3 ? 1.0 : 0.0, mx = 0.0, cf = 0.0, s2 = 0.0, cnt = 0.0;
+  const long total = (long)g.nx * g.ny * g.nz;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx);
+    const long r = t / g.nx;
+    const int j = (int)(r % g.ny), k = (int)(r / g.ny);
+    double x = (double)a[fidx<T>(g, i, j, k)];
+    if (q == 0 || q == 1) cf = fmax(cf, fabs(x) * cflh);
+    if (q == 2) {
+      cf = fmax(cf, fabs(x) * g.dt * dzinv[k]);
+      if (zg[k] < zlim) {
+        s2 += x * x;
+        cnt += 1.0;
+      }
+    }
+    if (q == 3) x += 1.0 + rg * zg[k];
+    mn = fmin(mn, x);
+    mx = fmax(mx, x);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    cf = fmax(cf, __shfl_xor_sync(0xffffffffu, cf, o));
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  }
+  __shared__ double sh[32][5];
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    sh[w][0] = mn;
+    sh[w][1] = mx;
+    sh[w][2] = cf;
+    sh[w][3] = s2;
+    sh[w][4] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int v = 1; v < nw; ++v) {
+      mn = fmin(mn, sh[v][0]);
+      mx = fmax(mx, sh[v][1]);
+      cf = fmax(cf, sh[v][2]);
+      s2 += sh[v][3];
+      cnt += sh[v][4];
+    }
+    double* o = part + 5 * (size_t)blockIdx.x;
+    o[0] = mn;
+    o[1] = mx;
+    o[2] = cf;
+    o[3] = s2;
+    o[4] = cnt;
+  }
 }
 
 template <typename T>

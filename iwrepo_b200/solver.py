@@ -113,7 +113,9 @@ class Solver:
     def diag(self) -> dict:
         d = IwDiagOut()
         _lib.check(_lib.lib().iw_diag(self.h, C.byref(d)))
-        return dict(ke=d.ke, eps=d.eps, t=d.t, istep=d.istep, avg=list(d.interface_avg_count))
+        return dict(ke=d.ke, eps=d.eps, t=d.t, istep=d.istep, avg=list(d.interface_avg_count),
+                    wrms_bottom=d.wrms_bottom, cfl=(d.cflx, d.cfly, d.cflz),
+                    minmax=(d.umin, d.umax, d.vmin, d.vmax, d.wmin, d.wmax, d.tmin, d.tmax))
 
     def mean_profiles(self, out: np.ndarray = None) -> np.ndarray:
         """(4, nz) mean profiles of u, v, w, rho (device -> host, synchronous)."""

@@ -124,6 +124,21 @@ def test_steps_3d_strict(small, solver):
             assert rel(a[q], b[q]) < 1e-11, (lev, q)
 
 
+def test_diag_maxcalc_and_bottom_rms_match_oracle(small):
+    """iw_diag: CFL (various.f:665-987, incl. the merged-interface dz), extrema
+    and the rms of w below 0.2 zlen, against the oracle on the same state."""
+    s, o = run_pair(small, 5, fourier_scale=True)
+    d = s.diag()
+    o.maxcalc()
+    m = o.last_maxcalc()
+    assert np.allclose(d["cfl"], m["cfl"], rtol=1e-10, atol=1e-300)
+    mm = np.array(d["minmax"])
+    keep = [0, 2, 3, 4, 5, 6, 7]  # the reference's running umax adds an offset (umax) and is not reproduced
+    assert np.allclose(mm[keep], m["minmax"][keep], rtol=1e-10, atol=1e-14)
+    assert abs(d["wrms_bottom"] - o.diag()["wrms_bottom"]) <= 1e-10 * o.diag()["wrms_bottom"]
+    assert abs(d["ke"] - o.diag()["ke"]) <= 1e-10 * o.diag()["ke"]
+
+
 def test_steps_3d_faithful_filter(small):
     s, o = run_pair(small, 20, fourier_scale=False)
     a, b = s.state(), o.state()
