@@ -856,7 +856,7 @@ static ZOp<T, NM> make_zop(const iw_handle* h) {
   for (int k1 = 0; k1 < h->N; ++k1)
     for (int k2 = 0; k2 < h->N; ++k2) {
       op.D[k1 * NM + k2] = (T)h->tab.D[(size_t)k1 * h->N + k2];
-      op.L[k1 * NM + k2] = (T)(h->tab.Lfil[(size_t)k1 * h->N + k2] - (k1 == k2 ? 1.0 : 0.0));
+      op.L[k1 * NM + k2] = h->tab.Lfil[(size_t)k1 * h->N + k2] - (k1 == k2 ? 1.0 : 0.0);
     }
   return op;
 }
@@ -919,7 +919,7 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
     default: break;
   }
   dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
-  size_t smem = (size_t)(2 * h->N * h->N + 2 * h->N * kTX) * sizeof(T);
+  size_t smem = (size_t)h->N * h->N * sizeof(double) + (size_t)(h->N * h->N + 2 * h->N * kTX) * sizeof(T);
   k_stageE<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c);
 }
 
@@ -1251,7 +1251,7 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
     launch_y<T>(h, fs, jb, 1, ng * 4, false);
   }
   long total = (long)h->ny * h->nz * nf;
-  k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 1);
+  k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
   k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1);
   return 0;
 }

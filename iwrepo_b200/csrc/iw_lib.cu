@@ -483,13 +483,13 @@ template <typename T>
 __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int N = g.N;
-  T* sD = (T*)smraw;       // N*N
-  T* sL = sD + N * N;      // N*N
-  T* tz = sL + N * N;      // N*kTX: Z tile
-  T* tf = tz + N * kTX;    // N*kTX: F* tile
+  double* sL = (double*)smraw;  // N*N, L - I in FP64 (see below)
+  T* sD = (T*)(sL + N * N);     // N*N
+  T* tz = sD + N * N;           // N*kTX: Z tile
+  T* tf = tz + N * kTX;         // N*kTX: F* tile
   for (int t = threadIdx.x; t < N * N; t += blockDim.x) {
     sD[t] = (T)g.D[t];
-    sL[t] = (T)(g.Lfil[t] - (t / N == t % N ? 1.0 : 0.0));  // L - I, formed before rounding
+    sL[t] = g.Lfil[t] - (t / N == t % N ? 1.0 : 0.0);
   }
   const int q = blockIdx.z;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -529,16 +529,20 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
   }
   __syncthreads();
   if (!act) return;
-  const T cfm1 = a.filter ? (T)(g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0) : (T)0;
+  // The Legendre filter acts on the state itself every step: L - I has O(1)
+  // entries (a projector onto the damped modes), so FP32 entries would add
+  // the same rounding error to the state each step.  It runs in FP64 with
+  // one rounding of the result; cf - 1 is small for the energetic modes.
+  const double cfm1 = a.filter ? g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0 : 0.0;
   for (int k1 = w; k1 < N; k1 += kTW) {
     T o;
     if (a.filter) {
-      const T* lr = sL + k1 * N;
-      T s = 0;
+      const double* lr = sL + k1 * N;
+      double s = 0;
 #pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) s += lr[k2] * tf[k2 * kTX + lane];
-      const T gv = tf[k1 * kTX + lane] + s;  // L f = f + (L - I) f
-      o = gv + cfm1 * gv;                    // cf g = g + (cf - 1) g
+      for (int k2 = 0; k2 < N; ++k2) s += lr[k2] * (double)tf[k2 * kTX + lane];
+      const double gv = (double)tf[k1 * kTX + lane] + s;  // L f = f + (L - I) f
+      o = (T)(gv + cfm1 * gv);                            // cf g = g + (cf - 1) g
     } else {
       o = tf[k1 * kTX + lane];
     }
@@ -559,8 +563,8 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
 // ---------------------------------------------------------------------------
 template <typename T, int NM>
 struct ZOp {
-  T D[NM * NM];  // D[k1*NM + k2], zero outside N x N
-  T L[NM * NM];  // precombined Legendre filter minus the identity, same layout
+  T D[NM * NM];       // D[k1*NM + k2], zero outside N x N
+  double L[NM * NM];  // precombined Legendre filter minus the identity, same layout (FP64, see k_stageE)
 };
 
 template <typename T, int NM>
@@ -669,17 +673,17 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
     }
     fs[k1] = fsv;
   }
-  const T cfm1 = a.filter ? (T)(g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0) : (T)0;
+  const double cfm1 = a.filter ? g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0 : 0.0;
 #pragma unroll
   for (int k1 = 0; k1 < NM; ++k1) {
     if (k1 < N) {
       T o;
       if (a.filter) {
-        T s = 0;
+        double s = 0;
 #pragma unroll
-        for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * fs[k2];  // (L - I) f
-        const T gv = fs[k1] + s;
-        o = gv + cfm1 * gv;
+        for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * (double)fs[k2];  // (L - I) f in FP64
+        const double gv = (double)fs[k1] + s;
+        o = (T)(gv + cfm1 * gv);
       } else {
         o = fs[k1];
       }
@@ -2095,7 +2099,8 @@ __global__ void k_project_planes(Geo g, T* F0, T* F1, T* F2, T* F3, int skip_ifa
 }
 
 // gather the 4 planes around each interface into a compact buffer:
-// G[(q*(ns-1)+f)*4 + m] plane = F_q level (f+1)*N - 2 + m
+// G[(q*(ns-1)+f)*4 + m] plane = F_q level (f+1)*N - 2 + m; back: add the
+// averaging change held in G to the two interface planes.
 template <typename T>
 __global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, const T* F3, T* G, int back) {
   long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2112,12 +2117,12 @@ __global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, con
   if (!back) {
     G[pl * per + e] = F[(size_t)k * per + e];
   } else if (m == 1 || m == 2) {
-    ((T*)F)[(size_t)k * per + e] = G[pl * per + e];
+    ((T*)F)[(size_t)k * per + e] += G[pl * per + e];  // spectral change made by the averaging
   }
 }
 
 // per (row j, interface plane group): x-inverse of 4 rows, average, x-forward
-// of the 2 interface rows.
+// of the change of the 2 interface rows.
 template <typename T>
 __global__ void k_iface_rows(Geo g, T* G, FftPlan pl, const typename cplx_t<T>::type* __restrict__ Wm,
                              const typename cplx_t<T>::type* __restrict__ Wn, int* counts) {
@@ -2137,16 +2142,22 @@ __global__ void k_iface_rows(Geo g, T* G, FftPlan pl, const typename cplx_t<T>::
   C* ph = fft_run<C>(A, B, pl, 4, Wm, true, threadIdx.x, blockDim.x);
   T* P = (T*)ph;
   int cnt = 0;
+  // The interface rows become the change made by the averaging (0 where it
+  // does not trigger): the spectral planes are then P(F) + transform of the
+  // change, so points left alone never take the round trip's rounding.
   for (int i = threadIdx.x; i < nx; i += blockDim.x) {
     T fsp = P[2 * nx + i], fsm = P[1 * nx + i];
     T favg2 = fsp + fsm;
     T c0 = fabs(fsp - fsm) / fabs(favg2);
+    T d1 = 0, d2 = 0;
     if (c0 > (T)0.005) {
       T ff = P[0 * nx + i] * (T)0.5 + P[1 * nx + i] * (T)0 + P[2 * nx + i] * (T)0 + P[3 * nx + i] * (T)0.5;
-      P[1 * nx + i] = ff;
-      P[2 * nx + i] = ff;
+      d1 = ff - fsm;
+      d2 = ff - fsp;
       ++cnt;
     }
+    P[1 * nx + i] = d1;
+    P[2 * nx + i] = d2;
   }
   if (cnt) atomicAdd(counts + q, cnt);
   __syncthreads();
