@@ -349,6 +349,11 @@ struct iw_handle {
   double bi_bdfv[SYS_KINDS] = {-1, -1, -1, -1};
   bool bi_f32[SYS_KINDS] = {false, false, false, false};
   bool bi_fold[SYS_KINDS] = {false, false, false, false};  // Legendre filter folded into ainv
+  // distinct subdomain blocks: subdomain ks uses block bmap[ks]; brep[b] is a
+  // subdomain of block b
+  int nb = 0;
+  int bmap[IW_MAX_SUBD] = {};
+  int brep[IW_MAX_SUBD] = {};
   double bi_dt[SYS_KINDS] = {-1, -1, -1, -1};
   double fac_bdfv[SYS_KINDS] = {-1, -1, -1, -1};  // bdfv the factors were built for
   double fac_dt[SYS_KINDS] = {-1, -1, -1, -1};
@@ -699,7 +704,7 @@ static int build_blockinv(iw_handle* h, int kind, bool fold) {
     cudaFree(B.colsys);
     B = iw_handle::BI();
     char* ai = nullptr;
-    if (dalloc(h, &ai, (size_t)std::max(nsys, 1) * ns * N * N * tib) ||
+    if (dalloc(h, &ai, (size_t)std::max(nsys, 1) * h->nb * N * N * tib) ||
         dalloc(h, &B.cvec, (size_t)std::max(nsys, 1) * ns * N) || dalloc(h, &B.dvec, (size_t)std::max(nsys, 1) * ns * N) ||
         dalloc(h, &B.minv, (size_t)std::max(nsys, 1) * std::max(m * m, 1)) ||
         dalloc(h, &B.pen, (size_t)std::max(nsys, 1) * 6 * ns) || dalloc(h, &B.sys, (size_t)std::max(nsys, 1)) ||
@@ -738,7 +743,7 @@ static int build_blockinv(iw_handle* h, int kind, bool fold) {
     cudaFree(B.ainv_raw);
     B.ainv_raw = nullptr;
     B.nsys_raw = nraw;
-    if (nraw > 0 && dalloc(h, &B.ainv_raw, (size_t)nraw * ns * N * N)) return IW_ERR_NOMEM;
+    if (nraw > 0 && dalloc(h, &B.ainv_raw, (size_t)nraw * h->nb * N * N)) return IW_ERR_NOMEM;
   }
   // chunked: assemble -> invert blocks -> interface matrix -> store
   const int CH = std::max(1, std::min(nsys, (int)(1200000000ull / ((size_t)ldab * n * 8 + (size_t)ns * N * N * 8 + 1))));
@@ -777,17 +782,15 @@ static int build_blockinv(iw_handle* h, int kind, bool fold) {
       k_left_vecs<<<1184, 256, 0, h->st>>>(g, cn, tinv, B.cvec + (size_t)s0 * ns * N, B.dvec + (size_t)s0 * ns * N,
                                          B.lvec + (size_t)s0 * m * N);
     const size_t cnt = (size_t)cn * ns * N * N;
+    BlockRep rep;
+    memcpy(rep.r, h->brep, sizeof rep.r);
+    const int nb = h->nb;
     if (fold && s0 < B.nsys_raw)
-      CK(cudaMemcpyAsync(B.ainv_raw + (size_t)s0 * ns * N * N, tinv,
-                         (size_t)(std::min(B.nsys_raw, s0 + cn) - s0) * ns * N * N * sizeof(double),
-                         cudaMemcpyDeviceToDevice, h->st));
-    if (f32)
-      k_convert<double, float><<<2048, 256, 0, h->st>>>(tinv, (float*)B.ainv + (size_t)s0 * ns * N * N, cnt);
-    else if (fold)
-      k_fold_filter<<<2368, 256, 0, h->st>>>(N, (size_t)cn * ns, h->dL, tinv, (double*)B.ainv + (size_t)s0 * ns * N * N);
-    else
-      CK(cudaMemcpyAsync((double*)B.ainv + (size_t)s0 * ns * N * N, tinv, cnt * sizeof(double),
-                         cudaMemcpyDeviceToDevice, h->st));
+      k_compact_blocks<<<2368, 256, 0, h->st>>>(N, std::min(B.nsys_raw, s0 + cn) - s0, ns, nb, rep, nullptr, tinv,
+                                                B.ainv_raw + (size_t)s0 * nb * N * N);
+    k_compact_blocks<<<2368, 256, 0, h->st>>>(N, cn, ns, nb, rep, fold ? h->dL : nullptr, tinv,
+                                              (double*)B.ainv + (size_t)s0 * nb * N * N);
+    (void)cnt;
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(h->st));
@@ -1138,6 +1141,8 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   bi.col_sys = h->bi[kind].colsys;
   bi.col_order = h->dcolorder;
   bi.lvec = h->bi[kind].lvec;
+  bi.nb = h->nb;
+  memcpy(bi.bmap, h->bmap, sizeof bi.bmap);
   const int mm = std::max(2 * (h->ns - 1), 1);
   const size_t sm = ((size_t)2 * R * h->nz + 2 * R * mm) * sizeof(double);
   T *F0, *F1 = nullptr, *F2 = nullptr;
@@ -1527,6 +1532,21 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
     return IW_ERR_NOMEM;
   }
   build_distinct(h);
+  // distinct subdomain blocks of the penalty systems: a block is fixed by
+  // epsilon, its height and whether it has neighbours below and above
+  h->nb = 0;
+  for (int ks = 0; ks < h->ns; ++ks) {
+    int found = -1;
+    for (int b = 0; b < h->nb && found < 0; ++b) {
+      const int r = h->brep[b];
+      if ((r > 0) == (ks > 0) && (r < h->ns - 1) == (ks < h->ns - 1) && prm->zh[r] == prm->zh[ks]) found = b;
+    }
+    if (found < 0) {
+      found = h->nb;
+      h->brep[h->nb++] = ks;
+    }
+    h->bmap[ks] = found;
+  }
   h->c = Coefs{1., 0., 0., 1., 0., 0., 1., prm->dt};
   *out = h;
   return IW_OK;

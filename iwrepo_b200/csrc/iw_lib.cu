@@ -1296,7 +1296,13 @@ __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ 
 // stored column major per block in TI (float for the mixed path).
 // ===========================================================================
 struct BlockInv {
-  const void* ainv;     // per system: ns blocks of N*N, [ks][col][row]
+  // per system: nb distinct blocks of N*N, [block][col][row].  Subdomain ks
+  // uses block bmap[ks]: a block is fixed by epsilon, the subdomain height and
+  // whether it has neighbours below and above, so with equal heights the
+  // interior subdomains share one inverse.
+  const void* ainv;
+  int nb;
+  int bmap[IW_MAX_SUBD];
   const double* cvec;   // per system: ns*N (c_ks, ks>=1)
   const double* dvec;   // per system: ns*N (d_ks, ks<=ns-2)
   const double* minv;   // per system: m*m, m = 2(ns-1), row major
@@ -1703,9 +1709,9 @@ constexpr int kSolveThreads = 128;
 // dst = (accum ? dst : 0) + A^-1 src for R right-hand sides of length n.
 // rz, zz: R*m doubles of shared scratch.  Ends synchronised.
 template <int R>
-__device__ void bi_apply_cta(const Geo& g, const double* __restrict__ ainv, const double* __restrict__ lvec,
-                             const double* __restrict__ minv, const double* src, double* dst, double* rz, double* zz,
-                             bool accum) {
+__device__ void bi_apply_cta(const Geo& g, const double* __restrict__ ainv, const int* bmap,
+                             const double* __restrict__ lvec, const double* __restrict__ minv, const double* src,
+                             double* dst, double* rz, double* zz, bool accum) {
   const int N = g.N, ns = g.ns, n = g.nz, m = 2 * (ns - 1);
   const int tid = threadIdx.x;
   if (m > 0) {
@@ -1733,7 +1739,7 @@ __device__ void bi_apply_cta(const Geo& g, const double* __restrict__ ainv, cons
   }
   for (int row = tid; row < n; row += kSolveThreads) {
     const int ks = row / N, kk = row - ks * N;
-    const double* ai = ainv + (size_t)ks * N * N + kk;
+    const double* ai = ainv + (size_t)bmap[ks] * N * N + kk;
     const double* sv = src + ks * N;
     double acc[R];
 #pragma unroll
@@ -1947,13 +1953,13 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
       }
     }
     __syncthreads();
-    const double* ainv = (const double*)bi.ainv + (size_t)s * ns * N * N;
+    const double* ainv = (const double*)bi.ainv + (size_t)s * bi.nb * N * N;
     const double* lv = bi.lvec + (size_t)s * (m > 0 ? m : 1) * N;
     const double* mi = bi.minv + (size_t)s * (m > 0 ? m * m : 1);
-    bi_apply_cta<R>(g, ainv, lv, mi, b, x, rz, zz, false);
+    bi_apply_cta<R>(g, ainv, bi.bmap, lv, mi, b, x, rz, zz, false);
     if (refine) {
       sub_A_cta<R>(g, D2t, zh, eps, bi.pen + (size_t)s * 6 * ns, x, b);
-      bi_apply_cta<R>(g, ainv, lv, mi, b, x, rz, zz, true);
+      bi_apply_cta<R>(g, ainv, bi.bmap, lv, mi, b, x, rz, zz, true);
     }
     if (cpen) {
       legen_filter_cta<R>(g, Lt, x, b);
@@ -2014,6 +2020,33 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
         if (role == 0 && rr < 2 && meanu && cii[ci] == 0 && cj[ci] == 0) v = tb.meang[k] * v;
         F[fidx<T>(g, 2 * cii[ci] + (rr & 1), cj[ci], k)] = (T)v;
       }
+    }
+  }
+}
+
+// Distinct blocks of each system into compact storage: out[s][b] = in[s][rep[b]],
+// with the Legendre filter folded in when L is given (out = L in, per column).
+struct BlockRep {
+  int r[IW_MAX_SUBD];
+};
+__global__ void k_compact_blocks(int N, int nsys, int ns, int nb, BlockRep rep, const double* __restrict__ L,
+                                 const double* __restrict__ in, double* __restrict__ out) {
+  const size_t nn = (size_t)N * N, tot = (size_t)nsys * nb * nn;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = q % nn;
+    const size_t sb = q / nn;
+    const int b = (int)(sb % nb);
+    const size_t s = sb / nb;
+    const double* src = in + (s * ns + rep.r[b]) * nn;
+    if (!L) {
+      out[q] = src[e];
+    } else {
+      const int kk = (int)(e % N);
+      const double* col = src + (e - kk);
+      const double* lr = L + (size_t)kk * N;
+      double acc = 0.0;
+      for (int j = 0; j < N; ++j) acc += lr[j] * col[j];
+      out[q] = acc;
     }
   }
 }
