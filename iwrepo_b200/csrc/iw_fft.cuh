@@ -301,4 +301,72 @@ struct FftOcc {
   static constexpr int v = sizeof(T) == 4 ? (DPT <= 8 ? 4 : DPT <= 16 ? 2 : 1) : (DPT <= 4 ? 4 : DPT <= 8 ? 2 : 1);
 };
 
+
+// ---------------------------------------------------------------------------
+// Compile-time plans for power-of-two lengths M (same passes as make_plan:
+// ceil(log2 M / 3) passes of radix <= 8, bits spread evenly).  Strides,
+// twiddle steps and lane guards become constants.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int ct_log2(int v) { return v <= 1 ? 0 : 1 + ct_log2(v / 2); }
+template <int M>
+struct CtPlan {
+  static constexpr int a = ct_log2(M);
+  static constexpr int np = (a + 2) / 3;
+  __host__ __device__ static constexpr int bits(int q) { return a / np + (q < a % np ? 1 : 0); }
+};
+
+template <typename C, int M, int R, int NS>
+__device__ __forceinline__ void fft_pass_ct(C* row, const C* __restrict__ W, bool inv, int lane) {
+  constexpr int nb = M / R;
+  constexpr int step = M / (NS * R);
+  constexpr int NB = (nb + 31) / 32;
+  C v[NB][R];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int j = lane + 32 * q;
+    if (nb % 32 == 0 || j < nb) {
+      const int jm = j & (NS - 1);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q][r] = row[fpad(j + r * nb)];
+      if (NS > 1) {
+        const int e = jm * step;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C tw = W[r * e];
+          if (inv) tw.y = -tw.y;
+          v[q][r] = cmul(v[q][r], tw);
+        }
+      }
+      dft_reg<C, R>(v[q], inv);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int j = lane + 32 * q;
+    if (nb % 32 == 0 || j < nb) {
+      const int jq = j / NS, jm = j & (NS - 1);
+      const int base = jq * NS * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) row[fpad(base + r * NS)] = v[q][r];
+    }
+  }
+  __syncwarp();
+}
+
+template <typename C, int M, int P, int NS>
+__device__ __forceinline__ void fft_passes_ct(C* row, const C* __restrict__ W, bool inv, int lane) {
+  if constexpr (P < CtPlan<M>::np) {
+    constexpr int R = 1 << CtPlan<M>::bits(P);
+    fft_pass_ct<C, M, R, NS>(row, W, inv, lane);
+    fft_passes_ct<C, M, P + 1, NS * R>(row, W, inv, lane);
+  }
+}
+
+// In-place transform of one padded row of power-of-two length M by one warp.
+template <typename C, int M>
+__device__ __forceinline__ void fft_warp_ct(C* row, const C* __restrict__ W, bool inv, int lane) {
+  fft_passes_ct<C, M, 0, 1>(row, W, inv, lane);
+}
+
 }  // namespace iw

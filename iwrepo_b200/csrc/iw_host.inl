@@ -945,6 +945,21 @@ static void launch_y_tx(iw_handle* h, YJobs<T>& jobs, dim3 grid, size_t smem, in
                         const typename cplx_t<T>::type* Wy) {
   Geo g = geo(h);
   const bool p2 = (h->ny & (h->ny - 1)) == 0;
+  if constexpr (TX == 8) {  // compile-time plans for the common power-of-two lengths
+    switch (p2 ? h->ny : 0) {
+#define IW_YCT(MC, D)                                                                                        \
+  case MC:                                                                                                   \
+    cudaFuncSetAttribute(k_yfft<T, TX, D, true, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    k_yfft<T, TX, D, true, MC><<<grid, 256, smem, h->st>>>(g, jobs, nplanes, h->ply, Wy);                    \
+    return;
+      IW_YCT(64, 4)
+      IW_YCT(128, 4)
+      IW_YCT(256, 8)
+      IW_YCT(512, 16)
+#undef IW_YCT
+      default: break;
+    }
+  }
   switch (fft_dpt(h->ny) * (p2 ? 1 : -1)) {
 #define IW_YCASE(D, P)                                                                                       \
   case (P ? D : -D):                                                                                         \
@@ -1059,6 +1074,20 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
     const size_t smem = 20 * (size_t)xstride(M) * sizeof(C);
     dim3 grid(h->ny, h->nz);
     const bool p2 = (M & (M - 1)) == 0;
+    switch (p2 && M >= 32 && M <= 512 ? M : 0) {  // compile-time plans for power-of-two lengths
+#define IW_XCT(MC, D)                                                                                       \
+  case MC:                                                                                                  \
+    cudaFuncSetAttribute(k_xrow_nl<T, D, true, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    k_xrow_nl<T, D, true, MC><<<grid, 256, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);                     \
+    goto xrow_done;
+      IW_XCT(32, 4)
+      IW_XCT(64, 4)
+      IW_XCT(128, 4)
+      IW_XCT(256, 8)
+      IW_XCT(512, 16)
+#undef IW_XCT
+      default: break;
+    }
     switch (fft_dpt(M) * (p2 ? 1 : -1)) {
 #define IW_XCASE(D, P)                                                                                   \
   case (P ? D : -D):                                                                                     \
@@ -1075,6 +1104,7 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
       IW_XCASE(32, false)
 #undef IW_XCASE
     }
+  xrow_done:;
   }
   mark(h, 2);
   // K_D: y-forward; B_q = Y(A_q) + i ky Y(P_q), Z_q = Y(P_zq)

@@ -161,7 +161,7 @@ __host__ __device__ __forceinline__ int ystride(int ny) {
   return s + ((2 - s) % 16 + 16) % 16;
 }
 
-template <typename T, int TX, int DPT, bool POW2>
+template <typename T, int TX, int DPT, bool POW2, int MC = 0>
 __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<T> jobs, int nplanes, FftPlan pl,
                                               const typename cplx_t<T>::type* __restrict__ Wy) {
   typedef typename cplx_t<T>::type C;
@@ -207,7 +207,10 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int r = threadIdx.x >> 5; r < nrow; r += nw) {
     C* row = r < nb ? A + r * RSY : A2 + (r - nb) * RSY;
-    fft_warp<C, DPT, POW2>(row, pl, Wy, !fwd, lane);
+    if constexpr (MC > 0)
+      fft_warp_ct<C, MC>(row, Wy, !fwd, lane);
+    else
+      fft_warp<C, DPT, POW2>(row, pl, Wy, !fwd, lane);
   }
   __syncthreads();
   const T sc = fwd ? (T)g.scaley : (T)1;
@@ -332,7 +335,7 @@ __host__ __device__ __forceinline__ int xstride(int M) { return fpadlen(M + 1); 
 
 // K_C: CTA per (j,k) row; 20 padded rows of M+1 values in shared memory; each
 // warp transforms whole rows in place.
-template <typename T, int DPT, bool POW2>
+template <typename T, int DPT, bool POW2, int MC = 0>
 __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLArgs<T> a, FftPlan pl,
                                                  const typename cplx_t<T>::type* __restrict__ Wm,
                                                  const typename cplx_t<T>::type* __restrict__ Wn) {
@@ -367,7 +370,12 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
     xprep_pair<C, T>(buf + r * RS, kk, M, Wn, r >= 4 && r < 8, kxs);
   }
   __syncthreads();
-  for (int r = wid; r < nrow; r += nw) fft_warp<C, DPT, POW2>(buf + r * RS, pl, Wm, true, lane);
+  for (int r = wid; r < nrow; r += nw) {
+    if constexpr (MC > 0)
+      fft_warp_ct<C, MC>(buf + r * RS, Wm, true, lane);
+    else
+      fft_warp<C, DPT, POW2>(buf + r * RS, pl, Wm, true, lane);
+  }
   __syncthreads();
   // physical value i of row r
   auto P = [&](int r, int i) -> T& { return ((T*)(buf + r * RS))[2 * fpad(i >> 1) + (i & 1)]; };
@@ -422,7 +430,12 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
     P(12, i) = -(w * t);
   }
   __syncthreads();
-  for (int r = wid; r < 13; r += nw) fft_warp<C, DPT, POW2>(buf + r * RS, pl, Wm, false, lane);
+  for (int r = wid; r < 13; r += nw) {
+    if constexpr (MC > 0)
+      fft_warp_ct<C, MC>(buf + r * RS, Wm, false, lane);
+    else
+      fft_warp<C, DPT, POW2>(buf + r * RS, pl, Wm, false, lane);
+  }
   __syncthreads();
   const T invN = (T)1 / (T)nx;
   // outputs: A_q = X(Q_q) + i kx X(P_uq) for q = u v w t ; then uv vv vw vt uw ww wt
