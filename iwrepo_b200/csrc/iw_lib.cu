@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
                                               const typename cplx_t<T>::type* __restrict__ Wy) {
   typedef typename cplx_t<T>::type C;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int ny = g.ny;
+  const int ny = MC > 0 ? MC : g.ny;  // a constant with a compile-time plan
   const int RSY = ystride(ny);
   C* A = (C*)smraw;
   C* A2 = A + (size_t)TX * RSY;
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
                                                  const typename cplx_t<T>::type* __restrict__ Wn) {
   typedef typename cplx_t<T>::type C;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int M = g.nx / 2;
+  const int M = MC > 0 ? MC : g.nx / 2;  // a constant with a compile-time plan
   const int RS = xstride(M);
   C* buf = (C*)smraw;
   const int j = blockIdx.x, k = blockIdx.y;
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
   __syncthreads();
   // physical value i of row r
   auto P = [&](int r, int i) -> T& { return ((T*)(buf + r * RS))[2 * fpad(i >> 1) + (i & 1)]; };
-  const int nx = g.nx;
+  const int nx = 2 * M;
   // upwind interface penalty (solver.f:700-839); products overwrite rows 0..12
   for (int i = tid; i < nx; i += nthr) {
     const T u = P(0, i), v = P(1, i), w = P(2, i), t = P(3, i);
