@@ -222,6 +222,7 @@ def run_ours(args, rank, world):
     seed = 1000 + rank
     s = iw.Solver(cfg, device=dev)
     s.init_mode1(amp, noise, seed)
+    tuning = s.autotune()  # launch choices for this device and size (state unchanged)
     ext = torch.cuda.ExternalStream(s.stream())
 
     def barrier():
@@ -358,7 +359,7 @@ def run_ours(args, rank, world):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 fields/FFTs + f64 solves" if args.precision == "mixed" else "f64",
             "data": "synthetic (mode-1 wave + seeded noise)",
-            "config": describe(cfg, args.precision),
+            "config": dict(describe(cfg, args.precision), tuning=tuning),
             "e2e": line_e2e, "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "roofline": roofline, "step_roofline_frac": step_frac, "phases": phases,
             "cpu_baseline": cpu, "clocks": clk,

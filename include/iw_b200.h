@@ -170,6 +170,15 @@ int iw_step(iw_handle *h);
  * per call and freed before it returns. */
 int iw_run(iw_handle *h, int nsteps, int use_graph);
 
+/* Not in the reference.  Times the launch candidates of this handle's step on
+ * its device and keeps the fastest for the following steps: y-tile width (2, 4
+ * or 8 columns) and the stage-A and stage-E variants (register-column or
+ * tiled).  Candidates run on the handle's scratch fields; the state is not
+ * changed.  The stage variants differ only in the order of floating-point sums.
+ * choices (optional, 3 ints): the y-tile width, and for stage A and stage E
+ * 1 = register-column, 0 = tiled, -1 = not applicable. */
+int iw_autotune(iw_handle *h, int *choices);
+
 /* Not in the reference (its main.f advances one run).  Advances n independent
  * runs of any sizes (separate handles on one device) by nsteps steps each.
  * Steps run eagerly until every member is invariant as for iw_run.  After

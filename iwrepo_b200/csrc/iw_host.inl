@@ -353,6 +353,10 @@ struct iw_handle {
   // subdomain of block b
   int nb = 0;
   int bmap[IW_MAX_SUBD] = {};
+  // launch choices set by iw_autotune (0 / -1: built-in heuristic)
+  int tune_ytx = 0;  // y-tile width
+  int tune_a = -1;   // stage A: 1 register-column, 0 tiled
+  int tune_e = -1;   // stage E: 1 register-column, 0 tiled
   int brep[IW_MAX_SUBD] = {};
   double bi_dt[SYS_KINDS] = {-1, -1, -1, -1};
   double fac_bdfv[SYS_KINDS] = {-1, -1, -1, -1};  // bdfv the factors were built for
@@ -873,7 +877,7 @@ static void launch_stageA_r(iw_handle* h, FieldSet<T>& fs, int proj) {
 
 template <typename T>
 static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
-  switch (zop_bucket(h->N)) {
+  switch (h->tune_a == 0 ? 0 : zop_bucket(h->N)) {
     case 9: launch_stageA_r<T, 9>(h, fs, proj); return;
     case 17: launch_stageA_r<T, 17>(h, fs, proj); return;
     case 21: launch_stageA_r<T, 21>(h, fs, proj); return;
@@ -907,7 +911,8 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   // The register-column stage E holds two columns per thread; past these sizes
   // its register count costs more occupancy than the tiled kernel loses.
   const int emax = sizeof(T) == 4 ? 25 : 17;
-  switch (h->N <= emax ? zop_bucket(h->N) : 0) {
+  const bool reg = h->tune_e < 0 ? h->N <= emax : h->tune_e == 1;
+  switch (reg ? zop_bucket(h->N) : 0) {
 #define IW_ECASE(NM)                                                                          \
   case NM:                                                                                    \
     k_stageE_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, make_zop<T, NM>(h));         \
@@ -935,7 +940,7 @@ static int fft_dpt(int M) {
 template <typename T>
 static int ytx(const iw_handle* h, bool two) {  // y-FFT tile width
   const size_t cs = 2 * sizeof(T);
-  int tx = 8;
+  int tx = h->tune_ytx > 0 ? h->tune_ytx : 8;
   while (tx > 1 && (two ? 2 : 1) * (size_t)tx * ystride(h->ny) * cs > 110 * 1024) tx /= 2;
   return tx;
 }
@@ -1309,6 +1314,97 @@ static int full_step(iw_handle* h, FieldSet<T>& fs) {
   prof_flush(h);
   CK(cudaGetLastError());
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuning of launch choices: candidates are timed with CUDA events on the
+// handle's stream, on zero-filled scratch fields standing in for the state
+// (the state itself is not touched; the scratch is rewritten by the next step).
+// Choices: y-tile width (2, 4, 8 columns), stage A and stage E variant
+// (register-column or tiled).  All candidates compute the same step; the stage
+// variants differ only in the order of floating-point sums.
+// ---------------------------------------------------------------------------
+template <typename T>
+static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
+  const size_t n = h->ntot;
+  for (auto* a : fs.Y12) CK(cudaMemsetAsync(a, 0, n * sizeof(T), h->st));
+  for (auto* a : fs.X11) CK(cudaMemsetAsync(a, 0, n * sizeof(T), h->st));
+  for (auto* a : fs.B8) CK(cudaMemsetAsync(a, 0, n * sizeof(T), h->st));
+  FieldSet<T> ts = fs;  // state arrays pointed at scratch
+  for (int q = 0; q < 4; ++q) {
+    ts.F[q] = fs.Y12[q];
+    ts.F1[q] = fs.Y12[4 + q];
+    ts.Z4[q] = fs.Y12[8 + q];
+    ts.Fn[q] = fs.X11[q];
+    ts.Fnm[q] = fs.X11[4 + q];
+    ts.Sn[q] = fs.X11[7 + q];
+    ts.Snm[q] = fs.B8[q];
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto timeit = [&](auto&& launch) {
+    launch();
+    cudaEventRecord(e0, h->st);
+    for (int r = 0; r < 3; ++r) launch();
+    cudaEventRecord(e1, h->st);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  const int save[3] = {h->tune_ytx, h->tune_a, h->tune_e};
+  // y tiles: the 12-job inverse and the 4-job forward-with-fold launches
+  float best = 1e30f;
+  int besttx = 8;
+  for (int tx : {8, 4, 2}) {
+    h->tune_ytx = tx;
+    if (ytx<T>(h, true) != tx) continue;  // does not fit in shared memory
+    const float ms = timeit([&] {
+      YJobs<T> ji, jf;
+      memset(&ji, 0, sizeof ji);
+      memset(&jf, 0, sizeof jf);
+      for (int q = 0; q < 11; ++q) ji.j[q] = YJob<T>{fs.Y12[q], nullptr, fs.X11[q], q < 4 ? 0 : 1};
+      for (int q = 0; q < 4; ++q) jf.j[q] = YJob<T>{fs.X11[q], fs.X11[4 + q], fs.B8[4 + q], 3};
+      launch_y<T>(h, ts, ji, 11, h->nz, false);
+      launch_y<T>(h, ts, jf, 4, h->nz, true);
+    });
+    if (ms < best) {
+      best = ms;
+      besttx = tx;
+    }
+  }
+  h->tune_ytx = besttx;
+  // stage A and stage E variants
+  int besta = -1, beste = -1;
+  if (zop_bucket(h->N)) {
+    float ta[2], te[2];
+    for (int v = 0; v < 2; ++v) {
+      h->tune_a = v;
+      ta[v] = timeit([&] { launch_stageA<T>(h, ts, 1); });
+      h->tune_e = v;
+      te[v] = timeit([&] { launch_stageE<T>(h, ts); });
+    }
+    besta = ta[1] <= ta[0] ? 1 : 0;
+    beste = te[1] <= te[0] ? 1 : 0;
+  }
+  h->tune_a = besta;
+  h->tune_e = beste;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    h->tune_ytx = save[0];
+    h->tune_a = save[1];
+    h->tune_e = save[2];
+    return set_err(IW_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(err));
+  }
+  if (choice) {
+    choice[0] = h->tune_ytx;
+    choice[1] = h->tune_a;
+    choice[2] = h->tune_e;
+  }
+  return IW_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1701,6 +1797,12 @@ int iw_run(iw_handle* h, int nsteps, int use_graph) {
     if (r) return r;
   }
   return run_graphs(&h, 1, nsteps - s);
+}
+
+int iw_autotune(iw_handle* h, int* choices) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  cudaSetDevice(h->dev);
+  return h->mixed ? tune_impl<float>(h, h->f32, choices) : tune_impl<double>(h, h->f64, choices);
 }
 
 int iw_ensemble_run(iw_handle* const* members, int n, int nsteps) {

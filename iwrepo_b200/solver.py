@@ -98,6 +98,14 @@ class Solver:
     def step(self, n: int = 1):
         _lib.check(_lib.lib().iw_run(self.h, n, 0))
 
+    def autotune(self) -> dict:
+        """Time this step's launch candidates and keep the fastest (y-tile
+        width, stage A / stage E variant); the state is not changed."""
+        ch = (C.c_int * 3)()
+        _lib.check(_lib.lib().iw_autotune(self.h, ch))
+        names = {1: "register", 0: "tiled", -1: "n/a"}
+        return {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]]}
+
     def run(self, n: int, graph: bool = True):
         """n steps; with graph=True the invariant steady-state step is replayed
         from captured CUDA graphs (identical results, one launch per step)."""

@@ -57,3 +57,27 @@ def test_ensemble_of_uneven_members_equals_individual_runs():
             assert np.array_equal(x, y)
     for s in ens + alone:
         s.close()
+
+
+@pytest.mark.parametrize("precision,tol", [(cf.IW_PREC_FP64, 1e-11), (cf.IW_PREC_MIXED, 1e-5)])
+def test_autotune_keeps_results(precision, tol):
+    """iw_autotune only changes launch choices: the state is untouched and the
+    following steps agree with an untuned run to rounding."""
+    import iwrepo_b200 as iw
+    cfg = cf.Config(nx=32, ny=32, nzloc=9, nsubd=3, dt=1e-3, precision=precision).validate()
+    a, b = iw.Solver(cfg), iw.Solver(cfg)
+    for s in (a, b):
+        s.init_mode1(0.05, 1e-4, 31)
+    a.step(2)
+    b.step(2)
+    before = b.state(0)
+    ch = b.autotune()
+    assert ch["y_tile"] in (2, 4, 8) and ch["stage_a"] in ("register", "tiled") and ch["stage_e"] in ("register", "tiled")
+    assert np.array_equal(before, b.state(0))
+    a.step(6)
+    b.step(6)
+    for x, y in zip(_all_levels(a), _all_levels(b)):
+        for q in range(4):
+            assert np.linalg.norm(x[q] - y[q]) <= tol * max(np.linalg.norm(y[q]), 1e-300)
+    a.close()
+    b.close()
