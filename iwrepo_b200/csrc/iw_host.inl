@@ -347,7 +347,6 @@ struct iw_handle {
   // estimated condition number above kRefineCond (small kx^2+ky^2 pressure)
   int nrefine[SYS_KINDS] = {0, 0, 0, 0};
   double bi_bdfv[SYS_KINDS] = {-1, -1, -1, -1};
-  bool bi_f32[SYS_KINDS] = {false, false, false, false};
   bool bi_fold[SYS_KINDS] = {false, false, false, false};  // Legendre filter folded into ainv
   // distinct subdomain blocks: subdomain ks uses block bmap[ks]; brep[b] is a
   // subdomain of block b
@@ -367,7 +366,6 @@ struct iw_handle {
   Coefs c{1, 0, 0, 1, 0, 0, 1, 0};
   int avg_count[4] = {0, 0, 0, 0};
   size_t bytes = 0;
-  cudaGraphExec_t gexec = 0;
   // helm batched
   std::map<std::string, int> helm_keys;
   // per-phase timing with CUDA events on the handle's stream
@@ -688,8 +686,7 @@ static void enumerate_systems(iw_handle* h, int kind, std::vector<SysDesc>& sys,
 // block inverses (FP32 for the mixed path, FP64 otherwise) of one kind
 static int build_blockinv(iw_handle* h, int kind, bool fold) {
   const int ns = h->ns, N = h->N, n = h->nz, ldab = 3 * N + 1, m = 2 * (ns - 1);
-  const bool f32 = false;  // the solves run in FP64 in both precisions
-  const size_t tib = f32 ? sizeof(float) : sizeof(double);
+  const size_t tib = sizeof(double);  // the solves run in FP64 in both precisions
   std::vector<SysDesc> sys;
   std::vector<double> pen;
   std::vector<int> colsys;
@@ -724,7 +721,6 @@ static int build_blockinv(iw_handle* h, int kind, bool fold) {
   }
   CK(scopy(h, B.colsys, colsys.data(), colsys.size() * sizeof(int), cudaMemcpyHostToDevice));
   if (build_tasks(h, kind, colsys, kind == SYS_U ? 1 : 2)) return IW_ERR_NOMEM;
-  h->bi_f32[kind] = f32;
   {
     // cond(I - eps (2/h)^2 D2 + penalty) <~ 1 + eps max_ks (2/h_ks)^2 |D2|_inf
     double d2n = 0;
@@ -1224,7 +1220,6 @@ static int calcuvwt_impl(iw_handle* h, FieldSet<T>& fs, int cpen) {
   const unsigned nblk = (unsigned)((h->ncol + warps - 1) / warps);
   const size_t smem = (size_t)warps * 4 * h->nz * sizeof(double);
   const int kstart = h->p.bc_variant == IW_BC_NOSLIP ? 1 : 0;
-  cudaFuncSetAttribute(k_press<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_visc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (h->use_bi) {
     launch_solve_bi<T>(h, fs, 3, cpen, kstart);
@@ -1681,7 +1676,6 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
 int iw_destroy(iw_handle* h) {
   if (!h) return IW_OK;
   cudaSetDevice(h->dev);
-  if (h->gexec) cudaGraphExecDestroy(h->gexec);
   free_fields(h->f64);
   free_fields(h->f32);
   for (double* p : {h->ddzinv, h->dpart, h->dDt, h->dD2t, h->dLt, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,

@@ -2,23 +2,27 @@
 // Legendre multidomain penalty z) and its C ABI (include/iw_b200.h).
 //
 // One step (main.f:653-1066) on device-resident fields:
-//   K_A  k_stageA      maxcalc/convec round-trip projection, w mean = 0,
+//   K_A  k_stageA(_r)  maxcalc/convec round-trip projection, w mean = 0,
 //                      z-derivatives of u,v,w,rho                   (z columns)
 //   K_B  k_yfft        y-inverse of u,v,w,rho, dz, and i ky (.)      (planes)
 //   K_C  k_xrow_nl     x-inverse of 16 rows -> skew-symmetric products,
 //                      buoyancy, upwind interface penalty, paddle ->
 //                      x-forward with i kx folded in                 (rows)
 //   K_D  k_yfft        y-forward with i ky folded in                 (planes)
-//   K_E  k_stageE      S = B + dz(Z), SS extrapolation, BDF u*, history,
+//   K_E  k_stageE(_r)  S = B + dz(Z), SS extrapolation, BDF u*, history,
 //                      Fourier x Legendre filter                     (z columns)
-//        k_wviscrot    rotational viscous pressure BC              (walls)
-//   K_F  k_press       pressure Poisson (band LU), filter, projection
-//   K_G  k_visc        u,v / w / rho Helmholtz solves, filters, mean mode
-//   K_H  interface averaging: planes next to interfaces go to physical space
-//        and back; every other plane gets the spectral effect of the round trip.
-// The band factors (penalty.f + band_lu.f) are assembled and factored on the
-// device (k_factor) when epsilon changes (steps 1-3 and a dt change), one per
-// distinct kx^2+ky^2 and system type.
+//        k_wviscrot    rotational viscous pressure BC                (walls)
+//   K_F  k_solve_cta   pressure Poisson (divergence, solve, filter, projection)
+//        k_solve_cta   u,v / w / rho Helmholtz solves, filters, mean mode
+//                      (block inverses; k_press_g / k_visc with the band LU
+//                      when the handle asks for the reference's LU)
+//   K_H  interface averaging: planes next to interfaces go to physical space,
+//        the averaging change comes back; every plane gets the spectral effect
+//        of the round trip.
+// The penalty systems (penalty.f + band_lu.f) are assembled on the device
+// (k_factor) when epsilon changes (steps 1-3 and a dt change), one per distinct
+// kx^2+ky^2 and system type, then factored (band LU) or turned into block
+// inverses of their distinct subdomain blocks.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1120,117 +1124,6 @@ struct SolveTabs {
   const int* col_order;  // columns sorted by kx^2+ky^2, so neighbouring warps share a factor
 };
 
-// K_F: pressure.  Warp per (ii,j) column.  Reads filtered u*,v*,w* (state F),
-// writes ub, vb, wb into the same arrays (calcuvwt.f:87-229 + update 826-901).
-template <typename T>
-__global__ void k_press(Geo g, SolveTabs tb, T* __restrict__ U, T* __restrict__ V, T* __restrict__ W,
-                        const double* __restrict__ wnl, const double* __restrict__ wvr, int cpen, int kstart) {
-  extern __shared__ __align__(16) double sm[];
-  const int warps = blockDim.x / 32;
-  const int wid = threadIdx.x / 32, lane = threadIdx.x & 31;
-  const int cw = blockIdx.x * warps + wid;
-  const int ncol = g.nxhp * g.ny;
-  if (cw >= ncol) return;
-  const int c = tb.col_order[cw];
-  const int n = g.nz, N = g.N;
-  double* buf = sm + (size_t)wid * 4 * n;  // [0,2n): w* re/im, [2n,4n): rhs/phi re/im
-  const int j = c / g.nxhp, ii = c % g.nxhp;
-  const double xw = g.xw[ii], yw = g.yw[j], dt = g.dt;
-  const int s = tb.col_sys[c];
-  for (int k = lane; k < n; k += 32) {
-    buf[k] = (double)W[fidx<T>(g, 2 * ii, j, k)];
-    buf[n + k] = (double)W[fidx<T>(g, 2 * ii + 1, j, k)];
-  }
-  __syncwarp();
-  double* rr = buf + 2 * n;
-  double* ri = buf + 3 * n;
-  if (s >= 0) {
-    const SysDesc sd = tb.sys[s];
-    const double eps = sd.eps;
-    // divcolc (derv.f:35-85) and rhs = div/dt, then rhs *= -eps
-    for (int k = lane; k < n; k += 32) {
-      int ks = k / N, k1 = k % N;
-      double sr = 0.0, si = 0.0;
-      for (int k2 = 0; k2 < N; ++k2) {
-        double dd = g.D[k1 * N + k2];
-        sr = radd(sr, rmul(dd, buf[ks * N + k2]));
-        si = radd(si, rmul(dd, buf[n + ks * N + k2]));
-      }
-      double fac = g.hfac[ks];
-      double dwr = rmul(sr, fac), dwi = rmul(si, fac);
-      double ur = (double)U[fidx<T>(g, 2 * ii, j, k)], ui = (double)U[fidx<T>(g, 2 * ii + 1, j, k)];
-      double vr = (double)V[fidx<T>(g, 2 * ii, j, k)], vi = (double)V[fidx<T>(g, 2 * ii + 1, j, k)];
-      double dr = radd(radd(0.0, -rmul(xw, ui)), -rmul(yw, vi));
-      double di = radd(radd(0.0, rmul(xw, ur)), rmul(yw, vr));
-      dr = radd(dr, dwr);
-      di = radd(di, dwi);
-      double r1 = __ddiv_rn(dr, dt), r2 = __ddiv_rn(di, dt);
-      rr[k] = -rmul(r1, eps);
-      ri[k] = -rmul(r2, eps);
-    }
-    __syncwarp();
-    if (lane == 0) {
-      size_t p1 = (size_t)g.nxpp * j + 2 * ii, p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii;
-      double bcrbot = radd(wnl[p1], wvr[p1]), bcibot = radd(wnl[p1 + 1], wvr[p1 + 1]);
-      double bcrtop = radd(wnl[p2], wvr[p2]), bcitop = radd(wnl[p2 + 1], wvr[p2 + 1]);
-      // Neumann rows (penalty.f:594-604)
-      rr[0] = rsub(rr[0], rmul(rmul(sd.tau1_bot, bcrbot), eps));
-      ri[0] = rsub(ri[0], rmul(rmul(sd.tau1_bot, bcibot), eps));
-      rr[n - 1] = radd(rr[n - 1], rmul(rmul(sd.tau2_top, bcrtop), eps));
-      ri[n - 1] = radd(ri[n - 1], rmul(rmul(sd.tau2_top, bcitop), eps));
-    }
-    __syncwarp();
-    const int ldab = 3 * N + 1;
-    band_solve_warp(tb.ab + (size_t)s * ldab * n, tb.ipiv + (size_t)s * n, rr, 2, n, N, N, lane);
-    if (cpen) {
-      legen_filter_cols(rr, 2, n, N, g.ns, tb.wg, tb.alpol, tb.sigma, lane);
-      __syncwarp();
-    }
-  } else {
-    for (int k = lane; k < n; k += 32) {
-      rr[k] = 0.0;
-      ri[k] = 0.0;
-    }
-    __syncwarp();
-  }
-  // projection (update): ub = u* - dt i kx phi, vb likewise, wb = w* - dt dphi/dz
-  const bool lzero = (ii == 0 && j == 0);
-  const double dtx = rmul(dt, xw), dty = rmul(dt, yw);
-  for (int k = lane; k < n; k += 32) {
-    size_t pr = fidx<T>(g, 2 * ii, j, k), pi = pr + 1;
-    if (k < kstart) {
-      U[pr] = 0;
-      U[pi] = 0;
-      V[pr] = 0;
-      V[pi] = 0;
-      W[pr] = 0;
-      W[pi] = 0;
-      continue;
-    }
-    double phr = rr[k], phi = ri[k];
-    double ur = (double)U[pr], ui = (double)U[pi], vr = (double)V[pr], vi = (double)V[pi];
-    U[pr] = (T)rsub(ur, rsub(rmul(0.0, phr), rmul(dtx, phi)));
-    U[pi] = (T)rsub(ui, radd(rmul(0.0, phi), rmul(dtx, phr)));
-    V[pr] = (T)rsub(vr, rsub(rmul(0.0, phr), rmul(dty, phi)));
-    V[pi] = (T)rsub(vi, radd(rmul(0.0, phi), rmul(dty, phr)));
-    if (lzero) {
-      W[pr] = 0;
-      W[pi] = 0;
-    } else {
-      int ks = k / N, k1 = k % N;
-      double sr = 0.0, si = 0.0;
-      for (int k2 = 0; k2 < N; ++k2) {
-        double dd = g.D[k1 * N + k2];
-        sr = radd(sr, rmul(dd, rr[ks * N + k2]));
-        si = radd(si, rmul(dd, ri[ks * N + k2]));
-      }
-      double fac = g.hfac[ks];
-      W[pr] = (T)rsub(buf[k], rmul(dt, rmul(sr, fac)));
-      W[pi] = (T)rsub(buf[n + k], rmul(dt, rmul(si, fac)));
-    }
-  }
-}
-
 // K_G: viscous/diffusive solves.  role 0: u and v (4 RHS, one factor),
 // role 1: w, role 2: rho.  Warp per column.
 template <typename T>
@@ -2061,21 +1954,6 @@ __global__ void k_compact_blocks(int N, int nsys, int ns, int nb, BlockRep rep, 
       for (int j = 0; j < N; ++j) acc += lr[j] * col[j];
       out[q] = acc;
     }
-  }
-}
-
-// out[blk][c][kk] = sum_j L[kk][j] in[blk][c][j]: the per-subdomain Legendre
-// filter folded into stored block inverses (L row major, N*N).
-__global__ void k_fold_filter(int N, size_t nblk, const double* __restrict__ L, const double* __restrict__ in,
-                              double* __restrict__ out) {
-  const size_t tot = nblk * N * N;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
-    const int kk = (int)(q % N);
-    const double* col = in + (q - kk);
-    const double* lr = L + (size_t)kk * N;
-    double acc = 0.0;
-    for (int j = 0; j < N; ++j) acc += lr[j] * col[j];
-    out[q] = acc;
   }
 }
 
