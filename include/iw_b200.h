@@ -101,7 +101,9 @@ typedef struct iw_params {
   int32_t forcing;       /* virtual paddle in rhsfm (solver.f:942)   */
   int32_t precision;     /* IW_PREC_*                                */
   int32_t solver;        /* IW_SOLVE_AUTO or IW_SOLVE_LU             */
-  int32_t pad_;
+  int32_t imaxcalc;      /* 1: adaptive dt from the CFL numbers of   */
+                         /* each step's start (main.f:47,657;        */
+                         /* various.f:892-982); 0: dt fixed          */
   /* subd.dat */
   double z0[IW_MAX_SUBD];
   double zh[IW_MAX_SUBD];
@@ -123,6 +125,7 @@ typedef struct iw_diag_out {
   double cflx, cfly, cflz;
   double wrms_bottom; /* rms of w over z < 0.2 zlen (noise growth)      */
   double t;
+  double dt;          /* current step (changes only with imaxcalc = 1)  */
   int32_t istep;
   int32_t interface_avg_count[4];
 } iw_diag_out;
@@ -310,6 +313,21 @@ double bdfvarv_(const double *dt1, const double *dt2, const double *dt3);
 double bdfvar1_(const double *dt1, const double *dt2, const double *dt3);
 double bdfvar2_(const double *dt1, const double *dt2, const double *dt3);
 double bdfvar3_(const double *dt1, const double *dt2, const double *dt3);
+
+/* various.f:892-982: the adaptive time-step rule maxcalc applies at the start
+ * of every step, as a pure host function (the handle API applies it itself
+ * when imaxcalc = 1).  In: the CFL numbers cflx, cflz of the fields at the
+ * start of the step, the time t, the current step dt and the wave frequency
+ * xomega (main.f:341-346).  Returns 1 and sets *dt_new = dt / cdt and *cdt when
+ * the step changes, else 0 and leaves both untouched.  The step changes when
+ * int(t / dt) > 20 and cflz > 0.7, cflz < 0.1 or cflx > 0.16; cdt = 1.25 if
+ * cflz > 0.7 or cflx > 0.16, else max(0.8, dt / Tlim) with
+ * Tlim = 2 pi / (50 xomega).  The step count is taken from t = 0: the
+ * reference's Tso (various.f:918,924) is a local without SAVE that is read
+ * before it is written, and its own recorded run (dtchange.dat) changes dt
+ * exactly when int(t / dt) > 20. */
+int iw_dt_rule(double cflx, double cflz, double t, double dt, double xomega,
+               double *dt_new, double *cdt);
 
 #ifdef __cplusplus
 }

@@ -27,7 +27,7 @@ EXPORTS = [
     "iw_device_bytes", "iw_helm_solve_batched", "iw_bind", "iw_profile", "iw_profile_read", "iw_mean_profiles",
     "horfft_", "dpdz_", "filter_3dlegenfourier_", "filter_legenpen_", "interface_avg3d_",
     "penalty_main_", "bandlu_solve_", "iw_bandlu_solve_noalloc", "penalty_setup_", "convec_", "calcuvwt_",
-    "abvar1_", "abvar2_", "abvar3_", "bdfvarv_", "bdfvar1_", "bdfvar2_", "bdfvar3_",
+    "abvar1_", "abvar2_", "abvar3_", "bdfvarv_", "bdfvar1_", "bdfvar2_", "bdfvar3_", "iw_dt_rule",
 ]
 
 
@@ -96,6 +96,8 @@ def lib():
     for n in ("abvar1_", "abvar2_", "abvar3_", "bdfvarv_", "bdfvar1_", "bdfvar2_", "bdfvar3_"):
         getattr(L, n).argtypes = [PD, PD, PD]
         getattr(L, n).restype = C.c_double
+    L.iw_dt_rule.argtypes = [C.c_double] * 5 + [PD, PD]
+    L.iw_dt_rule.restype = C.c_int
     _lib = L
     return L
 

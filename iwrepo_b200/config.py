@@ -51,7 +51,7 @@ class IwParams(C.Structure):
         ("ispecfilternl", C.c_int32), ("ispecfilterexp", C.c_int32),
         ("nspecfilterexp", C.c_int32), ("navgintrfc", C.c_int32),
         ("bc_variant", C.c_int32), ("meanu_damping", C.c_int32), ("forcing", C.c_int32),
-        ("precision", C.c_int32), ("solver", C.c_int32), ("pad_", C.c_int32),
+        ("precision", C.c_int32), ("solver", C.c_int32), ("imaxcalc", C.c_int32),
         ("z0", C.c_double * IW_MAX_SUBD), ("zh", C.c_double * IW_MAX_SUBD),
     ]
 
@@ -66,7 +66,7 @@ class IwDiagOut(C.Structure):
         ("umin", C.c_double), ("umax", C.c_double), ("vmin", C.c_double), ("vmax", C.c_double),
         ("wmin", C.c_double), ("wmax", C.c_double), ("tmin", C.c_double), ("tmax", C.c_double),
         ("cflx", C.c_double), ("cfly", C.c_double), ("cflz", C.c_double),
-        ("wrms_bottom", C.c_double), ("t", C.c_double),
+        ("wrms_bottom", C.c_double), ("t", C.c_double), ("dt", C.c_double),
         ("istep", C.c_int32), ("interface_avg_count", C.c_int32 * 4),
     ]
 
@@ -116,7 +116,7 @@ class Config:
     forcing: int = 0
     precision: int = IW_PREC_FP64
     solver: int = IW_SOLVE_AUTO
-    pad_: int = 0
+    imaxcalc: int = 0
     z0: Optional[List[float]] = None
     zh: Optional[List[float]] = None
     name: str = "custom"
@@ -179,6 +179,8 @@ class Config:
             raise ConfigError(f"bc_variant={self.bc_variant}")
         if self.precision not in (IW_PREC_FP64, IW_PREC_MIXED):
             raise ConfigError(f"precision={self.precision}")
+        if self.imaxcalc not in (0, 1):
+            raise ConfigError(f"imaxcalc={self.imaxcalc}")
         return self
 
     # -- C structs -----------------------------------------------------
@@ -247,7 +249,7 @@ def from_files(input_dat: str, subd_dat: str, nx: int, ny: int, nzloc: int, nsub
         facdir=f["facdir"], facneumn=f["facneumn"], facrobin=f["facrobin"],
         ispecfilternl=int(f["ispecfilternl"]), ispecfilterexp=int(f["ispecfilterexp"]),
         nspecfilterexp=int(f["nspecfilterexp"]), navgintrfc=int(f["navgintrfc"]),
-        forcing=1 if p.get("xacrit", 0.0) != 0.0 else 0,
+        forcing=1 if p.get("xacrit", 0.0) != 0.0 else 0, imaxcalc=1,
         z0=z0[:nsubd], zh=zh[:nsubd], name="files")
     cfg = cfg.replace(**overrides)
     return cfg.validate()
@@ -256,7 +258,9 @@ def from_files(input_dat: str, subd_dat: str, nx: int, ny: int, nzloc: int, nsub
 # ----------------------------------------------------------------------
 # Synthetic workloads (non-dimensional: Lx=Ly=2 pi, H=1, N=1, g=rho0=1,
 # nu = 1/Re, kappa = nu (Pr=1), no paddle, no-slip bottom / free-slip top,
-# filter order 8 amplitude 36 every step).
+# filter order 8 amplitude 36 every step, dt fixed: imaxcalc = 0, so that
+# every step does the same work; the reference hard-codes the adaptive step,
+# main.f:47, which from_files and shipped_2d keep).
 # ----------------------------------------------------------------------
 def baseline(name: str, **overrides) -> Config:
     name = name.upper()
@@ -308,5 +312,5 @@ def shipped_2d(nx: int = 256, nzloc: int = 25, nsubd: int = 12, **overrides) -> 
                  xbcrit=0.84, zcen=0.13, fwave=8.0, amp=35.0, p=5.0, pf=10.0, fackc=0.0,
                  facdir=1.0, facneumn=1.0, facrobin=1e4, ispecfilternl=1, ispecfilterexp=1,
                  nspecfilterexp=1, navgintrfc=1, bc_variant=IW_BC_FREESLIP, meanu_damping=1,
-                 forcing=1, z0=z0[:nsubd], zh=zh[:nsubd], name="shipped2d")
+                 forcing=1, imaxcalc=1, z0=z0[:nsubd], zh=zh[:nsubd], name="shipped2d")
     return cfg.replace(**overrides).validate()

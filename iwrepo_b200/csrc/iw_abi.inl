@@ -513,6 +513,7 @@ static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
   out->ke = 0.5 * red[0];
   out->eps = h->p.xnu * red[1];
   out->t = h->t;
+  out->dt = h->p.dt;
   out->istep = h->istep;
   int cnt[4] = {0, 0, 0, 0};
   CK(scopy(h, cnt, h->dcnt, sizeof cnt, cudaMemcpyDeviceToHost));
@@ -527,7 +528,48 @@ static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
   return IW_OK;
 }
 
+// CFL numbers of the state for the adaptive rule: maxcalc's cflxmax and
+// cflzmax (various.f:780-870), from the same per-block partials as iw_diag.
+template <typename T>
+static int step_cfl(iw_handle* h, FieldSet<T>& fs, double* cflx, double* cflz) {
+  Geo g = geo(h);
+  T* dst = fs.Y12[0];
+  T* tmp = fs.Y12[1];
+  const double dx = h->p.xlen / h->nx, rg = -(h->p.rho0 * h->p.brunt * h->p.brunt) / h->p.grav;
+  for (int q = 0; q <= 2; q += 2) {
+    phys_of<T>(h, fs, fs.F[q], dst, tmp, 0);
+    k_phys_stats<T><<<296, 256, 0, h->st>>>(g, dst, q, h->dzg, h->ddzinv, q == 0 ? h->p.dt / dx : 0.0, rg,
+                                            0.2 * h->p.zlen, h->dpart + (size_t)q * 296 * 5);
+  }
+  std::vector<double> part((size_t)3 * 296 * 5);
+  CK(cudaMemcpyAsync(part.data(), h->dpart, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  double cf[2] = {0, 0};
+  for (int b = 0; b < 296; ++b) {
+    cf[0] = std::max(cf[0], part[(size_t)b * 5 + 2]);
+    cf[1] = std::max(cf[1], part[((size_t)2 * 296 + b) * 5 + 2]);
+  }
+  *cflx = cf[0];
+  *cflz = cf[1];
+  return IW_OK;
+}
+
 extern "C" {
+
+// various.f:892-982; the step count is taken from t = 0 (see the header)
+int iw_dt_rule(double cflx, double cflz, double t, double dt, double xomega, double* dt_new, double* cdt) {
+  if (!(dt > 0) || !dt_new || !cdt) return 0;
+  const bool change_dt = cflz > 0.7 || cflz < 0.1 || cflx > 0.16;
+  const double pi2 = 8. * std::atan(1.0);
+  const double tlim = pi2 / (xomega * 50.);
+  if (!(std::trunc(t / dt) > 20.0) || !change_dt) return 0;
+  double c = 1.;
+  if (cflz < 0.1) c = std::max(0.8, dt / tlim);
+  if (cflz > 0.7 || cflx > 0.16) c = 1.25;
+  *cdt = c;
+  *dt_new = dt / c;
+  return 1;
+}
 
 int iw_diag(iw_handle* h, iw_diag_out* out) {
   if (!h || !out) return set_err(IW_ERR_STATE, "bad argument");

@@ -305,6 +305,11 @@ struct iw_handle {
   int nx, ny, nz, N, ns, nxpp, nxh, nxhp, nyh, ndims, ncol;
   size_t ntot, plane;
   bool mixed = false;
+  // adaptive time step (imaxcalc = 1): the wave frequency that bounds the step
+  // (Tlim) and the change in progress (COMMON /vardtflags/ ivardt, idtstep
+  // and cdt of comtime.h)
+  double xomega = 0, cdt = 1.0;
+  int ivardt = 0, idtstep = 0;
   Tables tab;
   // device tables
   double *ddzinv = 0, *dpart = 0;  // diagnostics: dt-free CFL spacing per level, per-block partials
@@ -1139,6 +1144,10 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
   return 0;
 }
 
+// main.f:741,832: the step after a change of dt (idtstep = 1) still has the
+// old step in its history
+static bool dt_adapting(const iw_handle* h) { return h->ivardt == 1 && h->idtstep < 2; }
+
 static void schedule_after_convec(iw_handle* h) {
   // coefficient schedule for the next step (main.f:700-777)
   if (h->istep < 2) {
@@ -1148,14 +1157,64 @@ static void schedule_after_convec(iw_handle* h) {
     h->c.bdf1 = 2.;
     h->c.bdf2 = -0.5;
     h->c.bdf3 = 0.;
-  } else {
+  } else if (!dt_adapting(h)) {
     h->c.fac1 = 3.;
     h->c.fac2 = -3.;
     h->c.fac3 = 1.;
     h->c.bdf1 = 3.;
     h->c.bdf2 = -1.5;
     h->c.bdf3 = 1. / 3.;
+  } else {  // main.f:760-775: two steps of the new dt, then one of the old
+    const double d1 = h->p.dt, d2 = h->p.dt, d3 = h->cdt * h->p.dt;
+    h->c.fac1 = abvar1_(&d1, &d2, &d3);
+    h->c.fac2 = abvar2_(&d1, &d2, &d3);
+    h->c.fac3 = abvar3_(&d1, &d2, &d3);
+    h->c.bdf1 = bdfvar1_(&d1, &d2, &d3);
+    h->c.bdf2 = bdfvar2_(&d1, &d2, &d3);
+    h->c.bdf3 = bdfvar3_(&d1, &d2, &d3);
   }
+}
+
+// bdfv for the next step's Helmholtz operators (main.f:815-855); ends a change
+// of dt in the step that made it (idtstep = 1 there)
+static void schedule_after_calcuvwt(iw_handle* h) {
+  if (h->istep < 2) {
+    h->c.bdfv = 1.5;
+  } else if (!dt_adapting(h)) {
+    h->c.bdfv = 11. / 6.;
+  } else {
+    const double d1 = h->p.dt, d2 = h->p.dt, d3 = h->cdt * h->p.dt;
+    h->c.bdfv = bdfvarv_(&d1, &d2, &d3);
+    h->cdt = 1.;
+    h->ivardt = 0;
+  }
+}
+
+template <typename T>
+static int step_cfl(iw_handle* h, FieldSet<T>& fs, double* cflx, double* cflz);
+
+// The adaptive rule of maxcalc (various.f:892-982) at the start of a step.
+// The CFL numbers (two inverse transforms, a reduction and a read-back) are
+// only needed once more than 20 steps of the current dt lie behind t; before
+// that the rule cannot change dt.  A change sets the step's variable-step
+// coefficients (the history holds one step of the new dt and two of the old)
+// and, through dt and bdfv, new Helmholtz operators.
+template <typename T>
+static int adapt_dt(iw_handle* h, FieldSet<T>& fs) {
+  if (!(std::trunc(h->t / h->p.dt) > 20.0)) return IW_OK;
+  double cflx = 0, cflz = 0;
+  int r = step_cfl<T>(h, fs, &cflx, &cflz);
+  if (r) return r;
+  double dtn = 0, cdt = 0;
+  if (!iw_dt_rule(cflx, cflz, h->t, h->p.dt, h->xomega, &dtn, &cdt)) return IW_OK;
+  h->p.dt = dtn;
+  h->cdt = cdt;
+  const double d1 = dtn, d2 = cdt * dtn, d3 = cdt * dtn;
+  h->c = Coefs{abvar1_(&d1, &d2, &d3),  abvar2_(&d1, &d2, &d3),  abvar3_(&d1, &d2, &d3),  bdfvar1_(&d1, &d2, &d3),
+               bdfvar2_(&d1, &d2, &d3), bdfvar3_(&d1, &d2, &d3), bdfvarv_(&d1, &d2, &d3), dtn};
+  h->ivardt = 1;
+  h->idtstep = 0;
+  return IW_OK;
 }
 
 template <typename T>
@@ -1294,13 +1353,16 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
 template <typename T>
 static int full_step(iw_handle* h, FieldSet<T>& fs) {
   h->istep += 1;
+  int r;
+  if (h->p.imaxcalc == 1 && (r = adapt_dt<T>(h, fs))) return r;
+  if (h->ivardt == 1) h->idtstep += 1;  // main.f:660-662
   const int cpen = (h->p.ispecfilterexp == 1) && (h->istep % h->p.nspecfilterexp == 0);
-  int r = ensure_factors(h, cpen);
+  r = ensure_factors(h, cpen);
   if (r) return r;
   convec_impl<T>(h, fs, 1);
   schedule_after_convec(h);
   calcuvwt_impl<T>(h, fs, cpen);
-  h->c.bdfv = (h->istep < 2) ? 1.5 : 11. / 6.;
+  schedule_after_calcuvwt(h);
   h->t = h->t + h->p.dt;
   if (h->p.navgintrfc > 0 && h->istep % h->p.navgintrfc == 0) {
     iface_avg<T>(h, fs, true);
@@ -1412,11 +1474,12 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
 // arrangement), launched alternately, therefore replay the step exactly.
 // Conditions that would make a step depend on its number keep the eager path:
 // paddle forcing (time in the arguments), a filter not applied every step,
-// interface averaging less often than every step, per-phase profiling.
+// interface averaging less often than every step, per-phase profiling, an
+// adaptive step (its rule reads the CFL numbers back at every step).
 // ---------------------------------------------------------------------------
 static bool graph_ready(const iw_handle* h) {
   return h->istep >= 3 && !h->prof && !h->p.forcing && (h->p.ispecfilterexp != 1 || h->p.nspecfilterexp == 1) &&
-         h->p.navgintrfc <= 1;
+         h->p.navgintrfc <= 1 && h->p.imaxcalc != 1;
 }
 
 static int step_dispatch(iw_handle* h) { return h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64); }
@@ -1669,6 +1732,10 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
     h->bmap[ks] = found;
   }
   h->c = Coefs{1., 0., 0., 1., 0., 0., 1., prm->dt};
+  {  // main.f:341-346 (bruntz = brunt)
+    const double pi2 = 8. * std::atan(1.0), kx = pi2 / prm->xlen, m = pi2 / (2. * prm->zlen);
+    h->xomega = (prm->brunt * kx) / std::sqrt(kx * kx + m * m);
+  }
   *out = h;
   return IW_OK;
 }
@@ -1754,6 +1821,9 @@ int iw_upload_state(iw_handle* h, const double* uvwt, const double* uvwt_n, cons
     }
   h->t = t;
   h->istep = istep_done;
+  h->cdt = 1.;
+  h->ivardt = 0;
+  h->idtstep = 0;
   if (istep_done == 0) {
     h->c = Coefs{1., 0., 0., 1., 0., 0., 1., h->p.dt};
   } else if (istep_done == 1) {

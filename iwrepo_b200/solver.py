@@ -121,7 +121,7 @@ class Solver:
     def diag(self) -> dict:
         d = IwDiagOut()
         _lib.check(_lib.lib().iw_diag(self.h, C.byref(d)))
-        return dict(ke=d.ke, eps=d.eps, t=d.t, istep=d.istep, avg=list(d.interface_avg_count),
+        return dict(ke=d.ke, eps=d.eps, t=d.t, dt=d.dt, istep=d.istep, avg=list(d.interface_avg_count),
                     wrms_bottom=d.wrms_bottom, cfl=(d.cflx, d.cfly, d.cflz),
                     minmax=(d.umin, d.umax, d.vmin, d.vmax, d.wmin, d.wmax, d.tmin, d.tmax))
 
@@ -240,6 +240,15 @@ def ensemble_run(members, n: int):
 def multistep(name: str, dt1: float, dt2: float, dt3: float) -> float:
     """multistep.f:7-89 through the C ABI (abvar1_ ... bdfvar3_)."""
     return getattr(_lib.lib(), name + "_")(_rd(dt1), _rd(dt2), _rd(dt3))
+
+
+def dt_rule(cflx: float, cflz: float, t: float, dt: float, xomega: float):
+    """maxcalc's adaptive time-step rule (various.f:892-982) through the C ABI
+    (iw_dt_rule): (new dt, cdt) when the step changes, else None."""
+    dn, c = C.c_double(0.0), C.c_double(0.0)
+    if _lib.lib().iw_dt_rule(cflx, cflz, t, dt, xomega, C.byref(dn), C.byref(c)):
+        return dn.value, c.value
+    return None
 
 
 def helm_solve_batched(solver: Solver, lam_dev_ptr: int, ncol: int, ifbcbot: int, ifbctop: int, rhs_dev_ptr: int,

@@ -68,6 +68,9 @@ def lib():
         L.orc_bandlu_solve.restype = C.c_int
         L.orc_band_factor.argtypes = [C.c_void_p, PD, PD, PI]
         L.orc_band_factor.restype = C.c_int
+        L.orc_get_dt.argtypes = [C.c_void_p, PD]
+        L.orc_dt_rule.argtypes = [D, D, D, D, D, PD, PD]
+        L.orc_dt_rule.restype = C.c_int
         for n in ("abvar1", "abvar2", "abvar3", "bdfvarv", "bdfvar1", "bdfvar2", "bdfvar3"):
             f = getattr(L, "orc_" + n)
             f.argtypes = [D, D, D]
@@ -123,6 +126,12 @@ class Oracle:
     def set_scalars(self, s):
         s = np.ascontiguousarray(s, dtype=np.float64)
         lib().orc_set_scalars(self.h, _p(s))
+
+    def dt_state(self) -> dict:
+        """Current dt and the adaptive step's state (cdt, ivardt, idtstep)."""
+        out = np.zeros(4)
+        lib().orc_get_dt(self.h, _p(out))
+        return dict(dt=out[0], cdt=out[1], ivardt=int(out[2]), idtstep=int(out[3]))
 
     def tables(self):
         c = self.cfg
@@ -210,6 +219,14 @@ class Oracle:
 
 def multistep(name: str, dt1: float, dt2: float, dt3: float) -> float:
     return getattr(lib(), "orc_" + name)(dt1, dt2, dt3)
+
+
+def dt_rule(cflx: float, cflz: float, t: float, dt: float, xomega: float):
+    """maxcalc's adaptive rule alone: (new dt, cdt) on a change, else None."""
+    dn, c = C.c_double(0.0), C.c_double(0.0)
+    if lib().orc_dt_rule(cflx, cflz, t, dt, xomega, C.byref(dn), C.byref(c)):
+        return dn.value, c.value
+    return None
 
 
 def set_threads(n: int):

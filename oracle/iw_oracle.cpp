@@ -115,6 +115,9 @@ struct Orc {
   double fac1 = 1, fac2 = 0, fac3 = 0, bdf1 = 1, bdf2 = 0, bdf3 = 0, bdfv = 1;
   double facvel, fact;
   int istep = 0;
+  // adaptive time step (COMMON /vardtflags/ ivardt, idtstep and cdt, comtime.h)
+  double cdt = 1.0;
+  int ivardt = 0, idtstep = 0;
   // penalty COMMON (comparampen.h) used by the single-call C API
   struct Pen* pen0 = nullptr;
   // filter tables
@@ -1396,12 +1399,65 @@ void maxcalc(Orc& o) {
   for (int q = 0; q < 4; ++q) horfft(o, o.F[q].data(), -1, o.nz);
 }
 
-// main.f:653-1066, one step with istart=0 and the adaptive step frozen.
+extern "C" double orc_abvar1(double, double, double);
+extern "C" double orc_abvar2(double, double, double);
+extern "C" double orc_abvar3(double, double, double);
+extern "C" double orc_bdfvarv(double, double, double);
+extern "C" double orc_bdfvar1(double, double, double);
+extern "C" double orc_bdfvar2(double, double, double);
+extern "C" double orc_bdfvar3(double, double, double);
+
+// various.f:892-937: the adaptive rule of maxcalc.  Tso (various.f:918,924) is
+// a local of maxcalc without SAVE that is read before any store to it, and
+// the store does not outlive the call; the reference's recorded run
+// (dtchange.dat: 2.1 0.125, 2.725 0.15625, ... from dtin = 0.1) changes dt
+// exactly when the count from Tso = 0 exceeds 20, which is what is kept here.
+bool dt_rule(double cflxmax, double cflzmax, double t, double& dt, double xomega, double& cdt) {
+  const double cflxmax_lim = 0.16, cflzmax_lim = 0.7, cflzmin_lim = 0.1;
+  const bool change_dt = (cflzmax > cflzmax_lim) || (cflzmax < cflzmin_lim) || (cflxmax > cflxmax_lim);
+  const double pi2 = 8.0 * std::atan(1.0);
+  const double Tlim = pi2 / (xomega * 50.);
+  const double Tso = 0.0;
+  const double q = (t - Tso) / dt;  // Nst = INT(q): truncation toward zero
+  const long long Nst = q >= 9.0e18 ? 9000000000000000000LL : q <= -9.0e18 ? -1LL : (long long)q;
+  if (Nst > 20 && change_dt) {
+    if (cflzmax < cflzmin_lim) cdt = std::max(0.8, dt / Tlim);
+    if ((cflzmax > cflzmax_lim) || (cflxmax > cflxmax_lim)) cdt = 1.25;
+    dt = dt / cdt;
+    return true;
+  }
+  return false;
+}
+
+// various.f:938-970: new dt, the coefficients of the step that follows (one
+// step of the new dt and two of the old in the history), facvel and fact
+void adapt_dt(Orc& o) {
+  const Wave wv = wave_params(o);
+  if (!dt_rule(o.cfl[0], o.cfl[2], o.t, o.dt, wv.xomega, o.cdt)) return;
+  const double dt1 = o.dt, dt2 = o.cdt * o.dt, dt3 = o.cdt * o.dt;
+  o.fac1 = orc_abvar1(dt1, dt2, dt3);
+  o.fac2 = orc_abvar2(dt1, dt2, dt3);
+  o.fac3 = orc_abvar3(dt1, dt2, dt3);
+  o.bdf1 = orc_bdfvar1(dt1, dt2, dt3);
+  o.bdf2 = orc_bdfvar2(dt1, dt2, dt3);
+  o.bdf3 = orc_bdfvar3(dt1, dt2, dt3);
+  o.bdfv = orc_bdfvarv(dt1, dt2, dt3);
+  o.fact = 1. / (o.pp.xkappa * o.dt);
+  o.facvel = 1. / (o.pp.xnu * o.dt);
+  o.ivardt = 1;
+  o.idtstep = 0;
+}
+
+// main.f:653-1066, one step with istart=0; maxcalc's adaptive step when
+// imaxcalc = 1 (the reference hard-codes 1, main.f:47), dt fixed otherwise.
 void step(Orc& o) {
   o.istep += 1;
   int istep = o.istep;
   maxcalc(o);
+  if (o.pp.imaxcalc == 1) adapt_dt(o);
+  if (o.ivardt == 1) o.idtstep = o.idtstep + 1;  // main.f:660-662
   convec(o);
+  bool ldtadapt = (o.ivardt == 1) && (o.idtstep < 2);  // main.f:741
   if (istep < 2) {
     o.fac1 = 2.;
     o.fac2 = -1.;
@@ -1409,18 +1465,36 @@ void step(Orc& o) {
     o.bdf1 = 2.;
     o.bdf2 = -0.5;
     o.bdf3 = 0.;
-  } else {
+  } else if (!ldtadapt) {
     o.fac1 = 3.;
     o.fac2 = -3.;
     o.fac3 = 1.;
     o.bdf1 = 3.;
     o.bdf2 = -1.5;
     o.bdf3 = 1. / 3.;
+  } else {  // main.f:760-775
+    const double dt1 = o.dt, dt2 = o.dt, dt3 = o.cdt * o.dt;
+    o.fac1 = orc_abvar1(dt1, dt2, dt3);
+    o.fac2 = orc_abvar2(dt1, dt2, dt3);
+    o.fac3 = orc_abvar3(dt1, dt2, dt3);
+    o.bdf1 = orc_bdfvar1(dt1, dt2, dt3);
+    o.bdf2 = orc_bdfvar2(dt1, dt2, dt3);
+    o.bdf3 = orc_bdfvar3(dt1, dt2, dt3);
   }
   for (int q = 0; q < 4; ++q) o.S[q] = o.F[q];
   bool cpen = (o.pp.ispecfilterexp == 1) && (istep % o.pp.nspecfilterexp == 0);
   calcuvwt(o, cpen);
-  o.bdfv = (istep < 2) ? 1.5 : 11. / 6.;
+  ldtadapt = (o.ivardt == 1) && (o.idtstep < 2);  // main.f:832
+  if (istep < 2) {
+    o.bdfv = 1.5;
+  } else if (!ldtadapt) {
+    o.bdfv = 11. / 6.;
+  } else {  // main.f:846-852
+    const double dt1 = o.dt, dt2 = o.dt, dt3 = o.cdt * o.dt;
+    o.bdfv = orc_bdfvarv(dt1, dt2, dt3);
+    o.cdt = 1.;
+    o.ivardt = 0;
+  }
   o.t = o.t + o.dt;
   if (o.pp.navgintrfc > 0 && istep % o.pp.navgintrfc == 0)
     for (int q = 0; q < 4; ++q) o.avg_count[q] = interface_avg3d(o, o.F[q].data());
@@ -1465,6 +1539,9 @@ void init_mode1(Orc& o, double A, double anoise, uint64_t seed) {
   for (int q = 0; q < 4; ++q) horfft(o, o.F[q].data(), -1, o.nz);
   o.t = 0.0;
   o.istep = 0;
+  o.cdt = 1.;
+  o.ivardt = 0;
+  o.idtstep = 0;
   o.fac1 = 1.;
   o.fac2 = o.fac3 = 0.;
   o.bdf1 = 1.;
@@ -1641,9 +1718,27 @@ void orc_set_scalars(void* h, const double* in) {
   o->bdf2 = in[6];
   o->bdf3 = in[7];
   o->bdfv = in[8];
+  o->cdt = 1.;
+  o->ivardt = 0;
+  o->idtstep = 0;
 }
 
 void orc_init_mode1(void* h, double A, double anoise, uint64_t seed) { init_mode1(*(Orc*)h, A, anoise, seed); }
+
+// current dt and the adaptive state: dt, cdt, ivardt, idtstep
+void orc_get_dt(void* h, double* out4) {
+  Orc* o = (Orc*)h;
+  double v[4] = {o->dt, o->cdt, (double)o->ivardt, (double)o->idtstep};
+  std::memcpy(out4, v, sizeof v);
+}
+// the rule alone (dt_rule): returns 1 and the new dt and cdt on a change
+int orc_dt_rule(double cflx, double cflz, double t, double dt, double xomega, double* dt_new, double* cdt) {
+  double d = dt, c = 1.;
+  if (!dt_rule(cflx, cflz, t, d, xomega, c)) return 0;
+  *dt_new = d;
+  *cdt = c;
+  return 1;
+}
 
 void orc_step(void* h) { step(*(Orc*)h); }
 void orc_run(void* h, int n) {

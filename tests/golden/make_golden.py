@@ -14,6 +14,11 @@ under tests/golden/.  The GPU box never reads the reference tree.
                      shipped 2-D forced run (various.f:743-745)
 * minmaxtest.dat, cfl.dat, avgint.dat -- per-step traces of the same run
 * runfolder/subd.dat, subd.dat -- subdomain tables used above
+* output, dtchange.dat -- the log of a recorded 400-step run (xlen = 40) and
+                     its record of time-step changes (write(65,*) t, dt,
+                     various.f:971): the run's parameters and wave frequency
+                     (main.f:370), maxcalc's cflzmax at the start of every
+                     step (various.f:882) and the (t, dt) of every change
 """
 import json
 import os
@@ -46,6 +51,21 @@ def main(ref):
     g["avgint"] = rows(os.path.join(ref, "avgint.dat"), 1)
     g["subd_runfolder"] = rows(os.path.join(ref, "runfolder", "subd.dat"))
     g["subd_shipped"] = rows(os.path.join(ref, "subd.dat"))
+    log = open(os.path.join(ref, "output"), "rb").read().decode("latin1").splitlines()
+
+    def logged(name):
+        for line in log:
+            key, _, val = line.partition("=")
+            if key.strip() == name:
+                return float(val.strip().rstrip(",").replace("D", "E"))
+        raise KeyError(name)
+
+    g["dt_run"] = {
+        "dtin": logged("DTIN"), "xlen": logged("XLEN"), "zlen": logged("ZLEN"), "brunt": logged("BRUNT"),
+        "omega": [float(l.split()[-1]) for l in log if "Wave Frequency omega" in l][0],
+        "cflz": [float(l.split()[-1]) for l in log if "At max CFLZ dz=" in l],
+        "changes": rows(os.path.join(ref, "dtchange.dat")),
+    }
     g["_source"] = "jmsegret/IWrepo mode1_bbl run artefacts; see make_golden.py"
     with open(os.path.join(here, "reference_runs.json"), "w") as f:
         json.dump(g, f, indent=0)

@@ -49,3 +49,22 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(L, "_lib", None)
     with pytest.raises(L.IwError):
         L.lib()
+
+
+def test_dt_rule_entry_point_host_only(golden):
+    """iw_dt_rule (maxcalc's adaptive rule, pure host code) replays the
+    recorded run's 18 changes and agrees bit for bit with the oracle's rule
+    on every branch."""
+    import itertools
+    import iwrepo_b200 as iw
+    import oracle
+    from test_oracle_pins import replay_dt_run, wave_omega
+    run = golden["dt_run"]
+    got = replay_dt_run(iw.dt_rule, run)
+    assert len(got) == len(run["changes"])
+    for (t, dt), (rt, rdt) in zip(got, run["changes"]):
+        assert abs(t - rt) <= 1e-13 * rt and abs(dt - rdt) <= 1e-14 * rdt
+    om = wave_omega(2 * 3.141592653589793, 1.0, 1.0)
+    for cx, cz, t, dt in itertools.product((0.0, 0.1, 0.16, 0.17), (0.0, 0.05, 0.1, 0.5, 0.7, 0.71, float("nan")),
+                                           (0.0, 2.0, 2.1, 2.2, 50.0), (0.1, 0.3, 0.4, 1.0)):
+        assert iw.dt_rule(cx, cz, t, dt, om) == oracle.dt_rule(cx, cz, t, dt, om)

@@ -1,0 +1,104 @@
+"""Adaptive time step (imaxcalc = 1; maxcalc's rule, various.f:892-982, and the
+variable-step coefficient schedule of main.f:655-860) on the GPU against the
+oracle.
+
+* The rule reads the CFL numbers of each step's start from the device; every
+  step's dt must equal the oracle's bit for bit.
+* FP64: <= 1e-10 relative L2 per field at the end, as for fixed steps.
+* Mixed precision: the same dt sequence; <= 1e-5 relative L2 against the FP64
+  GPU path (u, w, rho and the velocity vector).
+* Cases: "increase" (cflz < 0.1: dt grows by 5/4 at steps 22, 27, 32, 36) and
+  "decrease" (cflx > 0.16: dt shrinks by 5/4 at steps 22 and 23, the second
+  change starting right after the first has ended).
+"""
+import numpy as np
+import pytest
+
+from iwrepo_b200 import config as cf
+
+pytestmark = pytest.mark.gpu
+
+CASES = {"increase": (0.02, 0.05, 40), "decrease": (0.14, 0.1, 30)}
+
+
+def rel(a, b):
+    n = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+def _cfg(case, precision=cf.IW_PREC_FP64):
+    dt, _, _ = CASES[case]
+    return cf.Config(nx=32, ny=32, nzloc=9, nsubd=3, dt=dt, imaxcalc=1, precision=precision).validate()
+
+
+def _run_gpu(cfg, amp, nsteps):
+    import iwrepo_b200 as iw
+    s = iw.Solver(cfg)
+    s.init_mode1(amp, 1e-4, 11)
+    dts = []
+    for _ in range(nsteps):
+        s.step(1)
+        dts.append(s.diag()["dt"])
+    return s, dts
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_adaptive_dt_fp64_matches_oracle(case):
+    from oracle import Oracle
+    _, amp, nsteps = CASES[case]
+    cfg = _cfg(case)
+    o = Oracle(cfg)
+    o.init_mode1(amp, 1e-4, 11)
+    odts = []
+    for _ in range(nsteps):
+        o.step(1)
+        odts.append(o.dt_state()["dt"])
+    s, dts = _run_gpu(cfg, amp, nsteps)
+    assert dts == odts
+    assert len(set(dts)) >= 3  # at least two changes happened
+    d = s.diag()
+    assert abs(d["t"] - o.scalars()[0]) <= 1e-15 * d["t"] and d["istep"] == nsteps
+    a, b = s.state(), o.state()
+    for q in range(4):
+        assert rel(a[q], b[q]) <= 1e-10, q
+    s.close()
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_adaptive_dt_mixed_matches_fp64(case):
+    _, amp, nsteps = CASES[case]
+    s64, d64 = _run_gpu(_cfg(case), amp, nsteps)
+    s32, d32 = _run_gpu(_cfg(case, cf.IW_PREC_MIXED), amp, nsteps)
+    assert d32 == d64
+    a, b = s32.state(), s64.state()
+    for q in (0, 2, 3):
+        assert rel(a[q], b[q]) <= 1e-5, q
+    assert rel(a[:3], b[:3]) <= 1e-5
+    s32.close()
+    s64.close()
+
+
+def test_adaptive_dt_run_and_ensemble_equal_steps():
+    """iw_run with graphs requested and iw_ensemble_run step an adaptive
+    handle eagerly (its rule reads the CFL numbers back every step): the
+    results equal plain steps bit for bit, also next to a fixed-step member."""
+    import iwrepo_b200 as iw
+    _, amp, nsteps = CASES["decrease"]
+    ref, _ = _run_gpu(_cfg("decrease"), amp, nsteps)
+    a = iw.Solver(_cfg("decrease"))
+    a.init_mode1(amp, 1e-4, 11)
+    a.run(nsteps, graph=True)
+    fixed_cfg = cf.Config(nx=32, ny=32, nzloc=9, nsubd=3, dt=1e-3).validate()
+    e, f, f_alone = iw.Solver(_cfg("decrease")), iw.Solver(fixed_cfg), iw.Solver(fixed_cfg)
+    e.init_mode1(amp, 1e-4, 11)
+    for x in (f, f_alone):
+        x.init_mode1(0.05, 1e-4, 5)
+    iw.ensemble_run([e, f], nsteps)
+    f_alone.step(nsteps)
+    for lev in range(5):
+        assert np.array_equal(a.state(lev), ref.state(lev))
+        assert np.array_equal(e.state(lev), ref.state(lev))
+        assert np.array_equal(f.state(lev), f_alone.state(lev))
+    assert a.diag()["dt"] == e.diag()["dt"] == ref.diag()["dt"] < CASES["decrease"][0]
+    for x in (a, e, f, f_alone, ref):
+        x.close()

@@ -186,3 +186,93 @@ def test_factor_cache_is_bit_identical():
         o.step(4)
         st.append(o.state())
     assert np.array_equal(st[0], st[1])
+
+
+# ---------------------------------------------------------------------------
+# Adaptive time step (maxcalc, various.f:892-982)
+# ---------------------------------------------------------------------------
+def wave_omega(xlen, zlen, brunt):
+    """main.f:341-346 (bruntz = brunt)."""
+    pi2 = 8.0 * math.atan(1.0)
+    kx, m = pi2 / xlen, pi2 / (2.0 * zlen)
+    return brunt * kx / math.sqrt(kx * kx + m * m)
+
+
+def replay_dt_run(rule, run):
+    """Drive a dt rule with the recorded run's cflzmax at the start of every
+    step (cflx was not logged: 0) and return the (t, dt) of every change."""
+    om = wave_omega(run["xlen"], run["zlen"], run["brunt"])
+    t, dt, out = 0.0, run["dtin"], []
+    for cz in run["cflz"]:
+        r = rule(0.0, cz, t, dt, om)
+        if r is not None:
+            dt = r[0]
+            out.append((t, dt))
+        t = t + dt
+    return out
+
+
+def test_wave_frequency_matches_recorded_run(golden):
+    run = golden["dt_run"]
+    assert abs(wave_omega(run["xlen"], run["zlen"], run["brunt"]) - run["omega"]) <= 1e-14 * run["omega"]
+
+
+def test_oracle_dt_rule_replays_recorded_run(golden):
+    """All 18 changes of the recorded 400-step run (14 increases while
+    cflz < 0.1, then 4 decreases by 5/4 when cflz > 0.7), at the same t, with
+    the same dt, and no others."""
+    import oracle
+    run = golden["dt_run"]
+    got = replay_dt_run(oracle.dt_rule, run)
+    assert len(got) == len(run["changes"]) == 18
+    for (t, dt), (rt, rdt) in zip(got, run["changes"]):
+        assert abs(t - rt) <= 1e-13 * rt
+        assert abs(dt - rdt) <= 1e-14 * rdt
+
+
+def test_oracle_dt_rule_branches():
+    import oracle
+    om = wave_omega(2 * math.pi, 1.0, 1.0)
+    tlim = 8.0 * math.atan(1.0) / (om * 50.0)
+    assert oracle.dt_rule(0.0, 0.05, 20.0, 1.0, om) is None  # int(t/dt) = 20
+    assert oracle.dt_rule(0.0, 0.5, 30.0, 1.0, om) is None  # CFL inside the window
+    assert oracle.dt_rule(0.0, 0.05, 2.1, 0.1, om) == (0.1 / 0.8, 0.8)
+    assert oracle.dt_rule(0.2, 0.05, 2.1, 0.1, om) == (0.1 / 1.25, 1.25)  # cflx wins over cflz < 0.1
+    assert oracle.dt_rule(0.0, 0.8, 2.1, 0.1, om) == (0.1 / 1.25, 1.25)
+    dn, c = oracle.dt_rule(0.0, 0.05, 30.0 * tlim, 0.9 * tlim, om)  # capped at Tlim
+    assert c == 0.9 * tlim / tlim and dn == 0.9 * tlim / c
+    assert oracle.dt_rule(0.0, float("nan"), 30.0, 1.0, om) is None
+
+
+def test_oracle_adaptive_schedule():
+    """imaxcalc = 1: dt changes exactly where the rule says from the CFL
+    numbers of each step's start.  The change step itself has idtstep = 1, so
+    it already sets the next step's variable-step coefficients of
+    (dt, dt, cdt dt) and ends the change (ivardt = 0, cdt = 1; main.f:760-775,
+    846-852); the step after that sets SS3/BDF3 again."""
+    import oracle
+    cfg = cf.Config(nx=16, ny=16, nzloc=9, nsubd=3, dt=2e-3, imaxcalc=1).validate()
+    o = Oracle(cfg)
+    o.init_mode1(0.05, 1e-4, 7)
+    om = wave_omega(cfg.xlen, cfg.zlen, cfg.brunt)
+    changes = []
+    for _ in range(34):
+        t0, dt0 = o.scalars()[0], o.dt_state()["dt"]
+        o.step(1)
+        lm = o.last_maxcalc()
+        r = oracle.dt_rule(lm["cfl"][0], lm["cfl"][2], t0, dt0, om)
+        st = o.dt_state()
+        s = o.scalars()
+        if r is None:
+            assert st["dt"] == dt0
+        else:
+            changes.append(o.scalars()[1])
+            dt, cdt = r
+            assert st["dt"] == dt and st["ivardt"] == 0 and st["idtstep"] == 1 and st["cdt"] == 1.0
+            for k, name in enumerate(("abvar1", "abvar2", "abvar3", "bdfvar1", "bdfvar2", "bdfvar3", "bdfvarv")):
+                assert s[2 + k] == multistep(name, dt, dt, cdt * dt)
+            o.step(1)
+            st, s = o.dt_state(), o.scalars()
+            assert st["ivardt"] == 0 and st["dt"] == dt
+            assert list(s[2:9]) == [3.0, -3.0, 1.0, 3.0, -1.5, 1.0 / 3.0, 11.0 / 6.0]
+    assert len(changes) >= 2 and changes[0] in (22, 23)
