@@ -51,6 +51,11 @@ extern "C" {
 #define IW_ERR_STATE 5     /* call out of order (no handle bound, ...)    */
 #define IW_ERR_NOMEM 6     /* device allocation failed                    */
 #define IW_ERR_TIMEOUT 7   /* a bounded device wait gave up               */
+#define IW_ERR_IO 8        /* a file could not be opened, read or written */
+
+/* iw_read_restart modes */
+#define IW_RESTART_EXACT 0     /* continue exactly where the writer stopped */
+#define IW_RESTART_REFERENCE 1 /* main.f istart = 1 semantics               */
 
 /* boundary-condition variants of calcuvwt (reference files in brackets) */
 #define IW_BC_FREESLIP 0 /* calcuvwt.f / calcuvwt_freeslip.f: u,v Neumann at both ends */
@@ -153,6 +158,31 @@ int iw_upload_state(iw_handle *h, const double *uvwt, const double *uvwt_n,
                     const double *s_nm, double t, int istep_done);
 int iw_download_state(iw_handle *h, double *uvwt, double *uvwt_n,
                       double *uvwt_nm, double *s_n, double *s_nm);
+
+/* Replaces output.f:2-117 (subroutine output, the restart dump of
+ * main.f:974,988-989): writes the 49 records of output.f in its order and
+ * sizes, as ifort unformatted sequential (4-byte little-endian byte counts
+ * around each record; REAL*8 and INTEGER*4 items), so that restart.f reads
+ * the file.  Records 30-49 hold the state levels n, n-1, n-2 and the NL terms
+ * at n-1, n-2; the setup tables that the reference recomputes after a read
+ * hold this library's tables or 0.  One more record follows, which restart.f
+ * does not read: the step counter, the adaptive-step and restart state and
+ * the multistep coefficients.  Records over 2147483639 bytes are refused. */
+int iw_write_restart(iw_handle *h, const char *path);
+/* Replaces restart.f:2-126 and main.f:555-632 (istart = 1 or 2).  Checks every
+ * record's framing and size against the handle's dims before it changes
+ * anything (the reference only warns on a dims mismatch: IW_ERR_CONFIG here).
+ * mode IW_RESTART_REFERENCE: the reference's semantics -- t from the file,
+ * the step counter from 0, and the first step's coefficients for a step dt
+ * after two of cdtin*dt (main.f:613-632, 716-730, 820-826); dt is the
+ * handle's.  Works on files the reference wrote.
+ * mode IW_RESTART_EXACT: also restores the step counter, dt, the multistep
+ * coefficients and the adaptive-step state from this library's extra
+ * record, so the run continues bit for bit; IW_ERR_CONFIG if it is absent.
+ * The handle's parameters stand: the reference also takes pr, ra and umax
+ * from the file, which equal the namelist values when a run continues with
+ * its own input.dat. */
+int iw_read_restart(iw_handle *h, const char *path, int mode, double cdtin);
 
 /* Mode-1 internal wave initial condition plus seeded uniform noise in the
  * bottom 20% of the depth, transformed to spectral space (a new init: the

@@ -310,6 +310,9 @@ struct iw_handle {
   // and cdt of comtime.h)
   double xomega = 0, cdt = 1.0;
   int ivardt = 0, idtstep = 0;
+  // 1 after iw_read_restart in the reference's mode (main.f istart = 1): the
+  // first step's schedule uses variable-step coefficients with ratio cdt
+  int istart = 0;
   Tables tab;
   // device tables
   double *ddzinv = 0, *dpart = 0;  // diagnostics: dt-free CFL spacing per level, per-block partials
@@ -1148,15 +1151,36 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
 // old step in its history
 static bool dt_adapting(const iw_handle* h) { return h->ivardt == 1 && h->idtstep < 2; }
 
+static void set_var_fac_bdf(iw_handle* h) {  // two steps of dt, then one of cdt*dt
+  const double d1 = h->p.dt, d2 = h->p.dt, d3 = h->cdt * h->p.dt;
+  h->c.fac1 = abvar1_(&d1, &d2, &d3);
+  h->c.fac2 = abvar2_(&d1, &d2, &d3);
+  h->c.fac3 = abvar3_(&d1, &d2, &d3);
+  h->c.bdf1 = bdfvar1_(&d1, &d2, &d3);
+  h->c.bdf2 = bdfvar2_(&d1, &d2, &d3);
+  h->c.bdf3 = bdfvar3_(&d1, &d2, &d3);
+}
+
+static void set_var_bdfv(iw_handle* h) {
+  const double d1 = h->p.dt, d2 = h->p.dt, d3 = h->cdt * h->p.dt;
+  h->c.bdfv = bdfvarv_(&d1, &d2, &d3);
+}
+
+// coefficient schedule for the next step (main.f:700-777): SS2/BDF2 after the
+// first step of a new run, the variable-step form after the first step of a
+// restarted one (istart = 1) and after a change of dt, SS3/BDF3 otherwise
 static void schedule_after_convec(iw_handle* h) {
-  // coefficient schedule for the next step (main.f:700-777)
   if (h->istep < 2) {
-    h->c.fac1 = 2.;
-    h->c.fac2 = -1.;
-    h->c.fac3 = 0.;
-    h->c.bdf1 = 2.;
-    h->c.bdf2 = -0.5;
-    h->c.bdf3 = 0.;
+    if (h->istart == 0) {
+      h->c.fac1 = 2.;
+      h->c.fac2 = -1.;
+      h->c.fac3 = 0.;
+      h->c.bdf1 = 2.;
+      h->c.bdf2 = -0.5;
+      h->c.bdf3 = 0.;
+    } else {
+      set_var_fac_bdf(h);
+    }
   } else if (!dt_adapting(h)) {
     h->c.fac1 = 3.;
     h->c.fac2 = -3.;
@@ -1164,27 +1188,24 @@ static void schedule_after_convec(iw_handle* h) {
     h->c.bdf1 = 3.;
     h->c.bdf2 = -1.5;
     h->c.bdf3 = 1. / 3.;
-  } else {  // main.f:760-775: two steps of the new dt, then one of the old
-    const double d1 = h->p.dt, d2 = h->p.dt, d3 = h->cdt * h->p.dt;
-    h->c.fac1 = abvar1_(&d1, &d2, &d3);
-    h->c.fac2 = abvar2_(&d1, &d2, &d3);
-    h->c.fac3 = abvar3_(&d1, &d2, &d3);
-    h->c.bdf1 = bdfvar1_(&d1, &d2, &d3);
-    h->c.bdf2 = bdfvar2_(&d1, &d2, &d3);
-    h->c.bdf3 = bdfvar3_(&d1, &d2, &d3);
+  } else {
+    set_var_fac_bdf(h);
   }
 }
 
-// bdfv for the next step's Helmholtz operators (main.f:815-855); ends a change
-// of dt in the step that made it (idtstep = 1 there)
+// bdfv for the next step's Helmholtz operators (main.f:815-855).  A change of
+// dt ends in the step that made it (idtstep = 1 there): cdt = 1, ivardt = 0.
+// The first step of a restarted run leaves both as they are.
 static void schedule_after_calcuvwt(iw_handle* h) {
   if (h->istep < 2) {
-    h->c.bdfv = 1.5;
+    if (h->istart == 0)
+      h->c.bdfv = 1.5;
+    else
+      set_var_bdfv(h);
   } else if (!dt_adapting(h)) {
     h->c.bdfv = 11. / 6.;
   } else {
-    const double d1 = h->p.dt, d2 = h->p.dt, d3 = h->cdt * h->p.dt;
-    h->c.bdfv = bdfvarv_(&d1, &d2, &d3);
+    set_var_bdfv(h);
     h->cdt = 1.;
     h->ivardt = 0;
   }
@@ -1824,6 +1845,7 @@ int iw_upload_state(iw_handle* h, const double* uvwt, const double* uvwt_n, cons
   h->cdt = 1.;
   h->ivardt = 0;
   h->idtstep = 0;
+  h->istart = 0;
   if (istep_done == 0) {
     h->c = Coefs{1., 0., 0., 1., 0., 0., 1., h->p.dt};
   } else if (istep_done == 1) {
@@ -2197,3 +2219,4 @@ static int helm_batched(iw_handle* h, const double* lam_dev, int ncol, int bot, 
 }
 
 #include "iw_abi.inl"
+#include "iw_restart.inl"

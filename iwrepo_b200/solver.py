@@ -98,6 +98,18 @@ class Solver:
     def step(self, n: int = 1):
         _lib.check(_lib.lib().iw_run(self.h, n, 0))
 
+    def write_restart(self, path: str):
+        """output.f's restart dump through iw_write_restart (the reference's 49
+        records plus the continuation record)."""
+        _lib.check(_lib.lib().iw_write_restart(self.h, str(path).encode()))
+
+    def read_restart(self, path: str, mode: str = "reference", cdtin: float = 1.0):
+        """restart.f through iw_read_restart: mode "reference" gives main.f's
+        istart = 1 start (cdtin = old dt / new dt), "exact" continues a run
+        written by write_restart bit for bit."""
+        m = {"exact": 0, "reference": 1}[mode]
+        _lib.check(_lib.lib().iw_read_restart(self.h, str(path).encode(), m, cdtin))
+
     def autotune(self) -> dict:
         """Time this step's launch candidates and keep the fastest (y-tile
         width, stage A / stage E variant); the state is not changed."""

@@ -69,6 +69,10 @@ def lib():
         L.orc_band_factor.argtypes = [C.c_void_p, PD, PD, PI]
         L.orc_band_factor.restype = C.c_int
         L.orc_get_dt.argtypes = [C.c_void_p, PD]
+        L.orc_write_restart.argtypes = [C.c_void_p, C.c_char_p]
+        L.orc_write_restart.restype = C.c_int
+        L.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, D]
+        L.orc_read_restart.restype = C.c_int
         L.orc_dt_rule.argtypes = [D, D, D, D, D, PD, PD]
         L.orc_dt_rule.restype = C.c_int
         for n in ("abvar1", "abvar2", "abvar3", "bdfvarv", "bdfvar1", "bdfvar2", "bdfvar3"):
@@ -126,6 +130,17 @@ class Oracle:
     def set_scalars(self, s):
         s = np.ascontiguousarray(s, dtype=np.float64)
         lib().orc_set_scalars(self.h, _p(s))
+
+    def write_restart(self, path: str):
+        """output.f's restart dump (see orc_write_restart)."""
+        if lib().orc_write_restart(self.h, str(path).encode()):
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def read_restart(self, path: str, mode: str = "reference", cdtin: float = 1.0):
+        """restart.f + main.f:555-632 ("reference": istart = 1 semantics;
+        "exact": continue from the file's continuation record)."""
+        if lib().orc_read_restart(self.h, str(path).encode(), {"exact": 0, "reference": 1}[mode], cdtin):
+            raise RuntimeError(lib().orc_last_error().decode())
 
     def dt_state(self) -> dict:
         """Current dt and the adaptive step's state (cdt, ivardt, idtstep)."""

@@ -118,6 +118,7 @@ struct Orc {
   // adaptive time step (COMMON /vardtflags/ ivardt, idtstep and cdt, comtime.h)
   double cdt = 1.0;
   int ivardt = 0, idtstep = 0;
+  int istart = 0;  // main.f istart after a restart read (0: a new run)
   // penalty COMMON (comparampen.h) used by the single-call C API
   struct Pen* pen0 = nullptr;
   // filter tables
@@ -1458,21 +1459,21 @@ void step(Orc& o) {
   if (o.ivardt == 1) o.idtstep = o.idtstep + 1;  // main.f:660-662
   convec(o);
   bool ldtadapt = (o.ivardt == 1) && (o.idtstep < 2);  // main.f:741
-  if (istep < 2) {
+  if (istep < 2 && o.istart == 0) {
     o.fac1 = 2.;
     o.fac2 = -1.;
     o.fac3 = 0.;
     o.bdf1 = 2.;
     o.bdf2 = -0.5;
     o.bdf3 = 0.;
-  } else if (!ldtadapt) {
+  } else if (istep >= 2 && !ldtadapt) {
     o.fac1 = 3.;
     o.fac2 = -3.;
     o.fac3 = 1.;
     o.bdf1 = 3.;
     o.bdf2 = -1.5;
     o.bdf3 = 1. / 3.;
-  } else {  // main.f:760-775
+  } else {  // main.f:716-730 (restart, istep = 1) and 760-775
     const double dt1 = o.dt, dt2 = o.dt, dt3 = o.cdt * o.dt;
     o.fac1 = orc_abvar1(dt1, dt2, dt3);
     o.fac2 = orc_abvar2(dt1, dt2, dt3);
@@ -1486,7 +1487,12 @@ void step(Orc& o) {
   calcuvwt(o, cpen);
   ldtadapt = (o.ivardt == 1) && (o.idtstep < 2);  // main.f:832
   if (istep < 2) {
-    o.bdfv = 1.5;
+    if (o.istart == 0) {
+      o.bdfv = 1.5;
+    } else {  // main.f:820-826
+      const double dt1 = o.dt, dt2 = o.dt, dt3 = o.cdt * o.dt;
+      o.bdfv = orc_bdfvarv(dt1, dt2, dt3);
+    }
   } else if (!ldtadapt) {
     o.bdfv = 11. / 6.;
   } else {  // main.f:846-852
@@ -1542,6 +1548,7 @@ void init_mode1(Orc& o, double A, double anoise, uint64_t seed) {
   o.cdt = 1.;
   o.ivardt = 0;
   o.idtstep = 0;
+  o.istart = 0;
   o.fac1 = 1.;
   o.fac2 = o.fac3 = 0.;
   o.bdf1 = 1.;
@@ -1721,6 +1728,7 @@ void orc_set_scalars(void* h, const double* in) {
   o->cdt = 1.;
   o->ivardt = 0;
   o->idtstep = 0;
+  o->istart = 0;
 }
 
 void orc_init_mode1(void* h, double A, double anoise, uint64_t seed) { init_mode1(*(Orc*)h, A, anoise, seed); }
@@ -1738,6 +1746,159 @@ int orc_dt_rule(double cflx, double cflz, double t, double dt, double xomega, do
   *dt_new = d;
   *cdt = c;
   return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Restart files.  output.f:2-117 writes them, restart.f:2-126 reads them and
+// main.f:555-632 sets up the steps after a read.  ifort unformatted
+// sequential: every record framed by its byte count (4-byte little-endian
+// integer) before and after; REAL*8 (-autodouble) and INTEGER*4 items.
+// Setup tables the oracle does not keep (dalpol, d3, atpz/btpz/ctpz), the
+// boundary arrays the step never reads (tubc/tbbc, uw/vw/ww), solks and the
+// soliton fields (never set: wavesetup is not called) are written as 0; past
+// nxhp, record 5 holds 0 (the reference writes past xw's bound there).  A
+// 50th record, which restart.f never reads, carries the step counter, the
+// adaptive and restart state and the coefficients (exact continuation).
+// ---------------------------------------------------------------------------
+struct RstRecs {
+  std::vector<std::vector<char>> r;
+  void open() { r.emplace_back(); }
+  void d(double v) { r.back().insert(r.back().end(), (const char*)&v, (const char*)&v + 8); }
+  void i(int32_t v) { r.back().insert(r.back().end(), (const char*)&v, (const char*)&v + 4); }
+  void zeros(size_t n8) { r.back().insert(r.back().end(), 8 * n8, (char)0); }
+  void field(const std::vector<double>& f) { r.back().insert(r.back().end(), (const char*)f.data(), (const char*)(f.data() + f.size())); }
+};
+static std::vector<size_t> rst_sizes(const Orc& o) {  // bytes of records 1..49, output.f:26-108
+  const size_t nx = o.nx, ny = o.ny, nz = o.nz, N = o.nzloc, ns = o.nsubd, nxpp = o.nxpp;
+  const size_t nz2 = ns * (N - 1) + 1;
+  std::vector<size_t> b = {8, 16, 36, 16, 16 * nx, 16 * ny, 8 * nx, 8 * ny, 8 * nz, 8 * nz2, 20 * ns, 8,
+                           8 * N * N, 8 * N * N, 8 * N, 8 * N, 8 * N * N, 8 * N * N, 8 * N * N, 24 * nz,
+                           16 * nxpp * ny, 96 * nxpp * ny, 8, 8, 16 * nxpp * nz, 16 * nxpp * nz, 16 * nxpp * nz,
+                           8 * nxpp * nz, 16 * nxpp * nz};
+  for (int q = 0; q < 20; ++q) b.push_back(8 * o.ntot);
+  return b;
+}
+
+int orc_write_restart(void* h, const char* path) {
+  Orc& o = *(Orc*)h;
+  const int N = o.nzloc, ns = o.nsubd;
+  RstRecs w;
+  w.open(); w.d(o.t);                                    // output.f:26
+  w.open(); w.d(o.pp.xnu); w.d(0.0);                     // :27, pr = xnu (main.f:428), ra = 0
+  w.open();                                              // :28
+  for (int32_t v : {o.nx, o.ny, o.nz, N - 1, o.nxpp * o.ny, (int32_t)o.ntot, ns, N, 1}) w.i(v);
+  w.open(); w.d(o.alpha); w.d(o.beta);                   // :29
+  w.open();                                              // :30
+  for (int i = 0; i < o.nx; ++i) {
+    w.d(i < o.nxhp ? o.xw[i] : 0.0);
+    w.d(i < o.nxhp ? o.xsq[i] : 0.0);
+  }
+  w.open();                                              // :31
+  for (int j = 0; j < o.ny; ++j) { w.d(o.yw[j]); w.d(o.ysq[j]); }
+  w.open(); for (double v : o.xg) w.d(v);                // :32
+  w.open(); for (double v : o.yg) w.d(v);                // :33
+  w.open(); for (double v : o.zg) w.d(v);                // :34
+  w.open(); for (int k = 1; k <= ns * (N - 1) + 1; ++k) w.d(o.zf[k]);  // :35
+  w.open(); for (int k = 0; k < ns; ++k) { w.d(o.pp.z0[k]); w.d(o.pp.zh[k]); w.i(1); }  // :36
+  w.open(); w.d(o.pp.zlen * (1. / ns));                  // :37, setup.f:281,289
+  w.open(); for (int k = 0; k < N; ++k) for (int j = 0; j < N; ++j) w.d(o.alpol[(size_t)j * N + k]);  // :38
+  w.open(); w.zeros((size_t)N * N);                      // :39 dalpol
+  w.open(); for (double v : o.zpts) w.d(v);              // :40
+  w.open(); for (double v : o.wg) w.d(v);                // :41
+  w.open(); for (int j = 0; j < N; ++j) for (int i = 0; i < N; ++i) w.d(o.dmat[(size_t)i * N + j]);   // :42
+  w.open(); for (int j = 0; j < N; ++j) for (int i = 0; i < N; ++i) w.d(o.d2mat[(size_t)i * N + j]);  // :43
+  w.open(); w.zeros((size_t)N * N);                      // :44 d3
+  w.open(); w.zeros(3 * (size_t)o.nz);                   // :45
+  w.open(); w.zeros(2 * (size_t)o.nxpp * o.ny);          // :46
+  w.open(); w.zeros(12 * (size_t)o.nxpp * o.ny);         // :47-49
+  w.open(); w.d(o.pp.umax);                              // :52
+  w.open(); w.d(0.0);                                    // :53 solks
+  for (size_t n : {2, 2, 2, 1, 2}) { w.open(); w.zeros(n * (size_t)o.nxpp * o.nz); }  // :54-58
+  for (auto* L : {o.F, o.Fn, o.Fnm, o.Sn, o.Snm})       // :66-105
+    for (int q = 0; q < 4; ++q) { w.open(); w.field(L[q]); }
+  w.open();
+  for (int32_t v : {0x32425749, 1, o.istep, o.ivardt, o.idtstep, o.istart}) w.i(v);
+  for (double v : {o.dt, o.cdt, o.fac1, o.fac2, o.fac3, o.bdf1, o.bdf2, o.bdf3, o.bdfv}) w.d(v);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) { g_err = std::string("cannot open ") + path; return 1; }
+  bool ok = true;
+  for (const auto& r : w.r) {
+    const uint32_t m = (uint32_t)r.size();
+    ok = ok && std::fwrite(&m, 4, 1, f) == 1 && (r.empty() || std::fwrite(r.data(), 1, r.size(), f) == r.size()) &&
+         std::fwrite(&m, 4, 1, f) == 1;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) { g_err = std::string("write error on ") + path; return 1; }
+  return 0;
+}
+
+// mode 0: exact continuation (needs the 50th record); 1: main.f istart = 1
+int orc_read_restart(void* h, const char* path, int mode, double cdtin) {
+  Orc& o = *(Orc*)h;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) { g_err = std::string("cannot open ") + path; return 1; }
+  std::vector<std::vector<char>> recs;
+  for (;;) {
+    uint32_t m = 0, m2 = 0;
+    if (std::fread(&m, 4, 1, f) != 1) break;
+    std::vector<char> r(m);
+    if ((m && std::fread(r.data(), 1, m, f) != m) || std::fread(&m2, 4, 1, f) != 1 || m2 != m) {
+      std::fclose(f);
+      g_err = "bad record framing";
+      return 1;
+    }
+    recs.push_back(std::move(r));
+  }
+  std::fclose(f);
+  const auto sz = rst_sizes(o);
+  if (recs.size() < sz.size()) { g_err = "fewer than 49 records"; return 1; }
+  for (size_t k = 0; k < sz.size(); ++k)
+    if (recs[k].size() != sz[k]) { g_err = "record " + std::to_string(k + 1) + " has the wrong size"; return 1; }
+  int32_t dims[9];
+  std::memcpy(dims, recs[2].data(), sizeof dims);
+  const int32_t want[8] = {o.nx, o.ny, o.nz, o.nzloc - 1, o.nxpp * o.ny, (int32_t)o.ntot, o.nsubd, o.nzloc};
+  for (int k = 0; k < 8; ++k)
+    if (dims[k] != want[k]) { g_err = "dims differ"; return 1; }
+  bool extra = recs.size() > sz.size() && recs[sz.size()].size() == 6 * 4 + 9 * 8;
+  int32_t ei[6] = {0, 0, 0, 0, 0, 0};
+  double ed[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (extra) {
+    std::memcpy(ei, recs[sz.size()].data(), sizeof ei);
+    std::memcpy(ed, recs[sz.size()].data() + sizeof ei, sizeof ed);
+    extra = ei[0] == 0x32425749 && ei[1] == 1;
+  }
+  if (mode == 0 && !extra) { g_err = "no continuation record"; return 1; }
+  std::memcpy(&o.t, recs[0].data(), 8);                  // restart.f:25
+  size_t k = 29;
+  for (auto* L : {o.F, o.Fn, o.Fnm, o.Sn, o.Snm})       // restart.f:73-113
+    for (int q = 0; q < 4; ++q, ++k) std::memcpy(L[q].data(), recs[k].data(), o.ntot * 8);
+  o.ivardt = 0;
+  o.idtstep = 0;
+  if (mode == 0) {
+    o.istep = ei[2];
+    o.ivardt = ei[3];
+    o.idtstep = ei[4];
+    o.istart = ei[5];
+    o.dt = ed[0];
+    o.cdt = ed[1];
+    o.fac1 = ed[2]; o.fac2 = ed[3]; o.fac3 = ed[4];
+    o.bdf1 = ed[5]; o.bdf2 = ed[6]; o.bdf3 = ed[7]; o.bdfv = ed[8];
+  } else {  // main.f:613-632 with istart = 1
+    o.istep = 0;
+    o.istart = 1;
+    o.cdt = cdtin;
+    const double dt1 = o.dt, dt2 = o.cdt * o.dt, dt3 = o.cdt * o.dt;
+    o.fac1 = orc_abvar1(dt1, dt2, dt3);
+    o.fac2 = orc_abvar2(dt1, dt2, dt3);
+    o.fac3 = orc_abvar3(dt1, dt2, dt3);
+    o.bdf1 = orc_bdfvar1(dt1, dt2, dt3);
+    o.bdf2 = orc_bdfvar2(dt1, dt2, dt3);
+    o.bdf3 = orc_bdfvar3(dt1, dt2, dt3);
+    o.bdfv = orc_bdfvarv(dt1, dt2, dt3);
+  }
+  o.fact = 1. / (o.pp.xkappa * o.dt);
+  o.facvel = 1. / (o.pp.xnu * o.dt);
+  return 0;
 }
 
 void orc_step(void* h) { step(*(Orc*)h); }

