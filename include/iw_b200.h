@@ -184,6 +184,21 @@ int iw_write_restart(iw_handle *h, const char *path);
  * its own input.dat. */
 int iw_read_restart(iw_handle *h, const char *path, int mode, double cdtin);
 
+/* Replaces output.f:118-265 (plotf; main.f:543,607,1039): u, v, w and temp
+ * in physical space, after t, nx ny nz ntot and the x, y, z grids.
+ * iform 0: unformatted sequential (as the restart files), the fields as
+ * REAL*4 over (nxpp, ny, nz); iform 1: formatted, 5e14.6 for reals and 5i10
+ * for the dims.  The padding entries i = nx+1, nx+2 hold 0.  Asynchronous:
+ * the transforms and the copies into a pinned host buffer are queued on the
+ * handle's stream and the call returns; a host thread writes the file while
+ * later steps run.  Call iw_wait_fields before reading the file.  The state
+ * is not changed (the reference transforms it back, a projection the next
+ * step's maxcalc round trip applies anyway). */
+int iw_write_fields(iw_handle *h, const char *path, int iform);
+/* Waits for the last iw_write_fields to finish its file; returns its status
+ * (IW_ERR_IO with the reason in iw_last_error() if the file failed). */
+int iw_wait_fields(iw_handle *h);
+
 /* Mode-1 internal wave initial condition plus seeded uniform noise in the
  * bottom 20% of the depth, transformed to spectral space (a new init: the
  * reference init.f sets zeros).  Deterministic for a given seed. */

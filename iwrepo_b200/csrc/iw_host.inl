@@ -313,6 +313,14 @@ struct iw_handle {
   // 1 after iw_read_restart in the reference's mode (main.f istart = 1): the
   // first step's schedule uses variable-step coefficients with ratio cdt
   int istart = 0;
+  // asynchronous field dumps (iw_write_fields): pinned staging buffer, the
+  // event after the last copy into it, and the writer thread of the last dump
+  void* out_host = nullptr;
+  size_t out_bytes = 0;
+  cudaEvent_t out_ev = nullptr;
+  std::thread* out_thread = nullptr;
+  int out_status = 0;
+  std::string out_msg;
   Tables tab;
   // device tables
   double *ddzinv = 0, *dpart = 0;  // diagnostics: dt-free CFL spacing per level, per-block partials
@@ -1761,9 +1769,14 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
   return IW_OK;
 }
 
+static int out_join(iw_handle* h);
+
 int iw_destroy(iw_handle* h) {
   if (!h) return IW_OK;
   cudaSetDevice(h->dev);
+  out_join(h);
+  if (h->out_host) cudaFreeHost(h->out_host);
+  if (h->out_ev) cudaEventDestroy(h->out_ev);
   free_fields(h->f64);
   free_fields(h->f32);
   for (double* p : {h->ddzinv, h->dpart, h->dDt, h->dD2t, h->dLt, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
@@ -2220,3 +2233,4 @@ static int helm_batched(iw_handle* h, const double* lam_dev, int ncol, int bot, 
 
 #include "iw_abi.inl"
 #include "iw_restart.inl"
+#include "iw_output.inl"

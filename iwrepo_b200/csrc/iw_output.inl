@@ -1,0 +1,222 @@
+// Field dumps: output.f:118-265 (subroutine plotf).  u, v, w and temp are
+// transformed to physical space and written with the run time, the dims and
+// the grid:
+//   iform = 0: unformatted sequential (the framing of the restart files):
+//              t | nx, ny, nz, ntot | x(1..nx) | y | z | then u, v, w, temp as
+//              REAL*4 over (nxpp, ny, nz), one record each;
+//   iform = 1: formatted, FORMAT 5e14.6 for the reals and 5i10 for the dims,
+//              the four fields in one list (output.f:214-223).
+// The two padding entries of every x row (i = nx+1, nx+2) hold 0, which is
+// what the inverse transform of horfft leaves there.  The reference ends
+// plotf by transforming the fields back to spectral space, a projection that
+// the next step's maxcalc round trip applies anyway; here the state is not
+// touched at all.
+//
+// The dump is asynchronous: the transforms and the copies into a pinned host
+// buffer are queued on the handle's stream, and a host thread waits for them
+// and writes the file while later steps run.  iw_wait_fields joins it.
+
+namespace fout {
+
+// Fortran Ew.d output for w = 14, d = 6: [-]0.dddddd E[+-]ee, right-justified.
+static void e14_6(std::string& s, double v) {
+  char cell[32];
+  if (std::isnan(v)) {
+    snprintf(cell, sizeof cell, "%14s", "NaN");
+  } else if (std::isinf(v)) {
+    snprintf(cell, sizeof cell, "%14s", v < 0 ? "-Infinity" : "Infinity");
+  } else if (v == 0.0) {
+    snprintf(cell, sizeof cell, "%14s", std::signbit(v) ? "-0.000000E+00" : "0.000000E+00");
+  } else {
+    char m[32];
+    snprintf(m, sizeof m, "%.5e", std::fabs(v));  // d.ddddde[+-]x..x, correctly rounded
+    const int e = atoi(m + 8) + 1;                // exponent of the 0.dddddd form
+    char body[32];
+    const char* sign = v < 0 ? "-" : "";
+    const int ae = e < 0 ? -e : e;
+    if (ae <= 99)
+      snprintf(body, sizeof body, "%s0.%c%.5sE%c%02d", sign, m[0], m + 2, e < 0 ? '-' : '+', ae);
+    else  // three-digit exponents drop the E
+      snprintf(body, sizeof body, "%s0.%c%.5s%c%03d", sign, m[0], m + 2, e < 0 ? '-' : '+', ae);
+    snprintf(cell, sizeof cell, "%14s", body);
+  }
+  s += cell;
+}
+
+// one formatted WRITE of a list of reals with FORMAT 5e14.6
+struct List {
+  std::string s;
+  int col = 0;
+  void real(double v) {
+    if (col == 5) {
+      s += '\n';
+      col = 0;
+    }
+    e14_6(s, v);
+    ++col;
+  }
+  void end() {
+    s += '\n';
+    col = 0;
+  }
+};
+
+struct Job {
+  std::string path;
+  int iform = 0, dev = 0, nx = 0, ny = 0, nz = 0, nxpp = 0;
+  size_t ntot = 0;
+  bool fp32 = false;  // the pinned buffer holds float (mixed handles) or double
+  double t = 0;
+  std::vector<double> x, y, z;
+  const void* host = nullptr;
+  cudaEvent_t ev = nullptr;
+};
+
+static double value(const Job& j, size_t q, size_t p) {
+  const size_t i = p % (size_t)j.nxpp;
+  if (i >= (size_t)j.nx) return 0.0;
+  return j.fp32 ? (double)((const float*)j.host)[q * j.ntot + p] : ((const double*)j.host)[q * j.ntot + p];
+}
+
+static bool write_job(const Job& j, std::string* msg) {
+  FILE* f = fopen(j.path.c_str(), j.iform == 0 ? "wb" : "w");
+  if (!f) {
+    *msg = "cannot open " + j.path + " for writing";
+    return false;
+  }
+  bool ok = true;
+  if (j.iform == 0) {
+    auto rec = [&](const void* d, size_t n) { return rst::put_record(f, d, n); };
+    const int32_t dims[4] = {j.nx, j.ny, j.nz, (int32_t)j.ntot};
+    ok = rec(&j.t, 8) && rec(dims, sizeof dims) && rec(j.x.data(), 8 * j.x.size()) && rec(j.y.data(), 8 * j.y.size()) &&
+         rec(j.z.data(), 8 * j.z.size());
+    std::vector<float> buf(j.ntot);
+    for (size_t q = 0; q < 4 && ok; ++q) {
+      for (size_t p = 0; p < j.ntot; ++p) buf[p] = (float)value(j, q, p);  // real(u(i,j,k)), output.f:158
+      ok = rec(buf.data(), 4 * j.ntot);
+    }
+  } else {
+    List l;
+    l.real(j.t);
+    l.end();
+    char c[16];
+    for (int v : {j.nx, j.ny, j.nz, (int)j.ntot}) {
+      snprintf(c, sizeof c, "%10d", v);
+      l.s += c;
+    }
+    l.s += '\n';
+    for (const auto* a : {&j.x, &j.y, &j.z}) {
+      for (double v : *a) l.real(v);
+      l.end();
+    }
+    ok = fwrite(l.s.data(), 1, l.s.size(), f) == l.s.size();
+    l.s.clear();
+    for (size_t q = 0; q < 4 && ok; ++q)
+      for (size_t p = 0; p < j.ntot && ok; ++p) {
+        l.real(value(j, q, p));
+        if (l.s.size() > (1u << 22)) {
+          ok = fwrite(l.s.data(), 1, l.s.size(), f) == l.s.size();
+          l.s.clear();
+        }
+      }
+    l.end();
+    ok = ok && fwrite(l.s.data(), 1, l.s.size(), f) == l.s.size();
+  }
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) *msg = "write error on " + j.path;
+  return ok;
+}
+
+}  // namespace fout
+
+static int out_join(iw_handle* h) {
+  if (!h->out_thread) return IW_OK;
+  h->out_thread->join();
+  delete h->out_thread;
+  h->out_thread = nullptr;
+  return h->out_status;
+}
+
+extern "C" {
+
+int iw_write_fields(iw_handle* h, const char* path, int iform) {
+  if (!h || !path) return set_err(IW_ERR_STATE, "iw_write_fields: bad argument");
+  if (iform != 0 && iform != 1) return set_err(IW_ERR_CONFIG, "iw_write_fields: iform must be 0 or 1");
+  if (!rst::little_endian()) return set_err(IW_ERR_CONFIG, "unformatted files are little-endian; this host is not");
+  if ((size_t)4 * h->ntot > rst::kMaxRecord)
+    return set_err(IW_ERR_CONFIG, "a REAL*4 field record would exceed 2147483639 bytes");
+  cudaSetDevice(h->dev);
+  if (out_join(h) != IW_OK) {
+    h->out_status = IW_OK;
+    return set_err(IW_ERR_IO, "the previous field dump failed: " + h->out_msg);
+  }
+  const size_t esz = h->mixed ? sizeof(float) : sizeof(double);
+  const size_t need = 4 * h->ntot * esz;
+  if (h->out_bytes < need) {
+    if (h->out_host) cudaFreeHost(h->out_host);
+    h->out_host = nullptr;
+    h->out_bytes = 0;
+    CK(cudaMallocHost(&h->out_host, need));
+    h->out_bytes = need;
+  }
+  if (!h->out_ev) CK(cudaEventCreateWithFlags(&h->out_ev, cudaEventDisableTiming));
+  for (int q = 0; q < 4; ++q) {
+    void* dst = (char*)h->out_host + (size_t)q * h->ntot * esz;
+    if (h->mixed) {
+      phys_of<float>(h, h->f32, h->f32.F[q], h->f32.Y12[0], h->f32.Y12[1], 0);
+      CK(cudaMemcpyAsync(dst, h->f32.Y12[0], h->ntot * esz, cudaMemcpyDeviceToHost, h->st));
+    } else {
+      phys_of<double>(h, h->f64, h->f64.F[q], h->f64.Y12[0], h->f64.Y12[1], 0);
+      CK(cudaMemcpyAsync(dst, h->f64.Y12[0], h->ntot * esz, cudaMemcpyDeviceToHost, h->st));
+    }
+  }
+  CK(cudaEventRecord(h->out_ev, h->st));
+  fout::Job j;
+  j.path = path;
+  j.iform = iform;
+  j.dev = h->dev;
+  j.nx = h->nx;
+  j.ny = h->ny;
+  j.nz = h->nz;
+  j.nxpp = h->nxpp;
+  j.ntot = h->ntot;
+  j.fp32 = h->mixed;
+  j.t = h->t;
+  j.host = h->out_host;
+  j.ev = h->out_ev;
+  {  // setup.f:136-166 grids
+    const double pi2 = 8. * std::atan(1.0), xl = pi2 / (pi2 / h->p.xlen), yl = pi2 / (pi2 / h->p.ylen);
+    for (int i = 0; i < h->nx; ++i) j.x.push_back(i * xl / h->nx);
+    for (int jj = 0; jj < h->ny; ++jj) j.y.push_back(jj * yl / h->ny);
+    for (int ks = 0; ks < h->ns; ++ks)
+      for (int kl = 0; kl < h->N; ++kl) j.z.push_back(h->p.z0[ks] + 0.5 * h->p.zh[ks] * (h->tab.zpts[kl] + 1.0));
+  }
+  h->out_status = IW_OK;
+  h->out_msg.clear();
+  h->out_thread = new std::thread([h, j]() {
+    cudaSetDevice(j.dev);
+    if (cudaEventSynchronize(j.ev) != cudaSuccess) {
+      h->out_msg = "the copies of the dump failed";
+      h->out_status = IW_ERR_CUDA;
+      return;
+    }
+    std::string msg;
+    if (!fout::write_job(j, &msg)) {
+      h->out_msg = msg;
+      h->out_status = IW_ERR_IO;
+    }
+  });
+  return IW_OK;
+}
+
+int iw_wait_fields(iw_handle* h) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  const int r = out_join(h);
+  if (r != IW_OK) {
+    h->out_status = IW_OK;
+    return set_err(r, "field dump: " + h->out_msg);
+  }
+  return IW_OK;
+}
+
+}  // extern "C"

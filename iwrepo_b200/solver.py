@@ -103,6 +103,17 @@ class Solver:
         records plus the continuation record)."""
         _lib.check(_lib.lib().iw_write_restart(self.h, str(path).encode()))
 
+    def write_fields(self, path: str, iform: int = 0, wait: bool = True):
+        """plotf's field dump through iw_write_fields (iform 0 unformatted
+        REAL*4, 1 formatted 5e14.6).  With wait=False the file is written by a
+        host thread while later steps run; call wait_fields() before reading it."""
+        _lib.check(_lib.lib().iw_write_fields(self.h, str(path).encode(), iform))
+        if wait:
+            self.wait_fields()
+
+    def wait_fields(self):
+        _lib.check(_lib.lib().iw_wait_fields(self.h))
+
     def read_restart(self, path: str, mode: str = "reference", cdtin: float = 1.0):
         """restart.f through iw_read_restart: mode "reference" gives main.f's
         istart = 1 start (cdtin = old dt / new dt), "exact" continues a run

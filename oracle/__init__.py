@@ -70,6 +70,9 @@ def lib():
         L.orc_band_factor.restype = C.c_int
         L.orc_get_dt.argtypes = [C.c_void_p, PD]
         L.orc_write_restart.argtypes = [C.c_void_p, C.c_char_p]
+        L.orc_plotf.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+        L.orc_plotf.restype = C.c_int
+        L.orc_format_e14_6.argtypes = [D, C.c_char_p]
         L.orc_write_restart.restype = C.c_int
         L.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, D]
         L.orc_read_restart.restype = C.c_int
@@ -134,6 +137,11 @@ class Oracle:
     def write_restart(self, path: str):
         """output.f's restart dump (see orc_write_restart)."""
         if lib().orc_write_restart(self.h, str(path).encode()):
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def plotf(self, path: str, iform: int = 0):
+        """output.f's field dump (see orc_plotf)."""
+        if lib().orc_plotf(self.h, str(path).encode(), iform):
             raise RuntimeError(lib().orc_last_error().decode())
 
     def read_restart(self, path: str, mode: str = "reference", cdtin: float = 1.0):
@@ -242,6 +250,13 @@ def dt_rule(cflx: float, cflz: float, t: float, dt: float, xomega: float):
     if lib().orc_dt_rule(cflx, cflz, t, dt, xomega, C.byref(dn), C.byref(c)):
         return dn.value, c.value
     return None
+
+
+def format_e14_6(v: float) -> str:
+    """The oracle's Fortran E14.6 edit descriptor for one value."""
+    b = C.create_string_buffer(16)
+    lib().orc_format_e14_6(v, b)
+    return b.value.decode()
 
 
 def set_threads(n: int):

@@ -1901,6 +1901,89 @@ int orc_read_restart(void* h, const char* path, int mode, double cdtin) {
   return 0;
 }
 
+// output.f:118-265 (plotf): the fields in physical space (horfft +1 on
+// copies: the oracle's state is left as it is), after t, the dims and the
+// grids; iform 0 unformatted with REAL*4 fields, 1 formatted 5e14.6 / 5i10.
+static std::string fortran_e14_6(double v) {
+  char out[40];
+  if (std::isnan(v)) { std::snprintf(out, sizeof out, "%14s", "NaN"); return out; }
+  if (std::isinf(v)) { std::snprintf(out, sizeof out, "%14s", v > 0 ? "Infinity" : "-Infinity"); return out; }
+  std::string body = std::signbit(v) ? "-0." : "0.";
+  int e = 0;
+  if (v != 0.0) {
+    char m[40];
+    std::snprintf(m, sizeof m, "%.5e", std::fabs(v));  // 6 significant digits
+    body += m[0];
+    body.append(m + 2, 5);
+    e = std::atoi(m + 8) + 1;
+  } else {
+    body += "000000";
+  }
+  char ex[16];
+  if (std::abs(e) <= 99) std::snprintf(ex, sizeof ex, "E%c%02d", e < 0 ? '-' : '+', std::abs(e));
+  else std::snprintf(ex, sizeof ex, "%c%03d", e < 0 ? '-' : '+', std::abs(e));
+  body += ex;
+  std::snprintf(out, sizeof out, "%14s", body.c_str());
+  return out;
+}
+
+// one Ew.d cell (w = 14, d = 6) into out (15 bytes)
+void orc_format_e14_6(double v, char* out) { std::snprintf(out, 15, "%s", fortran_e14_6(v).c_str()); }
+
+int orc_plotf(void* h, const char* path, int iform) {
+  Orc& o = *(Orc*)h;
+  std::vector<double> phys[4];
+  for (int q = 0; q < 4; ++q) {
+    phys[q] = o.F[q];
+    horfft(o, phys[q].data(), 1, o.nz);
+  }
+  FILE* f = std::fopen(path, iform == 0 ? "wb" : "w");
+  if (!f) { g_err = std::string("cannot open ") + path; return 1; }
+  bool ok = true;
+  auto rec = [&](const void* d, uint32_t n) {
+    ok = ok && std::fwrite(&n, 4, 1, f) == 1 && (n == 0 || std::fwrite(d, 1, n, f) == n) && std::fwrite(&n, 4, 1, f) == 1;
+  };
+  if (iform == 0) {
+    const int32_t dims[4] = {o.nx, o.ny, o.nz, (int32_t)o.ntot};
+    rec(&o.t, 8);
+    rec(dims, 16);
+    rec(o.xg.data(), 8 * (uint32_t)o.nx);
+    rec(o.yg.data(), 8 * (uint32_t)o.ny);
+    rec(o.zg.data(), 8 * (uint32_t)o.nz);
+    std::vector<float> t4(o.ntot);
+    for (int q = 0; q < 4; ++q) {
+      for (size_t p = 0; p < o.ntot; ++p) t4[p] = (float)phys[q][p];  // tempout = real(u), output.f:158
+      rec(t4.data(), 4 * (uint32_t)o.ntot);
+    }
+  } else {
+    std::string s;
+    int col = 0;
+    auto put = [&](double v) {
+      if (col == 5) { s += '\n'; col = 0; }
+      s += fortran_e14_6(v);
+      ++col;
+    };
+    auto endl = [&]() { s += '\n'; col = 0; };
+    put(o.t); endl();
+    char c[16];
+    for (long v : {(long)o.nx, (long)o.ny, (long)o.nz, (long)o.ntot}) { std::snprintf(c, sizeof c, "%10ld", v); s += c; }
+    s += '\n';
+    for (double v : o.xg) put(v);
+    endl();
+    for (double v : o.yg) put(v);
+    endl();
+    for (double v : o.zg) put(v);
+    endl();
+    for (int q = 0; q < 4; ++q)
+      for (double v : phys[q]) put(v);
+    endl();
+    ok = std::fwrite(s.data(), 1, s.size(), f) == s.size();
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) { g_err = std::string("write error on ") + path; return 1; }
+  return 0;
+}
+
 void orc_step(void* h) { step(*(Orc*)h); }
 void orc_run(void* h, int n) {
   for (int s = 0; s < n; ++s) step(*(Orc*)h);
