@@ -195,6 +195,19 @@ int iw_read_restart(iw_handle *h, const char *path, int mode, double cdtin);
  * is not changed (the reference transforms it back, a projection the next
  * step's maxcalc round trip applies anyway). */
 int iw_write_fields(iw_handle *h, const char *path, int iform);
+/* Replaces the animation dumps of convec (solver.f:136-222, dtanim of the
+ * &inputs namelist): with dtanim > 0, every iw_step whose time t is at least
+ * dtanim past the last dump (Tdump, starting at 0 here) writes
+ * dir/vortanimout_NNNNN.dat (NNNNN counts the dumps from 1): a list-directed
+ * ZONE header, then x, z, u, w, temp, temp + rhomean(z) in physical space,
+ * FORMAT (1x,6(F25.16,3x)), for every subdomain point and x index.  The rows
+ * are those the reference reads: its y index is the value the preceding loop
+ * leaves, ny+1, i.e. row 1 of the next z-plane, and past the last plane the
+ * first rows of v, temp and un (COMMON /flow/ order).  Written like
+ * iw_write_fields, by a host thread; iw_wait_fields waits for the last one.
+ * dtanim <= 0 turns the dumps off.  Steps with dumps are not replayed from
+ * graphs. */
+int iw_set_animation(iw_handle *h, double dtanim, const char *dir);
 /* Waits for the last iw_write_fields to finish its file; returns its status
  * (IW_ERR_IO with the reason in iw_last_error() if the file failed). */
 int iw_wait_fields(iw_handle *h);

@@ -321,6 +321,14 @@ struct iw_handle {
   std::thread* out_thread = nullptr;
   int out_status = 0;
   std::string out_msg;
+  // animation dumps (solver.f:136-222): interval (0 = off), the time of the
+  // last dump (COMMON /Dump/ Tdump), the file counter, directory and staging
+  double dtanim = 0, tdump = 0;
+  int ianimc = 0;
+  bool anim_pending = false;  // this step's convec dumps (after stage A)
+  std::string anim_dir;
+  void* anim_host = nullptr;
+  size_t anim_bytes = 0;
   Tables tab;
   // device tables
   double *ddzinv = 0, *dpart = 0;  // diagnostics: dt-free CFL spacing per level, per-block partials
@@ -1036,6 +1044,9 @@ static void rotate_levels(FieldSet<T>& fs) {
 // convec (solver.f:6-514).  proj=1 also applies the maxcalc round trip that
 // precedes it in the main loop (main.f:657).
 template <typename T>
+static int anim_dump(iw_handle* h, FieldSet<T>& fs);
+
+template <typename T>
 static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
   typedef typename cplx_t<T>::type C;
   Geo g = geo(h);
@@ -1044,6 +1055,11 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
   // K_A
   launch_stageA<T>(h, fs, proj);
   mark(h, 0);
+  if (h->anim_pending) {  // the dump sees the fields convec sees: projected, mean w removed
+    h->anim_pending = false;
+    int r = anim_dump<T>(h, fs);
+    if (r) return r;
+  }
   // K_B: y-inverse of 12 arrays
   {
     YJobs<T> jb;
@@ -1385,6 +1401,11 @@ static int full_step(iw_handle* h, FieldSet<T>& fs) {
   int r;
   if (h->p.imaxcalc == 1 && (r = adapt_dt<T>(h, fs))) return r;
   if (h->ivardt == 1) h->idtstep += 1;  // main.f:660-662
+  if (h->dtanim > 0 && (h->t - h->tdump) >= h->dtanim) {  // solver.f:141-142, inside convec
+    h->tdump = h->t;
+    h->ianimc += 1;
+    h->anim_pending = true;
+  }
   const int cpen = (h->p.ispecfilterexp == 1) && (h->istep % h->p.nspecfilterexp == 0);
   r = ensure_factors(h, cpen);
   if (r) return r;
@@ -1504,11 +1525,12 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
 // Conditions that would make a step depend on its number keep the eager path:
 // paddle forcing (time in the arguments), a filter not applied every step,
 // interface averaging less often than every step, per-phase profiling, an
-// adaptive step (its rule reads the CFL numbers back at every step).
+// adaptive step (its rule reads the CFL numbers back at every step), animation
+// dumps (their schedule depends on t).
 // ---------------------------------------------------------------------------
 static bool graph_ready(const iw_handle* h) {
   return h->istep >= 3 && !h->prof && !h->p.forcing && (h->p.ispecfilterexp != 1 || h->p.nspecfilterexp == 1) &&
-         h->p.navgintrfc <= 1 && h->p.imaxcalc != 1;
+         h->p.navgintrfc <= 1 && h->p.imaxcalc != 1 && !(h->dtanim > 0);
 }
 
 static int step_dispatch(iw_handle* h) { return h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64); }
@@ -1776,6 +1798,7 @@ int iw_destroy(iw_handle* h) {
   cudaSetDevice(h->dev);
   out_join(h);
   if (h->out_host) cudaFreeHost(h->out_host);
+  if (h->anim_host) cudaFreeHost(h->anim_host);
   if (h->out_ev) cudaEventDestroy(h->out_ev);
   free_fields(h->f64);
   free_fields(h->f32);

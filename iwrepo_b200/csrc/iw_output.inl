@@ -137,7 +137,155 @@ static int out_join(iw_handle* h) {
   return h->out_status;
 }
 
+// Animation dumps, solver.f:136-222: when t - Tdump >= dtanim at the start of
+// convec, file vortanimout_NNNNN.dat (NNNNN = the dump counter, i5.5) holds
+//   ' ZONE F=POINT, I=', nx, ', J=', nz          (list-directed: I12 fields,
+//                                                 a blank before ', J=')
+// then, for ks, kloc, i: x, z, u, w, temp, temp + rhomean(z) in physical
+// space, FORMAT (1x,6(F25.16,3x)).  The reference indexes the fields with the
+// y loop variable that the loop of solver.f:82-100 leaves behind, j = ny+1:
+// u(i,ny+1,k) is u(i,1,k+1), and for k = nz the row after u, w and temp in
+// COMMON /flow/: v(i,1,1), temp(i,1,1) and un(i,1,1) (physical, physical,
+// and the spectral level n-1).  The same rows are written here.  The
+// animdump.log line of the reference is not written.
+namespace fout {
+
+struct AnimJob {
+  std::string path;
+  int dev = 0, nx = 0, nz = 0, nxpp = 0;
+  bool fp32 = false;
+  std::vector<double> x, z;
+  double rg = 0;  // rhograd (forcing.f:115-120)
+  const void* host = nullptr;
+  cudaEvent_t ev = nullptr;
+};
+
+static bool write_anim(const AnimJob& j, std::string* msg) {
+  FILE* f = fopen(j.path.c_str(), "w");
+  if (!f) {
+    *msg = "cannot open " + j.path + " for writing";
+    return false;
+  }
+  const size_t row = j.nxpp, nz = j.nz;
+  auto at = [&](size_t r, size_t i) -> double {
+    return j.fp32 ? (double)((const float*)j.host)[r * row + i] : ((const double*)j.host)[r * row + i];
+  };
+  std::string s;
+  char c[96];
+  snprintf(c, sizeof c, " ZONE F=POINT, I=%12d , J=%12d\n", j.nx, j.nz);
+  s += c;
+  bool ok = true;
+  for (size_t k = 0; k < nz && ok; ++k) {
+    const double zz = j.z[k];
+    // staging rows: u k=1..nz-1 | w | temp | v(k=0) | temp(k=0) | un(k=0)
+    const bool last = k + 1 == nz;
+    const size_t ru = last ? 3 * (nz - 1) : k, rw = last ? 3 * (nz - 1) + 1 : (nz - 1) + k,
+                 rt = last ? 3 * (nz - 1) + 2 : 2 * (nz - 1) + k;
+    for (int i = 0; i < j.nx; ++i) {
+      const double tt = at(rt, i);
+      const double v[6] = {j.x[i], zz, at(ru, i), at(rw, i), tt, tt + (1. + j.rg * zz)};
+      s += ' ';
+      for (double x : v) {
+        snprintf(c, sizeof c, "%25.16f   ", x);
+        s += c;
+      }
+      s += '\n';
+    }
+    if (s.size() > (1u << 22)) {
+      ok = fwrite(s.data(), 1, s.size(), f) == s.size();
+      s.clear();
+    }
+  }
+  ok = ok && fwrite(s.data(), 1, s.size(), f) == s.size();
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) *msg = "write error on " + j.path;
+  return ok;
+}
+
+}  // namespace fout
+
+template <typename T>
+static int anim_dump(iw_handle* h, FieldSet<T>& fs) {
+  if (out_join(h) != IW_OK) {
+    h->out_status = IW_OK;
+    return set_err(IW_ERR_IO, "the previous dump failed: " + h->out_msg);
+  }
+  const size_t row = h->nxpp, plane = (size_t)h->nxpp * h->ny, nz = h->nz, es = sizeof(T);
+  const size_t need = (3 * (nz - 1) + 3) * row * es;
+  if (h->anim_bytes < need) {
+    if (h->anim_host) cudaFreeHost(h->anim_host);
+    h->anim_host = nullptr;
+    h->anim_bytes = 0;
+    CK(cudaMallocHost(&h->anim_host, need));
+    h->anim_bytes = need;
+  }
+  if (!h->out_ev) CK(cudaEventCreateWithFlags(&h->out_ev, cudaEventDisableTiming));
+  T* dst = fs.Y12[0];
+  char* hb = (char*)h->anim_host;
+  // Sources: F1, stage A's copy of the state as convec sees it (after the
+  // maxcalc round trip, with the mean of w removed, solver.f:64-67); Y12 is
+  // free until the y-inverse that follows.
+  // rows j = 1 of planes k = 2..nz (0-based: plane k+1, row 0) of u, w, temp
+  const int qs[3] = {0, 2, 3};
+  for (int n = 0; n < 3; ++n) {
+    phys_of<T>(h, fs, fs.F1[qs[n]], dst, fs.Y12[1], 0);
+    if (nz > 1)
+      CK(cudaMemcpy2DAsync(hb + (size_t)n * (nz - 1) * row * es, row * es, dst + plane, plane * es, row * es, nz - 1,
+                           cudaMemcpyDeviceToHost, h->st));
+    if (qs[n] == 3)  // temp(i,1,1): the row after w in COMMON /flow/
+      CK(cudaMemcpyAsync(hb + (3 * (nz - 1) + 1) * row * es, dst, row * es, cudaMemcpyDeviceToHost, h->st));
+  }
+  phys_of<T>(h, fs, fs.F1[1], dst, fs.Y12[1], 0);  // v(i,1,1): the row after u
+  CK(cudaMemcpyAsync(hb + 3 * (nz - 1) * row * es, dst, row * es, cudaMemcpyDeviceToHost, h->st));
+  // un(i,1,1): the row after temp, the spectral level n-1 of u
+  CK(cudaMemcpyAsync(hb + (3 * (nz - 1) + 2) * row * es, fs.Fn[0], row * es, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaEventRecord(h->out_ev, h->st));
+  fout::AnimJob j;
+  char name[32];
+  snprintf(name, sizeof name, "vortanimout_%05d.dat", h->ianimc);  // fmt (i5.5,a4), solver.f:159-167
+  j.path = h->anim_dir.empty() ? std::string(name) : h->anim_dir + "/" + name;
+  j.dev = h->dev;
+  j.nx = h->nx;
+  j.nz = h->nz;
+  j.nxpp = h->nxpp;
+  j.fp32 = sizeof(T) == 4;
+  j.rg = -h->p.rho0 * (h->p.brunt * h->p.brunt) / h->p.grav;
+  {
+    const double pi2 = 8. * std::atan(1.0), xl = pi2 / (pi2 / h->p.xlen);
+    for (int i = 0; i < h->nx; ++i) j.x.push_back(i * xl / h->nx);
+    for (int ks = 0; ks < h->ns; ++ks)
+      for (int kl = 0; kl < h->N; ++kl) j.z.push_back(h->p.z0[ks] + 0.5 * h->p.zh[ks] * (h->tab.zpts[kl] + 1.0));
+  }
+  j.host = h->anim_host;
+  j.ev = h->out_ev;
+  h->out_status = IW_OK;
+  h->out_msg.clear();
+  h->out_thread = new std::thread([h, j]() {
+    cudaSetDevice(j.dev);
+    if (cudaEventSynchronize(j.ev) != cudaSuccess) {
+      h->out_msg = "the copies of the animation dump failed";
+      h->out_status = IW_ERR_CUDA;
+      return;
+    }
+    std::string msg;
+    if (!fout::write_anim(j, &msg)) {
+      h->out_msg = msg;
+      h->out_status = IW_ERR_IO;
+    }
+  });
+  return IW_OK;
+}
+
 extern "C" {
+
+int iw_set_animation(iw_handle* h, double dtanim, const char* dir) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  h->dtanim = dtanim > 0 ? dtanim : 0;
+  h->anim_dir = dir ? dir : "";
+  h->tdump = 0;
+  h->ianimc = 0;
+  return IW_OK;
+}
 
 int iw_write_fields(iw_handle* h, const char* path, int iform) {
   if (!h || !path) return set_err(IW_ERR_STATE, "iw_write_fields: bad argument");

@@ -114,6 +114,11 @@ class Solver:
     def wait_fields(self):
         _lib.check(_lib.lib().iw_wait_fields(self.h))
 
+    def set_animation(self, dtanim: float, directory: str = ""):
+        """convec's animation dumps (vortanimout_NNNNN.dat in directory) every
+        dtanim of simulated time; dtanim <= 0 turns them off."""
+        _lib.check(_lib.lib().iw_set_animation(self.h, dtanim, str(directory).encode()))
+
     def read_restart(self, path: str, mode: str = "reference", cdtin: float = 1.0):
         """restart.f through iw_read_restart: mode "reference" gives main.f's
         istart = 1 start (cdtin = old dt / new dt), "exact" continues a run

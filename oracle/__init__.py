@@ -73,6 +73,7 @@ def lib():
         L.orc_plotf.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
         L.orc_plotf.restype = C.c_int
         L.orc_format_e14_6.argtypes = [D, C.c_char_p]
+        L.orc_set_animation.argtypes = [C.c_void_p, D, C.c_char_p]
         L.orc_write_restart.restype = C.c_int
         L.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, D]
         L.orc_read_restart.restype = C.c_int
@@ -138,6 +139,10 @@ class Oracle:
         """output.f's restart dump (see orc_write_restart)."""
         if lib().orc_write_restart(self.h, str(path).encode()):
             raise RuntimeError(lib().orc_last_error().decode())
+
+    def set_animation(self, dtanim: float, directory: str = ""):
+        """convec's animation dumps (see anim_dump) every dtanim."""
+        lib().orc_set_animation(self.h, dtanim, str(directory).encode())
 
     def plotf(self, path: str, iform: int = 0):
         """output.f's field dump (see orc_plotf)."""

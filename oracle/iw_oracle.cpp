@@ -119,6 +119,10 @@ struct Orc {
   double cdt = 1.0;
   int ivardt = 0, idtstep = 0;
   int istart = 0;  // main.f istart after a restart read (0: a new run)
+  // animation dumps (solver.f:136-222): interval (0 = off), Tdump, counter
+  double dtanim = 0, tdump = 0;
+  int ianimc = 0;
+  std::string anim_dir;
   // penalty COMMON (comparampen.h) used by the single-call C API
   struct Pen* pen0 = nullptr;
   // filter tables
@@ -1449,6 +1453,47 @@ void adapt_dt(Orc& o) {
   o.idtstep = 0;
 }
 
+// solver.f:136-222: the animation dump of convec.  Physical fields by
+// horfft +1 on copies.  The reference reads u(i,j,k) with j = ny+1, the value
+// the y loop of solver.f:82-100 leaves: u(i,1,k+1), and for k = nz the first
+// row of the array after it in COMMON /flow/ (u -> v, w -> temp, temp -> un).
+void anim_dump(Orc& o) {
+  const size_t row = o.nxpp, plane = (size_t)o.nxpp * o.ny;
+  std::vector<double> ph[4];
+  for (int q = 0; q < 4; ++q) {
+    ph[q] = o.F[q];
+    if (q == 2)  // wc(1,1,k) = 0 at the top of convec (solver.f:64-67)
+      for (int k = 0; k < o.nz; ++k) ph[q][o.idx(0, 0, k)] = ph[q][o.idx(1, 0, k)] = 0.0;
+    horfft(o, ph[q].data(), 1, o.nz);
+  }
+  // COMMON /flow/ from u on: u v w temp (physical here) then un (spectral)
+  auto flow = [&](int arr, size_t idx) -> double {
+    const size_t n = o.ntot;
+    while (idx >= n) { idx -= n; ++arr; }
+    return arr < 4 ? ph[arr][idx] : o.Fn[arr - 4][idx];
+  };
+  char name[32];
+  std::snprintf(name, sizeof name, "vortanimout_%05d.dat", o.ianimc);
+  const std::string path = o.anim_dir.empty() ? std::string(name) : o.anim_dir + "/" + name;
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return;
+  std::fprintf(f, " ZONE F=POINT, I=%12d , J=%12d\n", o.nx, o.nz);
+  const double rg = rhograd(o);
+  for (int ks = 0; ks < o.nsubd; ++ks)
+    for (int kl = 0; kl < o.nzloc; ++kl) {
+      const int k = ks * o.nzloc + kl;
+      const double zz = o.zg[k];
+      for (int i = 0; i < o.nx; ++i) {
+        const size_t idx = (size_t)i + row * (size_t)o.ny + plane * (size_t)k;  // (i, ny+1, k)
+        const double u = flow(0, idx), w = flow(2, idx), tt = flow(3, idx);
+        std::fprintf(f, " ");
+        for (double v : {o.xg[i], zz, u, w, tt, tt + (1. + rg * zz)}) std::fprintf(f, "%25.16f   ", v);
+        std::fprintf(f, "\n");
+      }
+    }
+  std::fclose(f);
+}
+
 // main.f:653-1066, one step with istart=0; maxcalc's adaptive step when
 // imaxcalc = 1 (the reference hard-codes 1, main.f:47), dt fixed otherwise.
 void step(Orc& o) {
@@ -1457,6 +1502,11 @@ void step(Orc& o) {
   maxcalc(o);
   if (o.pp.imaxcalc == 1) adapt_dt(o);
   if (o.ivardt == 1) o.idtstep = o.idtstep + 1;  // main.f:660-662
+  if (o.dtanim > 0 && (o.t - o.tdump) >= o.dtanim) {  // solver.f:141-142
+    o.tdump = o.t;
+    o.ianimc = o.ianimc + 1;
+    anim_dump(o);
+  }
   convec(o);
   bool ldtadapt = (o.ivardt == 1) && (o.idtstep < 2);  // main.f:741
   if (istep < 2 && o.istart == 0) {
@@ -1982,6 +2032,14 @@ int orc_plotf(void* h, const char* path, int iform) {
   ok = (std::fclose(f) == 0) && ok;
   if (!ok) { g_err = std::string("write error on ") + path; return 1; }
   return 0;
+}
+
+void orc_set_animation(void* h, double dtanim, const char* dir) {
+  Orc& o = *(Orc*)h;
+  o.dtanim = dtanim > 0 ? dtanim : 0;
+  o.anim_dir = dir ? dir : "";
+  o.tdump = 0;
+  o.ianimc = 0;
 }
 
 void orc_step(void* h) { step(*(Orc*)h); }

@@ -18,7 +18,9 @@ under tests/golden/.  The GPU box never reads the reference tree.
                      its record of time-step changes (write(65,*) t, dt,
                      various.f:971): the run's parameters and wave frequency
                      (main.f:370), maxcalc's cflzmax at the start of every
-                     step (various.f:882) and the (t, dt) of every change
+                     step (various.f:882) and the (t, dt) of every change;
+                     the (counter, t) of every animation dump the run logged
+                     (solver.f:169-170)
 """
 import json
 import os
@@ -65,6 +67,8 @@ def main(ref):
         "omega": [float(l.split()[-1]) for l in log if "Wave Frequency omega" in l][0],
         "cflz": [float(l.split()[-1]) for l in log if "At max CFLZ dz=" in l],
         "changes": rows(os.path.join(ref, "dtchange.dat")),
+        "anim_dumps": [[int(l.split("vortanimout_")[1].split(".dat")[0]), float(l.split()[-1])]
+                       for l in log if "Dumping out animation" in l],
     }
     g["_source"] = "jmsegret/IWrepo mode1_bbl run artefacts; see make_golden.py"
     with open(os.path.join(here, "reference_runs.json"), "w") as f:

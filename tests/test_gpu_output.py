@@ -85,3 +85,38 @@ def test_mixed_precision_dump(tmp_path):
     for q in range(4):
         assert np.linalg.norm(fs[q] - fo[q]) <= 1e-6 * np.linalg.norm(fo[q]), q
     s.close()
+
+
+def test_animation_dumps_equal_oracle(tmp_path):
+    """convec's animation dumps (iw_set_animation, solver.f:136-222): the same
+    files at the same steps as the oracle's, the same header and layout,
+    values to 1e-12 of each column's scale (the rows the reference reads with
+    j = ny+1 included).  Requested graph replay stays eager while dumps are on."""
+    import iwrepo_b200 as iw
+    from oracle import Oracle
+    cfg = cf.Config(nx=32, ny=16, nzloc=9, nsubd=3, dt=2e-3).validate()
+    o, s = Oracle(cfg), iw.Solver(cfg)
+    (tmp_path / "o").mkdir()
+    (tmp_path / "s").mkdir()
+    for x, d in ((o, "o"), (s, "s")):
+        x.init_mode1(0.05, 1e-4, 9)
+        x.set_animation(3.5e-3, str(tmp_path / d))
+    o.step(9)
+    s.run(9, graph=True)
+    s.wait_fields()
+    names = sorted(p.name for p in (tmp_path / "o").iterdir())
+    assert names == sorted(p.name for p in (tmp_path / "s").iterdir())
+    assert names == ["vortanimout_%05d.dat" % n for n in (1, 2, 3, 4)]  # t = 2, 4, 6, 8 dt
+    for n in names:
+        lo = open(tmp_path / "o" / n).read().split("\n")
+        ls = open(tmp_path / "s" / n).read().split("\n")
+        assert lo[0] == ls[0] and len(lo) == len(ls) == cfg.nx * cfg.nz + 2
+        assert [len(x) for x in lo] == [len(x) for x in ls]
+        vo = np.array([[float(ln[1 + 28 * c: 26 + 28 * c]) for c in range(6)] for ln in lo[1:-1]])
+        vs = np.array([[float(ln[1 + 28 * c: 26 + 28 * c]) for c in range(6)] for ln in ls[1:-1]])
+        for c in range(6):
+            assert np.abs(vs[:, c] - vo[:, c]).max() <= 1e-12 * max(1e-300, np.abs(vo[:, c]).max()), (n, c)
+    a = s.state()
+    b = o.state()  # the steps themselves: the full-step FP64 bar
+    assert max(np.linalg.norm(a[q] - b[q]) / np.linalg.norm(b[q]) for q in range(4)) <= 1e-10
+    s.close()

@@ -276,3 +276,65 @@ def test_oracle_adaptive_schedule():
             assert st["ivardt"] == 0 and st["dt"] == dt
             assert list(s[2:9]) == [3.0, -3.0, 1.0, 3.0, -1.5, 1.0 / 3.0, 11.0 / 6.0]
     assert len(changes) >= 2 and changes[0] in (22, 23)
+
+
+def test_animation_dump_schedule_replays_recorded_run(golden):
+    """solver.f:141-142: a dump when t - Tdump >= dtanim at the start of
+    convec, Tdump = t.  Driven by the recorded run's time steps (the replay of
+    its dt changes), Tdump = 0 at the start and dtanim = 1 (the run's log does
+    not print dtanim; 1 is the value whose schedule this is), the rule gives
+    the run's 328 dumps with their counters and times, and no others."""
+    import oracle
+    run = golden["dt_run"]
+    om = wave_omega(run["xlen"], run["zlen"], run["brunt"])
+    t, dt, tdump, n, got = 0.0, run["dtin"], 0.0, 0, []
+    for cz in run["cflz"]:
+        r = oracle.dt_rule(0.0, cz, t, dt, om)
+        if r is not None:
+            dt = r[0]
+        if t - tdump >= 1.0:
+            tdump = t
+            n += 1
+            got.append((n, t))
+        t = t + dt
+    assert len(got) == len(run["anim_dumps"]) == 328
+    for (n1, t1), (n2, t2) in zip(got, run["anim_dumps"]):
+        assert n1 == n2 and abs(t1 - t2) <= 1e-13 * max(1.0, t2)
+
+
+def test_oracle_animation_dump_rows(tmp_path):
+    """vortanimout layout: the ZONE header, nx*nz lines of (1x,6(F25.16,3x)),
+    and the rows the reference reads with j = ny+1 (the next z-plane; past
+    the last plane v, temp and the spectral un of COMMON /flow/)."""
+    cfg = cf.Config(nx=16, ny=8, nzloc=9, nsubd=3, dt=2e-3).validate()
+    o = Oracle(cfg)
+    o.init_mode1(0.05, 1e-4, 3)
+    o.set_animation(2.5e-3, str(tmp_path))
+    o.step(1)  # t = 0: 0 - 0 >= dtanim is false
+    assert not list(tmp_path.iterdir())
+    o.step(1)  # t = dt: no
+    # what convec sees: maxcalc's round trip P, then the mean of w removed
+    pf = [o.horfft(o.horfft(o.state(0)[q].copy(), 1), -1) for q in range(4)]
+    pf[2][:, 0, 0:2] = 0.0
+    ph = [o.horfft(f, 1) for f in pf]
+    un = o.state(1)[0]
+    o.step(1)  # t = 2 dt >= dtanim: dump 1 of the state at the start of this step
+    files = sorted(p.name for p in tmp_path.iterdir())
+    assert files == ["vortanimout_00001.dat"]
+    lines = open(tmp_path / files[0]).read().split("\n")[:-1]
+    assert lines[0] == " ZONE F=POINT, I=%12d , J=%12d" % (cfg.nx, cfg.nz)
+    assert len(lines) == 1 + cfg.nx * cfg.nz
+    assert all(len(ln) == 1 + 6 * 28 for ln in lines[1:])
+    vals = np.array([[float(ln[1 + 28 * c: 26 + 28 * c]) for c in range(6)] for ln in lines[1:]])
+    vals = vals.reshape(cfg.nz, cfg.nx, 6)
+    z = o.tables()["z"]
+    rg = -cfg.rho0 * cfg.brunt ** 2 / cfg.grav
+    for k in range(cfg.nz):
+        if k + 1 < cfg.nz:
+            u, w, t = ph[0][k + 1, 0, :cfg.nx], ph[2][k + 1, 0, :cfg.nx], ph[3][k + 1, 0, :cfg.nx]
+        else:
+            u, w, t = ph[1][0, 0, :cfg.nx], ph[3][0, 0, :cfg.nx], un[0, 0, :cfg.nx]
+        # F25.16 rounds at 5e-17
+        assert np.allclose(vals[k, :, 1], z[k], rtol=0, atol=1e-16)
+        for col, ref in ((2, u), (3, w), (4, t), (5, t + 1 + rg * z[k])):
+            assert np.allclose(vals[k, :, col], ref, rtol=0, atol=1e-15 * max(1.0, np.abs(ref).max())), (k, col)
