@@ -208,6 +208,15 @@ int iw_write_fields(iw_handle *h, const char *path, int iform);
  * dtanim <= 0 turns the dumps off.  Steps with dumps are not replayed from
  * graphs. */
 int iw_set_animation(iw_handle *h, double dtanim, const char *dir);
+/* Replaces main.f:905-910 with filtering.f:1110-1221 (speclegencalc): with
+ * ncalclegspec > 0, every iw_step whose step number is a multiple of it
+ * writes dir/speclegen<c><t>.dat for c = u, v, w, T after t += dt and before
+ * the interface averaging: per subdomain and Legendre mode, the mean over x
+ * of |a_k| in the x row at y index nyh.  Written like iw_write_fields, by a
+ * host thread; iw_wait_fields waits for the last one.  IW_ERR_CONFIG for
+ * ny = 1, where the reference's y index nyh = 0 lies outside the field.
+ * ncalclegspec <= 0 turns the spectra off. */
+int iw_set_speclegen(iw_handle *h, int ncalclegspec, const char *dir);
 /* Waits for the last iw_write_fields to finish its file; returns its status
  * (IW_ERR_IO with the reason in iw_last_error() if the file failed). */
 int iw_wait_fields(iw_handle *h);

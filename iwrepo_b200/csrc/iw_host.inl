@@ -329,6 +329,13 @@ struct iw_handle {
   std::string anim_dir;
   void* anim_host = nullptr;
   size_t anim_bytes = 0;
+  // Legendre spectra (main.f:905-910, speclegencalc): every nlegspec steps
+  // (0 = off), |a_k| per (subdomain, x, k) on the device, staged to the host
+  int nlegspec = 0;
+  std::string leg_dir;
+  double* dlegspec = nullptr;
+  void* leg_host = nullptr;
+  size_t leg_bytes = 0;
   Tables tab;
   // device tables
   double *ddzinv = 0, *dpart = 0;  // diagnostics: dt-free CFL spacing per level, per-block partials
@@ -1045,6 +1052,8 @@ static void rotate_levels(FieldSet<T>& fs) {
 // precedes it in the main loop (main.f:657).
 template <typename T>
 static int anim_dump(iw_handle* h, FieldSet<T>& fs);
+template <typename T>
+static int legspec_dump(iw_handle* h, FieldSet<T>& fs);
 
 template <typename T>
 static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
@@ -1414,6 +1423,7 @@ static int full_step(iw_handle* h, FieldSet<T>& fs) {
   calcuvwt_impl<T>(h, fs, cpen);
   schedule_after_calcuvwt(h);
   h->t = h->t + h->p.dt;
+  if (h->nlegspec > 0 && h->istep % h->nlegspec == 0 && (r = legspec_dump<T>(h, fs))) return r;  // main.f:905-910
   if (h->p.navgintrfc > 0 && h->istep % h->p.navgintrfc == 0) {
     iface_avg<T>(h, fs, true);
     mark(h, 10);
@@ -1526,11 +1536,11 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
 // paddle forcing (time in the arguments), a filter not applied every step,
 // interface averaging less often than every step, per-phase profiling, an
 // adaptive step (its rule reads the CFL numbers back at every step), animation
-// dumps (their schedule depends on t).
+// dumps (their schedule depends on t), Legendre spectra.
 // ---------------------------------------------------------------------------
 static bool graph_ready(const iw_handle* h) {
   return h->istep >= 3 && !h->prof && !h->p.forcing && (h->p.ispecfilterexp != 1 || h->p.nspecfilterexp == 1) &&
-         h->p.navgintrfc <= 1 && h->p.imaxcalc != 1 && !(h->dtanim > 0);
+         h->p.navgintrfc <= 1 && h->p.imaxcalc != 1 && !(h->dtanim > 0) && h->nlegspec <= 0;
 }
 
 static int step_dispatch(iw_handle* h) { return h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64); }
@@ -1799,6 +1809,8 @@ int iw_destroy(iw_handle* h) {
   out_join(h);
   if (h->out_host) cudaFreeHost(h->out_host);
   if (h->anim_host) cudaFreeHost(h->anim_host);
+  if (h->leg_host) cudaFreeHost(h->leg_host);
+  cudaFree(h->dlegspec);
   if (h->out_ev) cudaEventDestroy(h->out_ev);
   free_fields(h->f64);
   free_fields(h->f32);

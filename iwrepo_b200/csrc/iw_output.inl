@@ -276,7 +276,172 @@ static int anim_dump(iw_handle* h, FieldSet<T>& fs) {
   return IW_OK;
 }
 
+// Legendre spectra, filtering.f:1110-1221 (speclegencalc) every ncalclegspec
+// steps after t += dt, before the interface averaging (main.f:905-910), for
+// u, v, w and T: in the x row of physical space at y index nyh (1-based),
+// per subdomain, the mean over x of |a_k|, a_k = (k + 1/2) sum_j wg_j f_j
+// P_k(z_j) (k < N-1) and (N-1)/2 sum_j ... for the top mode.  File
+// speclegen<c><t>.dat, t in F5.3 (F6.3, F7.3, F8.3 from nint(t) = 10, 100,
+// 1000), lines (1x,I2,2x,10(e12.6,2x)) with one line per kloc (more than 10
+// subdomains continue on the next line, by format reversion).
+template <typename T>
+__global__ void k_speclegen(Geo g, const T* __restrict__ f, int jrow, const double* __restrict__ wg,
+                            const double* __restrict__ alpol, double* __restrict__ out) {
+  const int ks = blockIdx.y, N = g.N;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nx) return;
+  double faux[64];
+  for (int kl = 0; kl < N; ++kl) faux[kl] = (double)f[(size_t)(ks * N + kl) * g.plane + (size_t)jrow * g.nxpp + i];
+  const int nzm = N - 1;
+  for (int k = 0; k <= nzm; ++k) {
+    double sum = 0.;
+    for (int k1 = 0; k1 < N; ++k1) sum = sum + wg[k1] * faux[k1] * alpol[(size_t)k * N + k1];
+    const double a = k == nzm ? 0.5 * nzm * sum : (k + 0.5) * sum;
+    out[((size_t)ks * g.nx + i) * N + k] = fabs(a);
+  }
+}
+
+namespace fout {
+
+// Fortran Fw.d (asterisks when the value does not fit)
+static std::string f_wd(double v, int w, int d) {
+  char b[64];
+  snprintf(b, sizeof b, "%.*f", d, v);
+  const std::string s(b);
+  if ((int)s.size() > w) return std::string(w, '*');
+  return std::string(w - s.size(), ' ') + s;
+}
+
+// Fortran Ew.6 for w = 12: 0.dddddd E+ee fills all 12 columns
+static std::string e12_6(double v) {
+  std::string s;
+  e14_6(s, v);
+  const size_t lead = s.find_first_not_of(' ');
+  std::string body = s.substr(lead);
+  if (body.size() > 12 && body.compare(0, 3, "-0.") == 0) body = "-" + body.substr(2);  // optional zero dropped
+  if (body.size() > 12) return std::string(12, '*');
+  return std::string(12 - body.size(), ' ') + body;
+}
+
+static std::string speclegen_name(char c, double t) {
+  const long n = std::lround(t);
+  const int w = n >= 1000 ? 8 : n >= 100 ? 7 : n >= 10 ? 6 : 5;
+  return std::string("speclegen") + c + f_wd(t, w, 3) + ".dat";
+}
+
+struct LegJob {
+  std::string dir;
+  int dev = 0, nx = 0, ns = 0, N = 0;
+  double t = 0;
+  const double* host = nullptr;  // [4][ns][nx][N] |a_k|
+  cudaEvent_t ev = nullptr;
+};
+
+static bool write_leg(const LegJob& j, std::string* msg) {
+  const char names[4] = {'u', 'v', 'w', 'T'};
+  const size_t per = (size_t)j.ns * j.nx * j.N;
+  for (int q = 0; q < 4; ++q) {
+    std::vector<double> spec((size_t)j.ns * j.N, 0.0);  // specout(ks, kloc)
+    for (int ks = 0; ks < j.ns; ++ks) {
+      for (int i = 0; i < j.nx; ++i)
+        for (int k = 0; k < j.N; ++k) spec[(size_t)ks * j.N + k] += j.host[q * per + ((size_t)ks * j.nx + i) * j.N + k];
+      for (int k = 0; k < j.N; ++k) spec[(size_t)ks * j.N + k] = spec[(size_t)ks * j.N + k] / j.nx;
+    }
+    const std::string name = speclegen_name(names[q], j.t);
+    const std::string path = j.dir.empty() ? name : j.dir + "/" + name;
+    FILE* f = fopen(path.c_str(), "w");
+    if (!f) {
+      *msg = "cannot open " + path + " for writing";
+      return false;
+    }
+    std::string s;
+    char c[16];
+    for (int k = 0; k < j.N; ++k) {
+      snprintf(c, sizeof c, " %2d  ", k + 1);
+      s += c;
+      for (int ks = 0; ks < j.ns; ++ks) {
+        if (ks > 0) s += (ks % 10 == 0) ? "\n" : "  ";
+        s += e12_6(spec[(size_t)ks * j.N + k]);
+      }
+      s += '\n';
+    }
+    const bool ok = fwrite(s.data(), 1, s.size(), f) == s.size();
+    if (fclose(f) != 0 || !ok) {
+      *msg = "write error on " + path;
+      return false;
+    }
+  }
+  return true;
+}
+
+}  // namespace fout
+
+template <typename T>
+static int legspec_dump(iw_handle* h, FieldSet<T>& fs) {
+  if (out_join(h) != IW_OK) {
+    h->out_status = IW_OK;
+    return set_err(IW_ERR_IO, "the previous dump failed: " + h->out_msg);
+  }
+  const size_t per = (size_t)h->ns * h->nx * h->N;
+  if (!h->dlegspec) {
+    const cudaError_t e = cudaMalloc(&h->dlegspec, 4 * per * sizeof(double));
+    if (e != cudaSuccess) return set_err(IW_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  if (h->leg_bytes < 4 * per * sizeof(double)) {
+    if (h->leg_host) cudaFreeHost(h->leg_host);
+    h->leg_host = nullptr;
+    h->leg_bytes = 0;
+    CK(cudaMallocHost(&h->leg_host, 4 * per * sizeof(double)));
+    h->leg_bytes = 4 * per * sizeof(double);
+  }
+  if (!h->out_ev) CK(cudaEventCreateWithFlags(&h->out_ev, cudaEventDisableTiming));
+  const int jrow = h->nyh - 1;  // j = nyh (filtering.f:1156); ny >= 2 here
+  for (int q = 0; q < 4; ++q) {
+    phys_of<T>(h, fs, fs.F[q], fs.Y12[0], fs.Y12[1], 0);
+    k_speclegen<T><<<dim3((unsigned)((h->nx + 127) / 128), (unsigned)h->ns), 128, 0, h->st>>>(
+        geo(h), fs.Y12[0], jrow, h->dwg, h->dal, h->dlegspec + q * per);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->leg_host, h->dlegspec, 4 * per * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaEventRecord(h->out_ev, h->st));
+  fout::LegJob j;
+  j.dir = h->leg_dir;
+  j.dev = h->dev;
+  j.nx = h->nx;
+  j.ns = h->ns;
+  j.N = h->N;
+  j.t = h->t;
+  j.host = (const double*)h->leg_host;
+  j.ev = h->out_ev;
+  h->out_status = IW_OK;
+  h->out_msg.clear();
+  h->out_thread = new std::thread([h, j]() {
+    cudaSetDevice(j.dev);
+    if (cudaEventSynchronize(j.ev) != cudaSuccess) {
+      h->out_msg = "the copies of the Legendre spectra failed";
+      h->out_status = IW_ERR_CUDA;
+      return;
+    }
+    std::string msg;
+    if (!fout::write_leg(j, &msg)) {
+      h->out_msg = msg;
+      h->out_status = IW_ERR_IO;
+    }
+  });
+  return IW_OK;
+}
+
 extern "C" {
+
+int iw_set_speclegen(iw_handle* h, int ncalclegspec, const char* dir) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  if (ncalclegspec > 0 && h->ny < 2)
+    return set_err(IW_ERR_CONFIG, "Legendre spectra need ny >= 2: the reference reads y index nyh = 0, outside the "
+                                  "field, when ny = 1");
+  h->nlegspec = ncalclegspec > 0 ? ncalclegspec : 0;
+  h->leg_dir = dir ? dir : "";
+  return IW_OK;
+}
 
 int iw_set_animation(iw_handle* h, double dtanim, const char* dir) {
   if (!h) return set_err(IW_ERR_STATE, "null handle");

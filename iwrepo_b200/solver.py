@@ -114,6 +114,11 @@ class Solver:
     def wait_fields(self):
         _lib.check(_lib.lib().iw_wait_fields(self.h))
 
+    def set_speclegen(self, ncalclegspec: int, directory: str = ""):
+        """speclegencalc's Legendre spectra of u, v, w, T every ncalclegspec
+        steps (speclegen<c><t>.dat in directory); <= 0 turns them off."""
+        _lib.check(_lib.lib().iw_set_speclegen(self.h, ncalclegspec, str(directory).encode()))
+
     def set_animation(self, dtanim: float, directory: str = ""):
         """convec's animation dumps (vortanimout_NNNNN.dat in directory) every
         dtanim of simulated time; dtanim <= 0 turns them off."""

@@ -74,6 +74,7 @@ def lib():
         L.orc_plotf.restype = C.c_int
         L.orc_format_e14_6.argtypes = [D, C.c_char_p]
         L.orc_set_animation.argtypes = [C.c_void_p, D, C.c_char_p]
+        L.orc_set_speclegen.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
         L.orc_write_restart.restype = C.c_int
         L.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, D]
         L.orc_read_restart.restype = C.c_int
@@ -139,6 +140,10 @@ class Oracle:
         """output.f's restart dump (see orc_write_restart)."""
         if lib().orc_write_restart(self.h, str(path).encode()):
             raise RuntimeError(lib().orc_last_error().decode())
+
+    def set_speclegen(self, n: int, directory: str = ""):
+        """speclegencalc every n steps (see speclegen)."""
+        lib().orc_set_speclegen(self.h, n, str(directory).encode())
 
     def set_animation(self, dtanim: float, directory: str = ""):
         """convec's animation dumps (see anim_dump) every dtanim."""

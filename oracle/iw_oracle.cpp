@@ -123,6 +123,8 @@ struct Orc {
   double dtanim = 0, tdump = 0;
   int ianimc = 0;
   std::string anim_dir;
+  int nlegspec = 0;  // ncalclegspec (0 = off)
+  std::string leg_dir;
   // penalty COMMON (comparampen.h) used by the single-call C API
   struct Pen* pen0 = nullptr;
   // filter tables
@@ -1494,6 +1496,59 @@ void anim_dump(Orc& o) {
   std::fclose(f);
 }
 
+// Fortran E12.6 for the non-negative values of the spectra: 0.dddddd E+ee
+static std::string e12_6_nonneg(double v) {
+  if (v == 0.0) return "0.000000E+00";
+  char m[40], out[40];
+  std::snprintf(m, sizeof m, "%.5e", v);  // d.ddddde+XX: 6 significant digits
+  const int e = std::atoi(m + 8) + 1;
+  if (std::abs(e) <= 99) std::snprintf(out, sizeof out, "0.%c%.5sE%c%02d", m[0], m + 2, e < 0 ? '-' : '+', std::abs(e));
+  else std::snprintf(out, sizeof out, "0.%c%.5s%c%03d", m[0], m + 2, e < 0 ? '-' : '+', std::abs(e));
+  return out;
+}
+
+// filtering.f:1110-1221 (speclegencalc) on a copy of one field: physical
+// space, the x row at y index nyh (1-based), per subdomain the mean over x of
+// |a_k|, then the file speclegen<c><t>.dat, FORMAT (1x,I2,2x,10(e12.6,2x)).
+void speclegen(Orc& o, char c, const std::vector<double>& field) {
+  std::vector<double> fin = field;
+  horfft(o, fin.data(), 1, o.nz);
+  const int N = o.nzloc, nzm = N - 1, j = o.nyh - 1;
+  std::vector<double> specout((size_t)o.nsubd * N, 0.0), faux(N), a(N);
+  for (int ks = 0; ks < o.nsubd; ++ks) {
+    for (int i = 0; i < o.nx; ++i) {
+      for (int kloc = 0; kloc < N; ++kloc) faux[kloc] = fin[o.idx(i, j, ks * N + kloc)];
+      for (int k = 0; k <= nzm; ++k) {
+        double sum = 0.;
+        for (int k1 = 0; k1 < N; ++k1) sum = sum + o.wg[k1] * faux[k1] * o.alpol[(size_t)k * N + k1];
+        a[k] = (k == nzm) ? 0.5 * nzm * sum : (k + 0.5) * sum;
+      }
+      for (int kloc = 0; kloc < N; ++kloc) specout[(size_t)ks * N + kloc] = specout[(size_t)ks * N + kloc] + std::fabs(a[kloc]);
+    }
+    for (int kloc = 0; kloc < N; ++kloc) specout[(size_t)ks * N + kloc] = specout[(size_t)ks * N + kloc] / o.nx;
+  }
+  // file name: 'speclegen' // c // t in F5.3 (F6.3 .. F8.3 by nint(t)) // '.dat'
+  const long nt = std::lround(o.t);
+  const int w = nt >= 1000 ? 8 : nt >= 100 ? 7 : nt >= 10 ? 6 : 5;
+  char tb[64];
+  std::snprintf(tb, sizeof tb, "%.3f", o.t);
+  std::string ts(tb);
+  ts = (int)ts.size() > w ? std::string(w, '*') : std::string(w - ts.size(), ' ') + ts;
+  const std::string name = std::string("speclegen") + c + ts + ".dat";
+  const std::string path = o.leg_dir.empty() ? name : o.leg_dir + "/" + name;
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return;
+  for (int kloc = 0; kloc < N; ++kloc) {
+    std::fprintf(f, " %2d  ", kloc + 1);
+    for (int ks = 0; ks < o.nsubd; ++ks) {
+      if (ks > 0) std::fputs(ks % 10 == 0 ? "\n" : "  ", f);  // format reversion after 10 values
+      std::fprintf(f, "%12s", e12_6_nonneg(specout[(size_t)ks * N + kloc]).c_str());
+    }
+    std::fputs("\n", f);
+  }
+  std::fclose(f);
+}
+
 // main.f:653-1066, one step with istart=0; maxcalc's adaptive step when
 // imaxcalc = 1 (the reference hard-codes 1, main.f:47), dt fixed otherwise.
 void step(Orc& o) {
@@ -1552,6 +1607,12 @@ void step(Orc& o) {
     o.ivardt = 0;
   }
   o.t = o.t + o.dt;
+  if (o.nlegspec > 0 && istep % o.nlegspec == 0) {  // main.f:905-910
+    speclegen(o, 'u', o.F[0]);
+    speclegen(o, 'v', o.F[1]);
+    speclegen(o, 'w', o.F[2]);
+    speclegen(o, 'T', o.F[3]);
+  }
   if (o.pp.navgintrfc > 0 && istep % o.pp.navgintrfc == 0)
     for (int q = 0; q < 4; ++q) o.avg_count[q] = interface_avg3d(o, o.F[q].data());
 }
@@ -2032,6 +2093,12 @@ int orc_plotf(void* h, const char* path, int iform) {
   ok = (std::fclose(f) == 0) && ok;
   if (!ok) { g_err = std::string("write error on ") + path; return 1; }
   return 0;
+}
+
+void orc_set_speclegen(void* h, int n, const char* dir) {
+  Orc& o = *(Orc*)h;
+  o.nlegspec = n > 0 ? n : 0;
+  o.leg_dir = dir ? dir : "";
 }
 
 void orc_set_animation(void* h, double dtanim, const char* dir) {

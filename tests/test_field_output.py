@@ -104,3 +104,67 @@ def test_fortran_e_format_cases(tmp_path):
              0.1: "  0.100000E+00", 9.9999949e-3: "  0.999999E-02", 9.9999994e-3: "  0.100000E-01"}
     for v, want in cases.items():
         assert f(v) == want, (v, f(v))
+
+
+def legendre_spectra(o, cfg, field):
+    """speclegencalc (filtering.f:1110-1221) in numpy from the oracle's tables:
+    x row at y index nyh (1-based), mean over x of |a_k| per subdomain."""
+    tb = o.tables()
+    N, ns = cfg.nzloc, cfg.nsubd
+    ph = o.horfft(field.copy(), 1)
+    row = ph[:, cfg.ny // 2 - 1, :cfg.nx]                  # (nz, nx)
+    out = np.zeros((ns, N))
+    for ks in range(ns):
+        col = row[ks * N:(ks + 1) * N, :]                  # (N, nx)
+        s = (tb["alpol"] * tb["wg"][None, :]) @ col        # s[k, i] = sum_j wg_j P_k(z_j) f_j
+        fac = np.array([k + 0.5 for k in range(N - 1)] + [0.5 * (N - 1)])
+        out[ks] = np.abs(fac[:, None] * s).mean(axis=1)
+    return out
+
+
+def parse_speclegen(path, ns):
+    rows = {}
+    cur = None
+    for ln in open(path).read().split("\n")[:-1]:
+        if ln.startswith(" ") and ln[1:3].strip().isdigit() and ln[3:5] == "  ":
+            cur = int(ln[1:3])
+            rows[cur] = []
+            body = ln[5:]
+        else:
+            body = ln
+        rows[cur] += [float(body[c:c + 12]) for c in range(0, len(body), 14)]
+    return np.array([rows[k] for k in sorted(rows)]).T        # (ns, N)
+
+
+def test_oracle_legendre_spectra(tmp_path):
+    cfg = cf.Config(nx=16, ny=8, nzloc=9, nsubd=3, dt=2e-3, navgintrfc=0).validate()
+    o = Oracle(cfg)
+    o.init_mode1(0.05, 1e-4, 3)
+    o.set_speclegen(2, str(tmp_path))
+    o.step(2)
+    names = sorted(p.name for p in tmp_path.iterdir())
+    assert names == sorted("speclegen%s0.004.dat" % c for c in "uvwT")
+    for q, c in enumerate("uvwT"):
+        got = parse_speclegen(tmp_path / ("speclegen%s0.004.dat" % c), cfg.nsubd)
+        ref = legendre_spectra(o, cfg, o.state(0)[q])
+        # 6 printed digits; the round-off-level top modes differ by summation order
+        assert np.all(np.abs(got - ref) <= 5.0001e-6 * np.abs(ref) + 1e-13 * np.abs(ref).max()), c
+        lines = open(tmp_path / ("speclegen%s0.004.dat" % c)).read().split("\n")[:-1]
+        assert len(lines) == cfg.nzloc and all(len(ln) == 5 + 12 * 3 + 2 * 2 for ln in lines)
+
+
+def test_oracle_legendre_spectra_format_reversion_and_names(tmp_path):
+    """12 subdomains: 10 values on a kloc's line, the other 2 on the next
+    (reversion to 10(e12.6,2x)); t = 10.4 -> F6.3 in the name."""
+    cfg = cf.Config(nx=8, ny=4, nzloc=5, nsubd=12, dt=5.2, navgintrfc=0, xnu=1.0, xkappa=1.0).validate()
+    o = Oracle(cfg)
+    o.init_mode1(1e-3, 0.0, 1)
+    o.set_speclegen(2, str(tmp_path))
+    o.step(2)
+    p = tmp_path / "speclegenu10.400.dat"
+    assert p.exists()
+    lines = open(p).read().split("\n")[:-1]
+    assert len(lines) == 2 * cfg.nzloc
+    assert all(len(lines[2 * k]) == 5 + 12 * 10 + 2 * 9 and len(lines[2 * k + 1]) == 12 * 2 + 2 for k in range(cfg.nzloc))
+    got = parse_speclegen(p, cfg.nsubd)
+    assert got.shape == (cfg.nsubd, cfg.nzloc)

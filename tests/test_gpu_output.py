@@ -120,3 +120,34 @@ def test_animation_dumps_equal_oracle(tmp_path):
     b = o.state()  # the steps themselves: the full-step FP64 bar
     assert max(np.linalg.norm(a[q] - b[q]) / np.linalg.norm(b[q]) for q in range(4)) <= 1e-10
     s.close()
+
+
+def test_legendre_spectra_equal_oracle(tmp_path):
+    """speclegencalc every 3 steps (iw_set_speclegen): the same files as the
+    oracle's, values equal up to the 6th digit (and a round-off floor for the
+    top modes); ny = 1 is refused."""
+    import iwrepo_b200 as iw
+    from oracle import Oracle
+    from test_field_output import parse_speclegen
+    cfg = cf.Config(nx=32, ny=16, nzloc=9, nsubd=3, dt=2e-3).validate()
+    o, s = Oracle(cfg), iw.Solver(cfg)
+    (tmp_path / "o").mkdir()
+    (tmp_path / "s").mkdir()
+    for x, d in ((o, "o"), (s, "s")):
+        x.init_mode1(0.05, 1e-4, 2)
+        x.set_speclegen(3, str(tmp_path / d))
+    o.step(7)
+    s.run(7, graph=True)
+    s.wait_fields()
+    names = sorted(p.name for p in (tmp_path / "o").iterdir())
+    assert names == sorted(p.name for p in (tmp_path / "s").iterdir())
+    assert names == sorted("speclegen%s%s.dat" % (c, t) for c in "uvwT" for t in ("0.006", "0.012"))
+    for n in names:
+        a, b = parse_speclegen(tmp_path / "s" / n, cfg.nsubd), parse_speclegen(tmp_path / "o" / n, cfg.nsubd)
+        assert np.all(np.abs(a - b) <= 1.0001e-5 * np.abs(b) + 1e-12 * np.abs(b).max()), n
+    flat = cf.Config(nx=32, ny=1, nzloc=9, nsubd=3, dt=2e-3).validate()
+    f = iw.Solver(flat)
+    with pytest.raises(iw.IwError, match="ny >= 2"):
+        f.set_speclegen(3, str(tmp_path))
+    for x in (s, f):
+        x.close()
