@@ -217,6 +217,24 @@ int iw_set_animation(iw_handle *h, double dtanim, const char *dir);
  * ny = 1, where the reference's y index nyh = 0 lies outside the field.
  * ncalclegspec <= 0 turns the spectra off. */
 int iw_set_speclegen(iw_handle *h, int ncalclegspec, const char *dir);
+
+/* Replaces postp.f:9-70 with energycalc_postp (postp.f:415-732) and its
+ * helpers (umeancalc, dudzmeancalc, dudymeancalc, perturbcalc): the TKE
+ * budget of the current state.  e18 receives the values of one energy.dat
+ * line, in its order: t - tstart, (t - tstart) brunt, tketot, u1tke, u2tke,
+ * u3tke, prody, prodz, prod, bflux, epsilon, epssgs, epstot, chi, chisgs,
+ * chitot, tkemean, tempvar; w18 those of energy_wake.dat.  u' is u minus its
+ * x mean (0 at the bottom level); sums run over levels 2..nz; bflux carries
+ * the reference's factor ra pr with ra = 0; the subgrid terms are 0 (no
+ * subgrid model); the wake values are 0 but tkemean (the wake radii are
+ * never set).  Either pointer may be NULL. */
+int iw_postp(iw_handle *h, double *e18, double *w18);
+/* main.f:935-936: with npostp > 0, every iw_step whose step number is a
+ * multiple of npostp (after the interface averaging) appends one line to
+ * dir/energy.dat, dir/energy_wake.dat and dir/wakescale.dat in the
+ * reference's formats (headers written by the first line).  tstart is the
+ * &mflags value the times are counted from.  npostp <= 0 turns it off. */
+int iw_set_postp(iw_handle *h, int npostp, double tstart, const char *dir);
 /* Waits for the last iw_write_fields to finish its file; returns its status
  * (IW_ERR_IO with the reason in iw_last_error() if the file failed). */
 int iw_wait_fields(iw_handle *h);

@@ -23,7 +23,7 @@ PI = C.POINTER(C.c_int)
 # every entry point declared in include/iw_b200.h
 EXPORTS = [
     "iw_init", "iw_destroy", "iw_last_error", "iw_upload_state", "iw_download_state", "iw_init_mode1",
-    "iw_write_restart", "iw_read_restart", "iw_write_fields", "iw_wait_fields", "iw_set_animation", "iw_set_speclegen", "iw_step", "iw_run", "iw_ensemble_run", "iw_autotune", "iw_step_coefs", "iw_diag", "iw_sync", "iw_field_ptr", "iw_stream",
+    "iw_write_restart", "iw_read_restart", "iw_write_fields", "iw_wait_fields", "iw_set_animation", "iw_set_speclegen", "iw_postp", "iw_set_postp", "iw_step", "iw_run", "iw_ensemble_run", "iw_autotune", "iw_step_coefs", "iw_diag", "iw_sync", "iw_field_ptr", "iw_stream",
     "iw_device_bytes", "iw_helm_solve_batched", "iw_bind", "iw_profile", "iw_profile_read", "iw_mean_profiles",
     "horfft_", "dpdz_", "filter_3dlegenfourier_", "filter_legenpen_", "interface_avg3d_",
     "penalty_main_", "bandlu_solve_", "iw_bandlu_solve_noalloc", "penalty_setup_", "convec_", "calcuvwt_",
@@ -101,6 +101,8 @@ def lib():
     L.iw_wait_fields.argtypes = [vp]
     L.iw_set_animation.argtypes = [vp, C.c_double, C.c_char_p]
     L.iw_set_speclegen.argtypes = [vp, C.c_int, C.c_char_p]
+    L.iw_postp.argtypes = [vp, PD, PD]
+    L.iw_set_postp.argtypes = [vp, C.c_int, C.c_double, C.c_char_p]
     L.iw_read_restart.argtypes = [vp, C.c_char_p, C.c_int, C.c_double]
     L.iw_dt_rule.argtypes = [C.c_double] * 5 + [PD, PD]
     L.iw_dt_rule.restype = C.c_int

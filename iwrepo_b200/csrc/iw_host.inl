@@ -336,6 +336,12 @@ struct iw_handle {
   double* dlegspec = nullptr;
   void* leg_host = nullptr;
   size_t leg_bytes = 0;
+  // TKE budget (postp, main.f:935-936): every npostp steps (0 = off)
+  int npostp = 0;
+  double tstart = 0;
+  std::string postp_dir;
+  bool postp_started = false;  // headers written
+  double* dpostp = nullptr;    // per-(y, z) row sums
   Tables tab;
   // device tables
   double *ddzinv = 0, *dpart = 0;  // diagnostics: dt-free CFL spacing per level, per-block partials
@@ -1054,6 +1060,8 @@ template <typename T>
 static int anim_dump(iw_handle* h, FieldSet<T>& fs);
 template <typename T>
 static int legspec_dump(iw_handle* h, FieldSet<T>& fs);
+template <typename T>
+static int postp_step(iw_handle* h, FieldSet<T>& fs);
 
 template <typename T>
 static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
@@ -1428,6 +1436,7 @@ static int full_step(iw_handle* h, FieldSet<T>& fs) {
     iface_avg<T>(h, fs, true);
     mark(h, 10);
   }
+  if (h->npostp > 0 && h->istep % h->npostp == 0 && (r = postp_step<T>(h, fs))) return r;  // main.f:935-936
   prof_flush(h);
   CK(cudaGetLastError());
   return 0;
@@ -1536,11 +1545,11 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
 // paddle forcing (time in the arguments), a filter not applied every step,
 // interface averaging less often than every step, per-phase profiling, an
 // adaptive step (its rule reads the CFL numbers back at every step), animation
-// dumps (their schedule depends on t), Legendre spectra.
+// dumps (their schedule depends on t), Legendre spectra, the TKE budget.
 // ---------------------------------------------------------------------------
 static bool graph_ready(const iw_handle* h) {
   return h->istep >= 3 && !h->prof && !h->p.forcing && (h->p.ispecfilterexp != 1 || h->p.nspecfilterexp == 1) &&
-         h->p.navgintrfc <= 1 && h->p.imaxcalc != 1 && !(h->dtanim > 0) && h->nlegspec <= 0;
+         h->p.navgintrfc <= 1 && h->p.imaxcalc != 1 && !(h->dtanim > 0) && h->nlegspec <= 0 && h->npostp <= 0;
 }
 
 static int step_dispatch(iw_handle* h) { return h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64); }
@@ -1811,6 +1820,7 @@ int iw_destroy(iw_handle* h) {
   if (h->anim_host) cudaFreeHost(h->anim_host);
   if (h->leg_host) cudaFreeHost(h->leg_host);
   cudaFree(h->dlegspec);
+  cudaFree(h->dpostp);
   if (h->out_ev) cudaEventDestroy(h->out_ev);
   free_fields(h->f64);
   free_fields(h->f32);
@@ -2269,3 +2279,4 @@ static int helm_batched(iw_handle* h, const double* lam_dev, int ncol, int bot, 
 #include "iw_abi.inl"
 #include "iw_restart.inl"
 #include "iw_output.inl"
+#include "iw_postp.inl"

@@ -114,6 +114,18 @@ class Solver:
     def wait_fields(self):
         _lib.check(_lib.lib().iw_wait_fields(self.h))
 
+    def postp(self):
+        """postp's TKE budget of the current state (iw_postp): the values of one
+        energy.dat line and one energy_wake.dat line (18 each)."""
+        e, w = np.zeros(18), np.zeros(18)
+        _lib.check(_lib.lib().iw_postp(self.h, _pd(e), _pd(w)))
+        return e, w
+
+    def set_postp(self, npostp: int, tstart: float = 0.0, directory: str = ""):
+        """Append the budget lines to energy.dat, energy_wake.dat and
+        wakescale.dat in directory every npostp steps; <= 0 turns it off."""
+        _lib.check(_lib.lib().iw_set_postp(self.h, npostp, tstart, str(directory).encode()))
+
     def set_speclegen(self, ncalclegspec: int, directory: str = ""):
         """speclegencalc's Legendre spectra of u, v, w, T every ncalclegspec
         steps (speclegen<c><t>.dat in directory); <= 0 turns them off."""

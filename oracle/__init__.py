@@ -75,6 +75,7 @@ def lib():
         L.orc_format_e14_6.argtypes = [D, C.c_char_p]
         L.orc_set_animation.argtypes = [C.c_void_p, D, C.c_char_p]
         L.orc_set_speclegen.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+        L.orc_postp.argtypes = [C.c_void_p, PD, PD, D]
         L.orc_write_restart.restype = C.c_int
         L.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, D]
         L.orc_read_restart.restype = C.c_int
@@ -140,6 +141,13 @@ class Oracle:
         """output.f's restart dump (see orc_write_restart)."""
         if lib().orc_write_restart(self.h, str(path).encode()):
             raise RuntimeError(lib().orc_last_error().decode())
+
+    def postp(self, tstart: float = 0.0):
+        """postp's TKE budget: the values of an energy.dat and an
+        energy_wake.dat line (18 each)."""
+        e, w = np.zeros(18), np.zeros(18)
+        lib().orc_postp(self.h, _p(e), _p(w), tstart)
+        return e, w
 
     def set_speclegen(self, n: int, directory: str = ""):
         """speclegencalc every n steps (see speclegen)."""

@@ -124,6 +124,7 @@ struct Orc {
   int ianimc = 0;
   std::string anim_dir;
   int nlegspec = 0;  // ncalclegspec (0 = off)
+  double tstart = 0;  // &mflags tstart (postp's time origin)
   std::string leg_dir;
   // penalty COMMON (comparampen.h) used by the single-call C API
   struct Pen* pen0 = nullptr;
@@ -1712,6 +1713,109 @@ void diag_energy(Orc& o, double* out) {
   out[2] = wcnt ? std::sqrt(wsum / wcnt) : 0.0;
 }
 
+// postp.f:9-70 (postp) on copies of the state, with umeancalc
+// (postp.f:129-213), dpdzyzplane (postp.f:984-1020), dudymeancalc
+// (postp.f:237-298), perturbcalc (postp.f:300-330) and energycalc_postp
+// (postp.f:415-732).  e18: one energy.dat line; w18: one energy_wake.dat line
+// (the wake radii are never set, wakelengthcalc being commented out at
+// postp.f:36-38, so no point is inside the wake and only tkemean is nonzero).
+void postp(Orc& o, double* e18, double* w18) {
+  const int nx = o.nx, ny = o.ny, nz = o.nz, N = o.nzloc;
+  std::vector<double> u = o.F[0], v = o.F[1], w = o.F[2], tp = o.F[3];
+  for (auto* f : {&u, &v, &w, &tp}) horfft(o, f->data(), 1, nz);
+  // umeancalc: x means for k = 2..nz
+  std::vector<double> umean((size_t)ny * nz, 0.0), dumeandz((size_t)ny * nz, 0.0), dumeandy((size_t)ny * nz, 0.0);
+  for (int k = 1; k < nz; ++k)
+    for (int j = 0; j < ny; ++j) {
+      double s = 0.;
+      for (int i = 0; i < nx; ++i) s = s + u[o.idx(i, j, k)];
+      umean[(size_t)j * nz + k] = s / nx;
+    }
+  // dudzmeancalc: dpdzcol per y and subdomain
+  for (int j = 0; j < ny; ++j)
+    for (int ks = 0; ks < o.nsubd; ++ks) {
+      double a[IW_MAX_NZLOC], b[IW_MAX_NZLOC];
+      for (int kl = 0; kl < N; ++kl) a[kl] = umean[(size_t)j * nz + ks * N + kl];
+      dpdzcol(o, a, b, o.pp.zh[ks]);
+      for (int kl = 0; kl < N; ++kl) dumeandz[(size_t)j * nz + ks * N + kl] = b[kl];
+    }
+  // dudymeancalc: real Fourier series in y times i ky; the imaginary Nyquist
+  // coefficient is dropped by the real inverse transform
+  if (ny > 1) {
+    const double pi2 = 8.0 * std::atan(1.0);
+    std::vector<cd> zin(ny), zout(ny), spec(ny);
+    for (int k = 0; k < nz; ++k) {
+      for (int j = 0; j < ny; ++j) zin[j] = cd(umean[(size_t)j * nz + k], 0.0);
+      o.fy.run(zin.data(), zout.data(), false);
+      std::fill(spec.begin(), spec.end(), cd(0.0, 0.0));
+      for (int m = 1; m < ny / 2; ++m) {
+        const cd a = zout[m] / (double)ny * cd(0.0, m * (pi2 / o.pp.ylen));
+        spec[m] = a;
+        spec[ny - m] = std::conj(a);
+      }
+      o.fy.run(spec.data(), zout.data(), true);
+      for (int j = 0; j < ny; ++j) dumeandy[(size_t)j * nz + k] = zout[j].real();
+    }
+  }
+  // perturbcalc
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) u[o.idx(i, j, k)] = u[o.idx(i, j, k)] - umean[(size_t)j * nz + k];
+  // energycalc_postp: gradients in spectral space, back to physical space
+  for (auto* f : {&u, &v, &w, &tp}) horfft(o, f->data(), -1, nz);
+  std::vector<double>* fl[4] = {&u, &v, &w, &tp};
+  std::vector<double> g[12];
+  for (auto& x : g) x.assign(o.ntot, 0.0);
+  for (int q = 0; q < 4; ++q) {
+    const std::vector<double>& f = *fl[q];
+    dpdz(o, f.data(), g[3 * q + 2].data());
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int ii = 0; ii < o.nxhp; ++ii) {
+          const size_t pr = o.idx(2 * ii, j, k), pi = pr + 1;
+          g[3 * q][pr] = -(o.xw[ii] * f[pi]);
+          g[3 * q][pi] = o.xw[ii] * f[pr];
+          g[3 * q + 1][pr] = -(o.yw[j] * f[pi]);
+          g[3 * q + 1][pi] = o.yw[j] * f[pr];
+        }
+  }
+  for (auto* f : {&u, &v, &w, &tp}) horfft(o, f->data(), 1, nz);
+  for (auto& x : g) horfft(o, x.data(), 1, nz);
+  double tketot = 0, u1 = 0, u2 = 0, u3 = 0, prody = 0, prodz = 0, bflux = 0, tempvar = 0, eps = 0, chi = 0, tkemean = 0;
+  for (int k = 1; k < nz; ++k)
+    for (int j = 0; j < ny; ++j) {
+      for (int i = 0; i < nx; ++i) {
+        const size_t p = o.idx(i, j, k);
+        const double uu = u[p], vv = v[p], ww = w[p], tt = tp[p];
+        tketot = tketot + (uu * uu + vv * vv + ww * ww);
+        u1 = u1 + uu * uu;
+        u2 = u2 + vv * vv;
+        u3 = u3 + ww * ww;
+        prody = prody - dumeandy[(size_t)j * nz + k] * (uu * vv);
+        prodz = prodz - dumeandz[(size_t)j * nz + k] * (uu * ww);
+        bflux = bflux + ww * tt;
+        tempvar = tempvar + tt * tt;
+        for (int q = 0; q < 9; ++q) eps = eps + g[q][p] * g[q][p];
+        for (int q = 9; q < 12; ++q) chi = chi + g[q][p] * g[q][p];
+      }
+      tkemean = tkemean + umean[(size_t)j * nz + k] * umean[(size_t)j * nz + k];
+    }
+  const double ra = 0.0, pr = o.pp.xnu;  // ra: start-up value (main.f:577-580); pr = xnu (main.f:428)
+  tketot = tketot * 0.5;
+  tkemean = tkemean * 0.5 * nx;
+  bflux = bflux * ra * pr;
+  eps = eps * pr;
+  chi = chi * o.pp.xkappa;
+  const double tt = o.t - o.tstart;
+  const double e[18] = {tt,  tt * o.pp.brunt, tketot, u1, u2, u3, prody, prodz, prody + prodz, bflux, eps, 0.0,
+                        eps + 0.0, chi, 0.0, 0.0 + chi, tkemean, tempvar};
+  std::memcpy(e18, e, sizeof e);
+  for (int n = 0; n < 18; ++n) w18[n] = 0.0;
+  w18[0] = e[0];
+  w18[1] = e[1];
+  w18[16] = tkemean;
+}
+
 std::string g_err;
 
 }  // namespace
@@ -2093,6 +2197,12 @@ int orc_plotf(void* h, const char* path, int iform) {
   ok = (std::fclose(f) == 0) && ok;
   if (!ok) { g_err = std::string("write error on ") + path; return 1; }
   return 0;
+}
+
+void orc_postp(void* h, double* e18, double* w18, double tstart) {
+  Orc& o = *(Orc*)h;
+  o.tstart = tstart;
+  postp(o, e18, w18);
 }
 
 void orc_set_speclegen(void* h, int n, const char* dir) {
