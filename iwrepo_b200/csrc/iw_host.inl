@@ -961,7 +961,10 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   }
   dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
   size_t smem = (size_t)h->N * h->N * sizeof(double) + (size_t)(h->N * h->N + 2 * h->N * kTX) * sizeof(T);
-  k_stageE<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c);
+  if constexpr (sizeof(T) == 4)
+    k_stageE_f32<<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c);
+  else
+    k_stageE<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c);
 }
 
 // values per lane of a warp transform of length M

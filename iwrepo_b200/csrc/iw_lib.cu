@@ -498,7 +498,7 @@ struct EArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c) {
+__device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, const Coefs& c) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int N = g.N;
   double* sL = (double*)smraw;  // N*N, L - I in FP64 (see below)
@@ -566,6 +566,17 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c)
     }
     a.F[q][fidx<T>(g, i, j, ks * N + k1)] = o;
   }
+}
+
+// The tiled K_E kernels.  FP32 fields: at most 32 registers so that 8 CTAs
+// fit on an SM (the kernel waits on global loads, more resident warps pay);
+// FP64 fields: the compiler's own allocation.
+template <typename T>
+__global__ void __launch_bounds__(kTX* kTW) k_stageE(Geo g, EArgs<T> a, Coefs c) {
+  stageE_tile<T>(g, a, c);
+}
+__global__ void __launch_bounds__(kTX* kTW, 8) k_stageE_f32(Geo g, EArgs<float> a, Coefs c) {
+  stageE_tile<float>(g, a, c);
 }
 
 // ---------------------------------------------------------------------------
