@@ -182,9 +182,9 @@ int iw_write_restart(iw_handle *h, const char *path);
  * The handle's parameters stand: the reference also takes pr, ra and umax
  * from the file, which equal the namelist values when a run continues with
  * its own input.dat.  The output schedules (iw_set_animation,
- * iw_set_speclegen, iw_set_postp) are not in the file: set them again; the
- * animation counter and Tdump restart from 0, as after the reference's own
- * restart (restart.f does not read them). */
+ * iw_set_speclegen, iw_set_postp) are not in the file and stay as set on
+ * the handle; the animation counter and Tdump restart from 0, as after the
+ * reference's own restart (restart.f does not read them). */
 int iw_read_restart(iw_handle *h, const char *path, int mode, double cdtin);
 
 /* Replaces output.f:118-265 (plotf; main.f:543,607,1039): u, v, w and temp

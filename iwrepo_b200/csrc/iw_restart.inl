@@ -281,6 +281,8 @@ int iw_read_restart(iw_handle* h, const char* path, int mode, double cdtin) {
   }
   int r = iw_upload_state(h, nullptr, nullptr, nullptr, nullptr, nullptr, t, 0);
   if (r) return r;
+  h->tdump = 0;  // COMMON /Dump/ of a restarted run (restart.f does not read it)
+  h->ianimc = 0;
   if (mode == IW_RESTART_EXACT) {
     h->istep = ei[2];
     h->ivardt = ei[3];

@@ -119,3 +119,26 @@ def test_restart_of_other_dims_is_refused(tmp_path):
     assert np.array_equal(c.state(0), a.state(0)) and len(raw) > len(ref_only)
     for x in (a, b, c):
         x.close()
+
+
+def test_read_restart_restarts_the_animation_counter(tmp_path):
+    """Tdump and the dump counter are not in the file (restart.f does not read
+    them): after a read they start from 0, as in a restarted reference run."""
+    import iwrepo_b200 as iw
+    cfg = _cfg()
+    a = iw.Solver(cfg)
+    a.init_mode1(0.05, 1e-4, 4)
+    d = tmp_path / "anim"
+    d.mkdir()
+    a.set_animation(1.5 * cfg.dt, str(d))
+    a.step(5)  # dumps at t = 2 dt and 4 dt
+    a.wait_fields()
+    assert sorted(p.name for p in d.iterdir()) == ["vortanimout_00001.dat", "vortanimout_00002.dat"]
+    a.write_restart(tmp_path / "run.dat")
+    for p in list(d.iterdir()):
+        p.unlink()
+    a.read_restart(tmp_path / "run.dat", "reference")
+    a.step(1)  # t - Tdump = 5 dt - 0 >= dtanim: dump number 1 again
+    a.wait_fields()
+    assert sorted(p.name for p in d.iterdir()) == ["vortanimout_00001.dat"]
+    a.close()
