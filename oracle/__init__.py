@@ -76,6 +76,10 @@ def lib():
         L.orc_set_animation.argtypes = [C.c_void_p, D, C.c_char_p]
         L.orc_set_speclegen.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
         L.orc_postp.argtypes = [C.c_void_p, PD, PD, D]
+        L.orc_rhograd.argtypes = [C.c_void_p]
+        L.orc_rhograd.restype = D
+        L.orc_rhomean.argtypes = [C.c_void_p, D]
+        L.orc_rhomean.restype = D
         L.orc_write_restart.restype = C.c_int
         L.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, D]
         L.orc_read_restart.restype = C.c_int
@@ -148,6 +152,14 @@ class Oracle:
         e, w = np.zeros(18), np.zeros(18)
         lib().orc_postp(self.h, _p(e), _p(w), tstart)
         return e, w
+
+    def rhomean(self, z: float) -> float:
+        """forcing.f:134-141."""
+        return lib().orc_rhomean(self.h, z)
+
+    def rhograd(self) -> float:
+        """forcing.f:115-120."""
+        return lib().orc_rhograd(self.h)
 
     def set_speclegen(self, n: int, directory: str = ""):
         """speclegencalc every n steps (see speclegen)."""

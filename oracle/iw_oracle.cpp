@@ -2205,6 +2205,10 @@ void orc_postp(void* h, double* e18, double* w18, double tstart) {
   postp(o, e18, w18);
 }
 
+// forcing.f:115-141: rhograd and rhomean(z)
+double orc_rhograd(void* h) { return rhograd(*(Orc*)h); }
+double orc_rhomean(void* h, double z) { return rhomean(*(Orc*)h, z); }
+
 void orc_set_speclegen(void* h, int n, const char* dir) {
   Orc& o = *(Orc*)h;
   o.nlegspec = n > 0 ? n : 0;

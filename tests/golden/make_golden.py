@@ -14,6 +14,8 @@ under tests/golden/.  The GPU box never reads the reference tree.
                      shipped 2-D forced run (various.f:743-745)
 * minmaxtest.dat, cfl.dat, avgint.dat -- per-step traces of the same run
 * runfolder/subd.dat, subd.dat -- subdomain tables used above
+* rhomean.dat      -- setup.f:170-184 of the shipped run: z, rhomean(z),
+                     rhograd, (N(z)/N)^2, fshear(z) from the top level down
 * output, dtchange.dat -- the log of a recorded 400-step run (xlen = 40) and
                      its record of time-step changes (write(65,*) t, dt,
                      various.f:971): the run's parameters and wave frequency
@@ -53,6 +55,7 @@ def main(ref):
     g["avgint"] = rows(os.path.join(ref, "avgint.dat"), 1)
     g["subd_runfolder"] = rows(os.path.join(ref, "runfolder", "subd.dat"))
     g["subd_shipped"] = rows(os.path.join(ref, "subd.dat"))
+    g["rhomean"] = rows(os.path.join(ref, "rhomean.dat"), 1)
     log = open(os.path.join(ref, "output"), "rb").read().decode("latin1").splitlines()
 
     def logged(name):

@@ -338,3 +338,19 @@ def test_oracle_animation_dump_rows(tmp_path):
         assert np.allclose(vals[k, :, 1], z[k], rtol=0, atol=1e-16)
         for col, ref in ((2, u), (3, w), (4, t), (5, t + 1 + rg * z[k])):
             assert np.allclose(vals[k, :, col], ref, rtol=0, atol=1e-15 * max(1.0, np.abs(ref).max())), (k, col)
+
+
+def test_mean_density_profile_matches_rhomean_dat(golden):
+    """setup.f:170-184 of the shipped run wrote, from the top level down,
+    z, rhomean(z), rhograd and (N(z)/N)^2 (6 digits each; the fifth column,
+    fshear, enters the path only times fcshear = 0)."""
+    rows = np.array(golden["rhomean"])
+    o = Oracle(cf.shipped_2d())
+    z = o.tables()["z"]
+    assert rows.shape == (len(z), 5)
+    for r, k in enumerate(range(len(z) - 1, -1, -1)):
+        zz, rm, rg, n2 = rows[r, :4]
+        assert abs(zz - z[k]) <= 5e-6 * max(abs(z[k]), 1e-2) + 1e-7
+        assert abs(rm - o.rhomean(z[k])) <= 5e-6 * abs(o.rhomean(z[k]))
+        assert abs(rg - o.rhograd()) <= 5e-6 * abs(o.rhograd())
+        assert n2 == 1.0
