@@ -10,7 +10,8 @@
 //                      x-forward with i kx folded in                 (rows)
 //   K_D  k_yfft        y-forward with i ky folded in                 (planes)
 //   K_E  k_stageE(_r)  S = B + dz(Z), SS extrapolation, BDF u*, history,
-//                      Fourier x Legendre filter                     (z columns)
+//                      Fourier x Legendre filter (k_stageE_f32: the
+//                      tiled kernel for FP32 fields)                 (z columns)
 //        k_wviscrot    rotational viscous pressure BC                (walls)
 //   K_F  k_solve_cta   pressure Poisson (divergence, solve, filter, projection)
 //        k_solve_cta   u,v / w / rho Helmholtz solves, filters, mean mode
@@ -19,6 +20,10 @@
 //   K_H  interface averaging: planes next to interfaces go to physical space,
 //        the averaging change comes back; every plane gets the spectral effect
 //        of the round trip.
+// Around the step (iw_restart.inl, iw_output.inl, iw_postp.inl): the adaptive
+// time step's CFL numbers (k_phys_stats), restart files, field and animation
+// dumps, Legendre spectra (k_speclegen) and the TKE budget (k_row_dot,
+// k_sub_rowmean), written by a host thread from pinned buffers.
 // The penalty systems (penalty.f + band_lu.f) are assembled on the device
 // (k_factor) when epsilon changes (steps 1-3 and a dt change), one per distinct
 // kx^2+ky^2 and system type, then factored (band LU) or turned into block
