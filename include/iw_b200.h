@@ -206,7 +206,8 @@ int iw_write_fields(iw_handle *h, const char *path, int iform);
  * FORMAT (1x,6(F25.16,3x)), for every subdomain point and x index.  The rows
  * are those the reference reads: its y index is the value the preceding loop
  * leaves, ny+1, i.e. row 1 of the next z-plane, and past the last plane the
- * first rows of v, temp and un (COMMON /flow/ order).  Written like
+ * first rows of v, temp and un (COMMON /flow/ order).  Each dump also
+ * appends its line to dir/animdump.log (solver.f:212-215).  Written like
  * iw_write_fields, by a host thread; iw_wait_fields waits for the last one.
  * dtanim <= 0 turns the dumps off.  Steps with dumps are not replayed from
  * graphs. */

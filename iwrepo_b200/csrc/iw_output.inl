@@ -146,12 +146,33 @@ static int out_join(iw_handle* h) {
 // y loop variable that the loop of solver.f:82-100 leaves behind, j = ny+1:
 // u(i,ny+1,k) is u(i,1,k+1), and for k = nz the row after u, w and temp in
 // COMMON /flow/: v(i,1,1), temp(i,1,1) and un(i,1,1) (physical, physical,
-// and the spectral level n-1).  The same rows are written here.  The
-// animdump.log line of the reference is not written.
+// and the spectral level n-1).  The same rows are written here.  After each
+// file, one line is appended to animdump.log (solver.f:212-215, list-directed:
+// t in 15 significant digits of F form between 3 and 6 blanks, I12 integers,
+// a blank before a character item that follows a number).
 namespace fout {
 
+// t as ifort's list-directed output writes a REAL*8 of magnitude in [1, 1e15):
+// 15 significant digits in F form
+static std::string list_real15(double v) {
+  char e[40], f[64];
+  snprintf(e, sizeof e, "%.14e", v);  // 15 significant digits, correctly rounded
+  const int ex = atoi(strchr(e, 'e') + 1);
+  const int dec = ex >= 14 ? 0 : 14 - ex;
+  snprintf(f, sizeof f, "%.*f", dec, v);
+  return f;
+}
+
+static std::string animdump_line(double t, int n, int istep) {
+  char c[128];
+  snprintf(c, sizeof c, "      vortanimout_%12d .datat step=%12d\n", n, istep);
+  return " Animation data dumped out at time   " + list_real15(t) + c;
+}
+
 struct AnimJob {
-  std::string path;
+  std::string path, log;  // the dump file and animdump.log
+  double t = 0;
+  int n = 0, istep = 0;
   int dev = 0, nx = 0, nz = 0, nxpp = 0;
   bool fp32 = false;
   std::vector<double> x, z;
@@ -198,7 +219,19 @@ static bool write_anim(const AnimJob& j, std::string* msg) {
   }
   ok = ok && fwrite(s.data(), 1, s.size(), f) == s.size();
   ok = (fclose(f) == 0) && ok;
-  if (!ok) *msg = "write error on " + j.path;
+  if (!ok) {
+    *msg = "write error on " + j.path;
+    return false;
+  }
+  FILE* lf = fopen(j.log.c_str(), "a");  // open(67,file='animdump.log',access='append')
+  if (!lf) {
+    *msg = "cannot open " + j.log;
+    return false;
+  }
+  const std::string ln = animdump_line(j.t, j.n, j.istep);
+  ok = fwrite(ln.data(), 1, ln.size(), lf) == ln.size();
+  ok = (fclose(lf) == 0) && ok;
+  if (!ok) *msg = "write error on " + j.log;
   return ok;
 }
 
@@ -244,6 +277,10 @@ static int anim_dump(iw_handle* h, FieldSet<T>& fs) {
   char name[32];
   snprintf(name, sizeof name, "vortanimout_%05d.dat", h->ianimc);  // fmt (i5.5,a4), solver.f:159-167
   j.path = h->anim_dir.empty() ? std::string(name) : h->anim_dir + "/" + name;
+  j.log = h->anim_dir.empty() ? std::string("animdump.log") : h->anim_dir + "/animdump.log";
+  j.t = h->t;
+  j.n = h->ianimc;
+  j.istep = h->istep;
   j.dev = h->dev;
   j.nx = h->nx;
   j.nz = h->nz;

@@ -76,6 +76,7 @@ def lib():
         L.orc_set_animation.argtypes = [C.c_void_p, D, C.c_char_p]
         L.orc_set_speclegen.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
         L.orc_postp.argtypes = [C.c_void_p, PD, PD, D]
+        L.orc_animdump_line.argtypes = [D, C.c_int, C.c_int, C.c_char_p, C.c_int]
         L.orc_rhograd.argtypes = [C.c_void_p]
         L.orc_rhograd.restype = D
         L.orc_rhomean.argtypes = [C.c_void_p, D]
@@ -287,6 +288,13 @@ def format_e14_6(v: float) -> str:
     b = C.create_string_buffer(16)
     lib().orc_format_e14_6(v, b)
     return b.value.decode()
+
+
+def animdump_line(t: float, n: int, istep: int) -> str:
+    """The oracle's animdump.log line (without its newline)."""
+    b = C.create_string_buffer(256)
+    lib().orc_animdump_line(t, n, istep, b, 256)
+    return b.value.decode().rstrip("\n")
 
 
 def set_threads(n: int):

@@ -1460,6 +1460,17 @@ void adapt_dt(Orc& o) {
 // horfft +1 on copies.  The reference reads u(i,j,k) with j = ny+1, the value
 // the y loop of solver.f:82-100 leaves: u(i,1,k+1), and for k = nz the first
 // row of the array after it in COMMON /flow/ (u -> v, w -> temp, temp -> un).
+// the animdump.log line (solver.f:212-215): list-directed t (15 significant
+// digits, F form), I12 counters, a blank before a character item after a number
+std::string animdump_line(double t, int n, int istep) {
+  char e[40], num[64], tail[128];
+  std::snprintf(e, sizeof e, "%.14e", t);
+  const int ex = std::atoi(std::strchr(e, 'e') + 1);
+  std::snprintf(num, sizeof num, "%.*f", ex >= 14 ? 0 : 14 - ex, t);
+  std::snprintf(tail, sizeof tail, "      vortanimout_%12d .datat step=%12d\n", n, istep);
+  return std::string(" Animation data dumped out at time   ") + num + tail;
+}
+
 void anim_dump(Orc& o) {
   const size_t row = o.nxpp, plane = (size_t)o.nxpp * o.ny;
   std::vector<double> ph[4];
@@ -1495,6 +1506,11 @@ void anim_dump(Orc& o) {
       }
     }
   std::fclose(f);
+  FILE* lf = std::fopen((o.anim_dir.empty() ? std::string("animdump.log") : o.anim_dir + "/animdump.log").c_str(), "a");
+  if (lf) {
+    std::fputs(animdump_line(o.t, o.ianimc, o.istep).c_str(), lf);
+    std::fclose(lf);
+  }
 }
 
 // Fortran E12.6 for the non-negative values of the spectra: 0.dddddd E+ee
@@ -2203,6 +2219,10 @@ void orc_postp(void* h, double* e18, double* w18, double tstart) {
   Orc& o = *(Orc*)h;
   o.tstart = tstart;
   postp(o, e18, w18);
+}
+
+void orc_animdump_line(double t, int n, int istep, char* out, int cap) {
+  std::snprintf(out, cap, "%s", animdump_line(t, n, istep).c_str());
 }
 
 // forcing.f:115-141: rhograd and rhomean(z)

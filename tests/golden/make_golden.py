@@ -72,6 +72,8 @@ def main(ref):
         "changes": rows(os.path.join(ref, "dtchange.dat")),
         "anim_dumps": [[int(l.split("vortanimout_")[1].split(".dat")[0]), float(l.split()[-1])]
                        for l in log if "Dumping out animation" in l],
+        # the run's lines of animdump.log (the file holds other runs' lines before them)
+        "animdump_log": open(os.path.join(ref, "animdump.log")).read().split("\n")[32:360],
     }
     g["_source"] = "jmsegret/IWrepo mode1_bbl run artefacts; see make_golden.py"
     with open(os.path.join(here, "reference_runs.json"), "w") as f:

@@ -104,9 +104,11 @@ def test_animation_dumps_equal_oracle(tmp_path):
     o.step(9)
     s.run(9, graph=True)
     s.wait_fields()
-    names = sorted(p.name for p in (tmp_path / "o").iterdir())
-    assert names == sorted(p.name for p in (tmp_path / "s").iterdir())
+    names = sorted(p.name for p in (tmp_path / "o").iterdir() if p.name != "animdump.log")
+    assert names == sorted(p.name for p in (tmp_path / "s").iterdir() if p.name != "animdump.log")
     assert names == ["vortanimout_%05d.dat" % n for n in (1, 2, 3, 4)]  # t = 2, 4, 6, 8 dt
+    log = (tmp_path / "s" / "animdump.log").read_text()
+    assert log == (tmp_path / "o" / "animdump.log").read_text() and len(log.splitlines()) == 4
     for n in names:
         lo = open(tmp_path / "o" / n).read().split("\n")
         ls = open(tmp_path / "s" / n).read().split("\n")

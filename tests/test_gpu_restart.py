@@ -133,12 +133,12 @@ def test_read_restart_restarts_the_animation_counter(tmp_path):
     a.set_animation(1.5 * cfg.dt, str(d))
     a.step(5)  # dumps at t = 2 dt and 4 dt
     a.wait_fields()
-    assert sorted(p.name for p in d.iterdir()) == ["vortanimout_00001.dat", "vortanimout_00002.dat"]
+    assert sorted(p.name for p in d.iterdir()) == ["animdump.log", "vortanimout_00001.dat", "vortanimout_00002.dat"]
     a.write_restart(tmp_path / "run.dat")
     for p in list(d.iterdir()):
         p.unlink()
     a.read_restart(tmp_path / "run.dat", "reference")
     a.step(1)  # t - Tdump = 5 dt - 0 >= dtanim: dump number 1 again
     a.wait_fields()
-    assert sorted(p.name for p in d.iterdir()) == ["vortanimout_00001.dat"]
+    assert sorted(p.name for p in d.iterdir()) == ["animdump.log", "vortanimout_00001.dat"]
     a.close()

@@ -288,18 +288,20 @@ def test_animation_dump_schedule_replays_recorded_run(golden):
     run = golden["dt_run"]
     om = wave_omega(run["xlen"], run["zlen"], run["brunt"])
     t, dt, tdump, n, got = 0.0, run["dtin"], 0.0, 0, []
-    for cz in run["cflz"]:
+    for step, cz in enumerate(run["cflz"], 1):
         r = oracle.dt_rule(0.0, cz, t, dt, om)
         if r is not None:
             dt = r[0]
         if t - tdump >= 1.0:
             tdump = t
             n += 1
-            got.append((n, t))
+            got.append((n, t, step))
         t = t + dt
     assert len(got) == len(run["anim_dumps"]) == 328
-    for (n1, t1), (n2, t2) in zip(got, run["anim_dumps"]):
+    for (n1, t1, _), (n2, t2) in zip(got, run["anim_dumps"]):
         assert n1 == n2 and abs(t1 - t2) <= 1e-13 * max(1.0, t2)
+    # and the run's animdump.log lines (solver.f:212-215), character for character
+    assert [oracle.animdump_line(t1, n1, s1) for (n1, t1, s1) in got] == run["animdump_log"]
 
 
 def test_oracle_animation_dump_rows(tmp_path):
@@ -319,8 +321,10 @@ def test_oracle_animation_dump_rows(tmp_path):
     ph = [o.horfft(f, 1) for f in pf]
     un = o.state(1)[0]
     o.step(1)  # t = 2 dt >= dtanim: dump 1 of the state at the start of this step
-    files = sorted(p.name for p in tmp_path.iterdir())
+    files = sorted(p.name for p in tmp_path.iterdir() if p.name != "animdump.log")
     assert files == ["vortanimout_00001.dat"]
+    import oracle as om
+    assert (tmp_path / "animdump.log").read_text() == om.animdump_line(2 * cfg.dt, 1, 3) + "\n"
     lines = open(tmp_path / files[0]).read().split("\n")[:-1]
     assert lines[0] == " ZONE F=POINT, I=%12d , J=%12d" % (cfg.nx, cfg.nz)
     assert len(lines) == 1 + cfg.nx * cfg.nz
