@@ -67,6 +67,13 @@ def main(ref):
 
     g["dt_run"] = {
         "dtin": logged("DTIN"), "xlen": logged("XLEN"), "zlen": logged("ZLEN"), "brunt": logged("BRUNT"),
+        # the run's namelist as its log prints it (&PARAMS, &MFLAGS)
+        "params": {k.lower(): logged(k) for k in ("YLEN", "XNU", "XKAPPA", "GRAV", "RHO0", "UMAX", "XACRIT", "XBCRIT",
+                                                "ZCEN", "AMP", "P", "PF", "FACKC", "FACDIR", "FACNEUMN", "FACROBIN",
+                                                "NAVGINTRFC", "ISPECFILTERNL", "ISPECFILTEREXP", "NSPECFILTEREXP",
+                                                "NSTEPS")},
+        "grid": [int(x) for x in [l for l in log if "Number of grid points in x and z" in l][0].split(":")[1].split()],
+        "nsubd": int([l for l in log if "Number of subdomains" in l][0].split()[-1]),
         "omega": [float(l.split()[-1]) for l in log if "Wave Frequency omega" in l][0],
         "cflz": [float(l.split()[-1]) for l in log if "At max CFLZ dz=" in l],
         "changes": rows(os.path.join(ref, "dtchange.dat")),

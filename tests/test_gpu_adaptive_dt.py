@@ -108,3 +108,25 @@ def test_adaptive_dt_run_and_ensemble_equal_steps():
     assert a.diag()["dt"] == e.diag()["dt"] == ref.diag()["dt"] < CASES["decrease"][0]
     for x in (a, e, f, f_alone, ref):
         x.close()
+
+
+def test_recorded_run_library_matches_oracle(golden):
+    """The reference's recorded 400-step run (forced, free-slip, adaptive dt;
+    the oracle reproduces its logged CFL numbers and dt changes, see
+    test_oracle_pins): the library in FP64 takes the same dt at every step
+    and ends within 1e-8 relative L2 of the oracle in every field."""
+    import oracle
+    import iwrepo_b200 as iw
+    from test_oracle_pins import recorded_run_config
+    cfg = recorded_run_config(golden)
+    oracle.set_threads(oracle.max_threads())
+    o, s = oracle.Oracle(cfg), iw.Solver(cfg)
+    nsteps = len(golden["dt_run"]["cflz"])
+    for n in range(nsteps):
+        o.step(1)
+        s.step(1)
+        assert s.diag()["dt"] == o.dt_state()["dt"], n + 1
+    a, b = s.state(), o.state()
+    errs = [rel(a[q], b[q]) for q in range(4)]
+    assert max(errs) <= 1e-8, errs
+    s.close()

@@ -358,3 +358,55 @@ def test_mean_density_profile_matches_rhomean_dat(golden):
         assert abs(rm - o.rhomean(z[k])) <= 5e-6 * abs(o.rhomean(z[k]))
         assert abs(rg - o.rhograd()) <= 5e-6 * abs(o.rhograd())
         assert n2 == 1.0
+
+
+def recorded_run_config(golden):
+    """The recorded 400-step run (its log `output` and dtchange.dat): grid
+    128 x (10 x 25) on runfolder/subd.dat, the namelist its log prints, the
+    forced free-slip path (calcuvwt.f), maxcalc's adaptive step, zero initial
+    fields.  fwave is not printed; the log shows the forcing at 1 for all 400
+    steps, which any fwave >= 4.3 wave periods gives (input.dat's 8 is used)."""
+    run = golden["dt_run"]
+    p = run["params"]
+    nx, nz = run["grid"]
+    ns = run["nsubd"]
+    sub = golden["subd_runfolder"][1:1 + ns]
+    return cf.Config(nx=nx, ny=1, nzloc=nz // ns, nsubd=ns, dt=run["dtin"], xlen=run["xlen"], ylen=p["ylen"],
+                     zlen=run["zlen"], brunt=run["brunt"], xnu=p["xnu"], xkappa=p["xkappa"], grav=p["grav"],
+                     rho0=p["rho0"], umax=p["umax"], xacrit=p["xacrit"], xbcrit=p["xbcrit"], zcen=p["zcen"], fwave=8.0,
+                     amp=p["amp"], p=p["p"], pf=p["pf"], fackc=p["fackc"], facdir=p["facdir"], facneumn=p["facneumn"],
+                     facrobin=p["facrobin"], ispecfilternl=int(p["ispecfilternl"]),
+                     ispecfilterexp=int(p["ispecfilterexp"]), nspecfilterexp=int(p["nspecfilterexp"]),
+                     navgintrfc=int(p["navgintrfc"]), bc_variant=cf.IW_BC_FREESLIP, meanu_damping=1, forcing=1,
+                     imaxcalc=1, z0=[r[0] for r in sub], zh=[r[1] for r in sub]).validate()
+
+
+def recorded_dt_per_step(golden):
+    """dt in effect at each of the recorded run's steps, from dtchange.dat."""
+    run = golden["dt_run"]
+    ch = {round(t, 9): dt for t, dt in run["changes"]}
+    t, dt, out = 0.0, run["dtin"], []
+    for _ in run["cflz"]:
+        dt = ch.get(round(t, 9), dt)
+        out.append(dt)
+        t = t + dt
+    return out
+
+
+def test_oracle_reproduces_recorded_run(golden):
+    """The oracle on the recorded run's configuration: maxcalc's cflz at the
+    start of every one of its 400 steps matches the run's log (16 printed
+    digits) to 5e-4 relative (it agrees to ~2e-5 typically), and dt changes at
+    the same steps to the same values (to dtchange.dat's 15 printed digits),
+    decreases included."""
+    import oracle
+    run = golden["dt_run"]
+    cfg = recorded_run_config(golden)
+    dts = recorded_dt_per_step(golden)
+    oracle.set_threads(oracle.max_threads())
+    o = Oracle(cfg)
+    for n, (cz, dt) in enumerate(zip(run["cflz"], dts)):
+        o.step(1)
+        c = o.last_maxcalc()["cfl"][2]
+        assert abs(c - cz) <= 5e-4 * cz + 1e-300 or (cz == 0.0 and c == 0.0), (n + 1, c, cz)
+        assert abs(o.dt_state()["dt"] - dt) <= 1e-14 * dt, (n + 1, o.dt_state()["dt"], dt)  # 15 printed digits
