@@ -147,6 +147,9 @@ def test_legendre_spectra_equal_oracle(tmp_path):
     for n in names:
         a, b = parse_speclegen(tmp_path / "s" / n, cfg.nsubd), parse_speclegen(tmp_path / "o" / n, cfg.nsubd)
         assert np.all(np.abs(a - b) <= 1.0001e-5 * np.abs(b) + 1e-12 * np.abs(b).max()), n
+    # the dumps leave the steps alone: the state equals the oracle's
+    a, b = s.state(), o.state()
+    assert max(np.linalg.norm(a[q] - b[q]) / np.linalg.norm(b[q]) for q in range(4)) <= 1e-10
     flat = cf.Config(nx=32, ny=1, nzloc=9, nsubd=3, dt=2e-3).validate()
     f = iw.Solver(flat)
     with pytest.raises(iw.IwError, match="ny >= 2"):
