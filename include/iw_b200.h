@@ -61,6 +61,14 @@ extern "C" {
 #define IW_BC_FREESLIP 0 /* calcuvwt.f / calcuvwt_freeslip.f: u,v Neumann at both ends */
 #define IW_BC_NOSLIP 1   /* calcuvwt_noslip.f: u,v Dirichlet bottom, Neumann top      */
 
+/* virtual paddle in rhsfm (solver.f:942-960), iw_params.forcing */
+#define IW_PADDLE_OFF 0
+#define IW_PADDLE_ALL_LEVELS 1  /* every z level, as the loop of solver.f:848 is written */
+#define IW_PADDLE_ABOVE_BOTTOM 2 /* z levels 2..nz: the bottom point is left out, as the */
+                                 /* comment at solver.f:848-849 says and as the reference's */
+                                 /* recorded 400-step run (its log `output`, uveltest.dat */
+                                 /* rows 641-1040) shows to 1e-10                          */
+
 /* storage precision of the bulk fields */
 #define IW_PREC_FP64 0  /* everything FP64 (parity path)                         */
 #define IW_PREC_MIXED 1 /* FP32 fields/FFTs/products/filters, FP64 solves        */
@@ -103,7 +111,7 @@ typedef struct iw_params {
   /* switches hard-coded in the reference */
   int32_t bc_variant;    /* IW_BC_*                                  */
   int32_t meanu_damping; /* (1,1)-mode u *= 1-fzgaus (calcuvwt.f:343) */
-  int32_t forcing;       /* virtual paddle in rhsfm (solver.f:942)   */
+  int32_t forcing;       /* IW_PADDLE_* (solver.f:942-960)           */
   int32_t precision;     /* IW_PREC_*                                */
   int32_t solver;        /* IW_SOLVE_AUTO or IW_SOLVE_LU             */
   int32_t imaxcalc;      /* 1: adaptive dt from the CFL numbers of   */

@@ -24,6 +24,7 @@ IW_MAX_SUBD = 64
 IW_MAX_NZLOC = 64
 IW_BC_FREESLIP = 0
 IW_BC_NOSLIP = 1
+IW_PADDLE_OFF, IW_PADDLE_ALL_LEVELS, IW_PADDLE_ABOVE_BOTTOM = 0, 1, 2
 IW_PREC_FP64 = 0
 IW_PREC_MIXED = 1
 IW_SOLVE_AUTO = 0
@@ -179,6 +180,8 @@ class Config:
             raise ConfigError(f"bc_variant={self.bc_variant}")
         if self.precision not in (IW_PREC_FP64, IW_PREC_MIXED):
             raise ConfigError(f"precision={self.precision}")
+        if self.forcing not in (IW_PADDLE_OFF, IW_PADDLE_ALL_LEVELS, IW_PADDLE_ABOVE_BOTTOM):
+            raise ConfigError(f"forcing={self.forcing}")
         if self.imaxcalc not in (0, 1):
             raise ConfigError(f"imaxcalc={self.imaxcalc}")
         return self
@@ -249,7 +252,7 @@ def from_files(input_dat: str, subd_dat: str, nx: int, ny: int, nzloc: int, nsub
         facdir=f["facdir"], facneumn=f["facneumn"], facrobin=f["facrobin"],
         ispecfilternl=int(f["ispecfilternl"]), ispecfilterexp=int(f["ispecfilterexp"]),
         nspecfilterexp=int(f["nspecfilterexp"]), navgintrfc=int(f["navgintrfc"]),
-        forcing=1 if p.get("xacrit", 0.0) != 0.0 else 0, imaxcalc=1,
+        forcing=IW_PADDLE_ALL_LEVELS if p.get("xacrit", 0.0) != 0.0 else IW_PADDLE_OFF, imaxcalc=1,
         z0=z0[:nsubd], zh=zh[:nsubd], name="files")
     cfg = cfg.replace(**overrides)
     return cfg.validate()
@@ -304,7 +307,9 @@ def ensemble_members(n: int = 48, seed: int = 2024) -> List[Config]:
 
 def shipped_2d(nx: int = 256, nzloc: int = 25, nsubd: int = 12, **overrides) -> Config:
     """The reference's shipped 2-D forced run (dim.h nx=256, ny=1, 12x25;
-    input.dat / subd.dat as shipped), with its values written out."""
+    input.dat / subd.dat as shipped), with its values written out.  The
+    paddle leaves out the bottom point, as the reference's recorded runs
+    do (IW_PADDLE_ABOVE_BOTTOM)."""
     z0 = [0.000, 0.025, 0.075, 0.175, 0.375, 0.775, 1.575, 2.575, 3.375, 3.975, 4.375, 4.775]
     zh = [0.025, 0.050, 0.100, 0.200, 0.400, 0.800, 1.000, 0.800, 0.600, 0.400, 0.400, 0.225]
     cfg = Config(nx=nx, ny=1, nzloc=nzloc, nsubd=nsubd, dt=0.1, xlen=20.0, ylen=1.0, zlen=5.0,
@@ -312,5 +317,6 @@ def shipped_2d(nx: int = 256, nzloc: int = 25, nsubd: int = 12, **overrides) -> 
                  xbcrit=0.84, zcen=0.13, fwave=8.0, amp=35.0, p=5.0, pf=10.0, fackc=0.0,
                  facdir=1.0, facneumn=1.0, facrobin=1e4, ispecfilternl=1, ispecfilterexp=1,
                  nspecfilterexp=1, navgintrfc=1, bc_variant=IW_BC_FREESLIP, meanu_damping=1,
-                 forcing=1, imaxcalc=1, z0=z0[:nsubd], zh=zh[:nsubd], name="shipped2d")
+                 forcing=IW_PADDLE_ABOVE_BOTTOM, imaxcalc=1, z0=z0[:nsubd], zh=zh[:nsubd],
+                 name="shipped2d")
     return cfg.replace(**overrides).validate()

@@ -1677,6 +1677,8 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
   if (std::fabs(zsum - prm->zlen) > 1e-9 * std::max(1.0, prm->zlen))
     return set_err(IW_ERR_CONFIG, "subdomain heights do not add up to zlen");
   if (!(prm->dt > 0) || !(prm->xnu > 0) || !(prm->xkappa > 0)) return set_err(IW_ERR_CONFIG, "dt, xnu, xkappa > 0");
+  if (prm->forcing < IW_PADDLE_OFF || prm->forcing > IW_PADDLE_ABOVE_BOTTOM)
+    return set_err(IW_ERR_CONFIG, "forcing: IW_PADDLE_OFF, IW_PADDLE_ALL_LEVELS or IW_PADDLE_ABOVE_BOTTOM");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(IW_ERR_CUDA, "no CUDA device");
   iw_handle* h = new iw_handle();

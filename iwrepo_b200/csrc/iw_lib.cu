@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
       qw -= tau * (ga * w - ga * P(18, i));
       qt -= tau * (ga * t - ga * P(19, i));
     }
-    if (a.forcing) {
+    if (a.forcing == IW_PADDLE_ALL_LEVELS || (a.forcing == IW_PADDLE_ABOVE_BOTTOM && k > 0)) {
       double xx = (double)i * a.dx, zz = g.zg[k];
       double arg = a.f_xk * xx - a.f_om * a.f_t;
       double sf, cf;

@@ -651,12 +651,15 @@ void rhsfm(Orc& o, std::vector<double>* G /*dudx,dudy,dudz,dvdx,...,dtdz*/) {
         }
       }
   // background-wave terms are zero arrays (wavesetup not called), fcshear=0,
-  // d2rhomeandz2=0: no-ops.  Virtual paddle (solver.f:942-960):
+  // d2rhomeandz2=0: no-ops.  Virtual paddle (solver.f:942-960).  The loop of
+  // solver.f:848 runs over k = 1..nz; its comment says the bottom point is
+  // left out, and the reference's recorded run (uveltest.dat rows 641-1040,
+  // the log `output`) was made that way: IW_PADDLE_ABOVE_BOTTOM starts at k = 2.
   if (o.pp.forcing) {
     Wave wv = wave_params(o);
     double ph = phit(o.t, wv, o.pp.fwave);
     double xa = o.pp.xacrit, um = o.pp.umax;
-    for (int k = 0; k < o.nz; ++k) {
+    for (int k = (o.pp.forcing == IW_PADDLE_ABOVE_BOTTOM ? 1 : 0); k < o.nz; ++k) {
       double zz = o.zg[k];
       double wzp = wv.xmcrit * std::cos(wv.xmcrit * zz);
       double wz = std::sin(wv.xmcrit * zz);

@@ -1,7 +1,8 @@
 """Extract the reference's own numeric artefacts into small fixtures.
 
-Run here (where the reference tree is mounted) with
-    python tests/golden/make_golden.py /root/reference/mode1_bbl
+Run where the reference tree is mounted, with its mode1_bbl directory as the
+one argument:
+    python tests/golden/make_golden.py <reference>/mode1_bbl
 It reads text files that the reference's runs wrote and stores them as JSON
 under tests/golden/.  The GPU box never reads the reference tree.
 
@@ -10,8 +11,10 @@ under tests/golden/.  The GPU box never reads the reference tree.
                      10 subdomains x 25 points of runfolder/subd.dat, zlen=5.
 * z_grid.dat      -- GLL grid of the shipped 12-subdomain run (setup.f:151-166)
 * x_grid.dat      -- x grid (setup.f:136-142)
-* uveltest.dat    -- rows 1041-1049: u(32,1,10), u(32,1,50) at t=0..0.8 of the
-                     shipped 2-D forced run (various.f:743-745)
+* uveltest.dat    -- u(32,1,10), u(32,1,50) at 16 digits (various.f:743-745):
+                     rows 1041-1049, t=0..0.8 of the shipped 2-D forced run,
+                     and rows 641-1040, the 400 steps of the recorded run
+                     whose log is `output`
 * minmaxtest.dat, cfl.dat, avgint.dat -- per-step traces of the same run
 * runfolder/subd.dat, subd.dat -- subdomain tables used above
 * rhomean.dat      -- setup.f:170-184 of the shipped run: z, rhomean(z),
@@ -50,6 +53,7 @@ def main(ref):
     g["x_grid"] = rows(os.path.join(ref, "x_grid.dat"))
     lines = open(os.path.join(ref, "uveltest.dat")).read().splitlines()
     g["uveltest"] = [[float(x) for x in l.split()] for l in lines[1040:1049]]
+    g["uveltest_recorded_run"] = [[float(x) for x in l.split()] for l in lines[640:1040]]
     g["minmaxtest"] = rows(os.path.join(ref, "minmaxtest.dat"))
     g["cfl"] = rows(os.path.join(ref, "cfl.dat"), 1)
     g["avgint"] = rows(os.path.join(ref, "avgint.dat"), 1)
@@ -89,4 +93,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/mode1_bbl")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference mode1_bbl directory>")
+    main(sys.argv[1])

@@ -29,7 +29,7 @@ def test_namelists(tmp_path):
     (tmp_path / "subd.dat").write_text(SUBD_DAT)
     c = cf.from_files(str(tmp_path / "input.dat"), str(tmp_path / "subd.dat"), nx=16, ny=1, nzloc=9, nsubd=3)
     assert c.dt == 0.1 and c.xlen == 20.0 and c.brunt == 0.2 and c.facrobin == 1e4
-    assert c.amp == 35.0 and c.p == 5.0 and c.pf == 10.0 and c.forcing == 1
+    assert c.amp == 35.0 and c.p == 5.0 and c.pf == 10.0 and c.forcing == cf.IW_PADDLE_ALL_LEVELS
     assert c.zh == [1.0, 2.5, 1.5] and c.nz == 27
 
 

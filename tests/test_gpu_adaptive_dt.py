@@ -112,17 +112,29 @@ def test_adaptive_dt_run_and_ensemble_equal_steps():
 
 def test_recorded_run_library_matches_oracle(golden):
     """The reference's recorded 400-step run (forced, free-slip, adaptive dt;
-    the oracle reproduces its logged CFL numbers and dt changes, see
-    test_oracle_pins): the library in FP64 takes the same dt at every step
-    and ends within 1e-8 relative L2 of the oracle in every field."""
+    the oracle reproduces its logged CFL numbers, probes and dt changes, see
+    test_oracle_pins): the library in FP64
+    * reproduces the reference's own 16-digit probes u(32,1,10), u(32,1,50)
+      (uveltest.dat rows 641-1040) at the start of every step to 1e-9 of
+      their scale;
+    * takes the same dt as the oracle at every step;
+    * ends within 1e-8 relative L2 of the oracle in every field."""
     import oracle
     import iwrepo_b200 as iw
-    from test_oracle_pins import recorded_run_config
+    from test_oracle_pins import probe_scale, recorded_run_config
     cfg = recorded_run_config(golden)
+    rows = golden["uveltest_recorded_run"]
     oracle.set_threads(oracle.max_threads())
     o, s = oracle.Oracle(cfg), iw.Solver(cfg)
     nsteps = len(golden["dt_run"]["cflz"])
     for n in range(nsteps):
+        # maxcalc's probes at the start of step n+1: physical u of the state
+        spec = s.state(0)[0][:, 0, :]  # (nz, nxpp), ny = 1
+        c = spec[:, 0::2] + 1j * spec[:, 1::2]
+        phys = np.fft.irfft(c * cfg.nx, n=cfg.nx, axis=1)
+        got = np.array([phys[9, 31], phys[49, 31]])
+        assert np.all(np.abs(got - np.array(rows[n][1:])) <= 1e-9 * probe_scale(rows, n) + 1e-300), \
+            (n + 1, got, rows[n])
         o.step(1)
         s.step(1)
         assert s.diag()["dt"] == o.dt_state()["dt"], n + 1

@@ -6,10 +6,17 @@ must reproduce (tests/golden/reference_runs.json, made by make_golden.py):
 * testout.dat (testhelm.f): penalty solve, 8 significant digits  -> exact pin
 * z_grid.dat / x_grid.dat: GLL / uniform grids, 7 decimals        -> exact pin
 * run log `output`: wave frequency of the 128x250 run, 15 digits  -> exact pin
-* uveltest.dat / cfl.dat / minmaxtest.dat: 9 steps of the shipped 2-D forced
-  run (calcuvwt_noslip.f).  The input.dat of that run is not recorded (it
-  stopped after 9 of the 400 steps the shipped file asks for); the oracle
-  follows it to 4-5 significant digits, the free-slip variant does not.
+* the recorded 400-step run (its log `output`, dtchange.dat and rows 641-1040
+  of uveltest.dat): every input is printed in the log; the oracle reproduces
+  its 16-digit probes u(32,1,10), u(32,1,50) and maxcalc's cflz at every step
+  to 1e-9, with the paddle left out of the bottom point (IW_PADDLE_ABOVE_BOTTOM,
+  the comment of solver.f:848-849).  With the paddle on every level, as the
+  loop of solver.f:848 is written, they differ by 1e-4 from the first step.
+* uveltest.dat / cfl.dat / minmaxtest.dat rows of a later 9-step run of the
+  shipped 2-D forced configuration (calcuvwt_noslip.f).  The input.dat of that
+  run is not recorded (it stopped after 9 of the 400 steps the shipped file
+  asks for); the oracle follows it to 4-5 significant digits, the free-slip
+  variant does not.
 """
 import math
 
@@ -377,7 +384,8 @@ def recorded_run_config(golden):
                      amp=p["amp"], p=p["p"], pf=p["pf"], fackc=p["fackc"], facdir=p["facdir"], facneumn=p["facneumn"],
                      facrobin=p["facrobin"], ispecfilternl=int(p["ispecfilternl"]),
                      ispecfilterexp=int(p["ispecfilterexp"]), nspecfilterexp=int(p["nspecfilterexp"]),
-                     navgintrfc=int(p["navgintrfc"]), bc_variant=cf.IW_BC_FREESLIP, meanu_damping=1, forcing=1,
+                     navgintrfc=int(p["navgintrfc"]), bc_variant=cf.IW_BC_FREESLIP, meanu_damping=1,
+                     forcing=cf.IW_PADDLE_ABOVE_BOTTOM,
                      imaxcalc=1, z0=[r[0] for r in sub], zh=[r[1] for r in sub]).validate()
 
 
@@ -393,20 +401,63 @@ def recorded_dt_per_step(golden):
     return out
 
 
+def probe_scale(rows, n, half=10):
+    """Scale of the probe values near step n: the largest |value| of that
+    probe within +-half steps (a probe crossing zero keeps the scale of its
+    swing, so a relative bound means something there too)."""
+    lo, hi = max(0, n - half), min(len(rows), n + half + 1)
+    return np.abs(np.array([r[1:] for r in rows[lo:hi]])).max(axis=0)
+
+
 def test_oracle_reproduces_recorded_run(golden):
-    """The oracle on the recorded run's configuration: maxcalc's cflz at the
-    start of every one of its 400 steps matches the run's log (16 printed
-    digits) to 5e-4 relative (it agrees to ~2e-5 typically), and dt changes at
-    the same steps to the same values (to dtchange.dat's 15 printed digits),
-    decreases included."""
+    """The oracle on the recorded run's configuration, for all 400 steps:
+    * maxcalc's cflz at the start of every step matches the run's log (16
+      printed digits) to 1e-9 relative;
+    * the probes u(32,1,10) and u(32,1,50) that maxcalc appends to
+      uveltest.dat (rows 641-1040, 16 digits) match to 1e-9 of their scale;
+    * dt changes at the same steps to the same values (to dtchange.dat's 15
+      printed digits), decreases included.
+    The agreement grows from 1e-13 over the first steps to about 1e-10 at the
+    end: FP64 rounding differences carried through 400 steps."""
     import oracle
     run = golden["dt_run"]
+    rows = golden["uveltest_recorded_run"]
     cfg = recorded_run_config(golden)
     dts = recorded_dt_per_step(golden)
     oracle.set_threads(oracle.max_threads())
     o = Oracle(cfg)
+    assert len(rows) == len(run["cflz"]) == 400
     for n, (cz, dt) in enumerate(zip(run["cflz"], dts)):
+        assert abs(o.scalars()[0] - rows[n][0]) <= 1e-13 * max(1.0, rows[n][0])  # t at the step's start
         o.step(1)
-        c = o.last_maxcalc()["cfl"][2]
-        assert abs(c - cz) <= 5e-4 * cz + 1e-300 or (cz == 0.0 and c == 0.0), (n + 1, c, cz)
+        lm = o.last_maxcalc()
+        c = lm["cfl"][2]
+        assert abs(c - cz) <= 1e-9 * cz or (cz == 0.0 and c == 0.0), (n + 1, c, cz)
+        assert np.all(np.abs(lm["probe"] - np.array(rows[n][1:])) <= 1e-9 * probe_scale(rows, n) + 1e-300), \
+            (n + 1, lm["probe"], rows[n])
         assert abs(o.dt_state()["dt"] - dt) <= 1e-14 * dt, (n + 1, o.dt_state()["dt"], dt)  # 15 printed digits
+
+
+def test_recorded_run_paddle_leaves_out_the_bottom_point(golden):
+    """The one difference between the shipped solver.f and the binary that
+    made the recorded run: the paddle loop of solver.f:848 runs over
+    k = 1..nz, while its comment says the bottom point is overlooked.  Over
+    the first 6 steps, the paddle on every level (IW_PADDLE_ALL_LEVELS) puts
+    the probes 2e-5 to 4e-4 and cflz 1e-4 away from the recorded values;
+    leaving the bottom point out (IW_PADDLE_ABOVE_BOTTOM) brings both within
+    1e-12."""
+    run = golden["dt_run"]
+    rows = golden["uveltest_recorded_run"]
+    errs = {}
+    for mode in (cf.IW_PADDLE_ALL_LEVELS, cf.IW_PADDLE_ABOVE_BOTTOM):
+        o = Oracle(recorded_run_config(golden).replace(forcing=mode))
+        ep, ec = 0.0, 0.0
+        for n in range(6):
+            o.step(1)
+            lm = o.last_maxcalc()
+            if n:
+                ep = max(ep, float(np.max(np.abs(lm["probe"] - rows[n][1:]) / np.abs(rows[n][1:]))))
+                ec = max(ec, abs(lm["cfl"][2] - run["cflz"][n]) / run["cflz"][n])
+        errs[mode] = (ep, ec)
+    assert errs[cf.IW_PADDLE_ALL_LEVELS][0] > 1e-4 and errs[cf.IW_PADDLE_ALL_LEVELS][1] > 5e-5
+    assert errs[cf.IW_PADDLE_ABOVE_BOTTOM][0] < 1e-12 and errs[cf.IW_PADDLE_ABOVE_BOTTOM][1] < 1e-12
