@@ -156,6 +156,12 @@ int iw_init(const iw_dims *dims, const iw_params *prm, int device,
             iw_handle **out);
 int iw_destroy(iw_handle *h);
 const char *iw_last_error(void);
+/* Not in the reference.  The IW_ERR_* code of the last failure recorded on
+ * this thread.  The reference-named routines that return nothing record
+ * theirs here: penalty_main_ and bandlu_solve_ start from 0 and record
+ * IW_ERR_PIVOT when SGBTF2 meets a zero pivot (its INFO, which the reference
+ * ignores; the solution then holds Inf or NaN as the reference's would). */
+int iw_last_status(void);
 
 /* Upload / download the complete multistep state in the reference layout.
  * Each pointer addresses 4 fields (u,v,w,temp) back to back, i.e.
@@ -259,7 +265,15 @@ int iw_init_mode1(iw_handle *h, double amplitude, double noise_amp,
 
 /* One complete time step of main.f:653-1066: maxcalc round trip, convec,
  * coefficient schedule, calcuvwt, t += dt, interface averaging.  The
- * coefficient schedule of main.f:700-856 is applied internally (fixed dt). */
+ * coefficient schedule of main.f:700-856 is applied internally (fixed dt).
+ * Failure detection (not in the reference): the first kernel of every step
+ * flags a NaN or Inf in the state it reads, and a solve kernel whose bounded
+ * wait for its tables gives up flags a timeout.  The flags reach the host
+ * without a wait, so iw_step and iw_run return IW_ERR_NONFINITE (or
+ * IW_ERR_TIMEOUT) from the first call after the flag has arrived, usually
+ * one or two steps later, and then refuse to step; iw_sync and iw_diag wait
+ * and report it at once.  A new state (iw_upload_state, iw_init_mode1,
+ * iw_read_restart) clears the flags. */
 int iw_step(iw_handle *h);
 /* nsteps steps of main.f:653-1066.  With use_graph != 0, once the step is
  * invariant, steps are replayed from two captured CUDA graphs, one launch per
@@ -272,12 +286,23 @@ int iw_run(iw_handle *h, int nsteps, int use_graph);
 
 /* Not in the reference.  Times the launch candidates of this handle's step on
  * its device and keeps the fastest for the following steps: y-tile width (2, 4
- * or 8 columns) and the stage-A and stage-E variants (register-column or
- * tiled).  Candidates run on the handle's scratch fields; the state is not
- * changed.  The stage variants differ only in the order of floating-point sums.
- * choices (optional, 3 ints): the y-tile width, and for stage A and stage E
- * 1 = register-column, 0 = tiled, -1 = not applicable. */
+ * or 8 columns), the stage-A and stage-E variants (register-column or tiled)
+ * and the solve variant (system-grouped CTAs with the tables staged in shared
+ * memory, or one CTA per task of <= 4 right-hand sides).  Candidates run on
+ * the handle's scratch fields; the state is not changed (the solver tables
+ * are built if no step has built them yet).  The stage variants differ only
+ * in the order of floating-point sums; the solve variants give the same bits.
+ * choices (optional, 4 ints): the y-tile width; for stage A and stage E
+ * 1 = register-column, 0 = tiled, -1 = not applicable; the solve variant
+ * (1 = system-grouped, 0 = per task). */
 int iw_autotune(iw_handle *h, int *choices);
+
+/* Not in the reference.  Sets one launch choice of iw_autotune directly. */
+#define IW_LAUNCH_YTILE 0   /* 0 (size heuristic), 2, 4 or 8 */
+#define IW_LAUNCH_STAGE_A 1 /* -1 (size heuristic), 0 tiled, 1 register-column */
+#define IW_LAUNCH_STAGE_E 2 /* as stage A */
+#define IW_LAUNCH_SOLVE 3   /* 1 system-grouped (default), 0 per task */
+int iw_set_launch(iw_handle *h, int which, int value);
 
 /* Not in the reference (its main.f advances one run).  Advances n independent
  * runs of any sizes (separate handles on one device) by nsteps steps each.
@@ -288,6 +313,13 @@ int iw_autotune(iw_handle *h, int *choices);
 int iw_ensemble_run(iw_handle *const *members, int n, int nsteps);
 /* As iw_step but with caller-supplied coefficients (variable-dt restarts). */
 int iw_step_coefs(iw_handle *h, const iw_coefs *c);
+/* The values main.f keeps in COMMON /ab/ /bdf/ (comtimeadvance.h), dt and t
+ * (COMMON /time/), set on the handle without stepping: convec_ reads fac1..3,
+ * bdf1..3, dt and t, calcuvwt_ reads bdfv and dt.  A Fortran driver that
+ * keeps main.f's own sequence (convec_, the coefficient updates of
+ * main.f:700-856, calcuvwt_, t = t + dt, interface_avg3d_) calls this where
+ * main.f assigns them. */
+int iw_set_coefs(iw_handle *h, const iw_coefs *c, double t);
 
 int iw_diag(iw_handle *h, iw_diag_out *out);
 /* Mean (kx=ky=0) profiles of u, v, w, rho (4*nz doubles) copied to the host

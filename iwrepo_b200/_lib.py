@@ -22,8 +22,8 @@ PI = C.POINTER(C.c_int)
 
 # every entry point declared in include/iw_b200.h
 EXPORTS = [
-    "iw_init", "iw_destroy", "iw_last_error", "iw_upload_state", "iw_download_state", "iw_init_mode1",
-    "iw_write_restart", "iw_read_restart", "iw_write_fields", "iw_wait_fields", "iw_set_animation", "iw_set_speclegen", "iw_postp", "iw_set_postp", "iw_step", "iw_run", "iw_ensemble_run", "iw_autotune", "iw_step_coefs", "iw_diag", "iw_sync", "iw_field_ptr", "iw_stream",
+    "iw_init", "iw_destroy", "iw_last_error", "iw_last_status", "iw_upload_state", "iw_download_state", "iw_init_mode1",
+    "iw_write_restart", "iw_read_restart", "iw_write_fields", "iw_wait_fields", "iw_set_animation", "iw_set_speclegen", "iw_postp", "iw_set_postp", "iw_step", "iw_run", "iw_ensemble_run", "iw_autotune", "iw_set_launch", "iw_step_coefs", "iw_set_coefs", "iw_diag", "iw_sync", "iw_field_ptr", "iw_stream",
     "iw_device_bytes", "iw_helm_solve_batched", "iw_bind", "iw_profile", "iw_profile_read", "iw_mean_profiles",
     "horfft_", "dpdz_", "filter_3dlegenfourier_", "filter_legenpen_", "interface_avg3d_",
     "penalty_main_", "bandlu_solve_", "iw_bandlu_solve_noalloc", "penalty_setup_", "convec_", "calcuvwt_",
@@ -32,7 +32,11 @@ EXPORTS = [
 
 
 class IwError(RuntimeError):
-    pass
+    """A nonzero status of the C ABI; .code holds the IW_ERR_* value."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 def build(verbose: bool = False) -> str:
@@ -53,6 +57,7 @@ def lib():
     vp = C.c_void_p
     L.iw_init.argtypes = [C.POINTER(IwDims), C.POINTER(IwParams), C.c_int, C.POINTER(vp)]
     L.iw_destroy.argtypes = [vp]
+    L.iw_last_status.restype = C.c_int
     L.iw_last_error.restype = C.c_char_p
     L.iw_upload_state.argtypes = [vp, PD, PD, PD, PD, PD, C.c_double, C.c_int]
     L.iw_download_state.argtypes = [vp, PD, PD, PD, PD, PD]
@@ -61,7 +66,9 @@ def lib():
     L.iw_run.argtypes = [vp, C.c_int, C.c_int]
     L.iw_ensemble_run.argtypes = [C.POINTER(vp), C.c_int, C.c_int]
     L.iw_autotune.argtypes = [vp, PI]
+    L.iw_set_launch.argtypes = [vp, C.c_int, C.c_int]
     L.iw_step_coefs.argtypes = [vp, C.POINTER(IwCoefs)]
+    L.iw_set_coefs.argtypes = [vp, C.POINTER(IwCoefs), C.c_double]
     L.iw_diag.argtypes = [vp, C.POINTER(IwDiagOut)]
     L.iw_sync.argtypes = [vp]
     L.iw_field_ptr.argtypes = [vp, C.c_int, C.POINTER(vp)]
@@ -112,4 +119,4 @@ def lib():
 
 def check(rc: int):
     if rc != 0:
-        raise IwError(f"iw error {rc}: {lib().iw_last_error().decode()}")
+        raise IwError(f"iw error {rc}: {lib().iw_last_error().decode()}", rc)

@@ -101,6 +101,7 @@ __global__ void k_legen_one(Geo g, const double* wg, const double* alpol, const 
 int factor_dense_or_params(iw_handle* h, const double* pen6, double eps, int bot, int top, const double* dense,
                            double** ab_out, int** ipiv_out) {
   const int n = h->nz, N = h->N, ldab = 3 * N + 1, ns = h->ns;
+  g_status = 0;
   SysDesc sd;
   memset(&sd, 0, sizeof sd);
   sd.eps = eps;
@@ -137,10 +138,14 @@ int factor_dense_or_params(iw_handle* h, const double* pen6, double eps, int bot
     fa.assemble = 0;
   }
   k_factor<<<1, 32, 0, h->st>>>(geo(h), fa);
-  CK(cudaStreamSynchronize(h->st));
+  int info = 0;
+  CK(scopy(h, &info, dinfo, sizeof info, cudaMemcpyDeviceToHost));
   cudaFree(dsd);
   cudaFree(dpen);
   cudaFree(dinfo);
+  // SGBTF2's INFO (bandludcmp.f:238-440): the reference ignores it (band_lu.f:23-34)
+  // and so does the solve that follows; it is recorded for iw_last_status.
+  if (info > 0) set_err(IW_ERR_PIVOT, "zero pivot in band factorisation at column " + std::to_string(info));
   *ab_out = dab;
   *ipiv_out = dip;
   return 0;
@@ -454,17 +459,19 @@ static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
   Geo g = geo(h);
   T* dst = fs.Y12[0];
   T* tmp = fs.Y12[1];
-  CK(cudaMemsetAsync(h->dred, 0, 8 * sizeof(double), h->st));
-  // KE: u,v,w ; eps: 9 gradients
+  // KE: u,v,w ; eps: 9 gradients.  Per-block slots (296 for KE, 296 for
+  // eps) in the second half of dpart, added in order on the host.
+  double* rp = h->dpart + (size_t)4 * 296 * 5;
+  CK(cudaMemsetAsync(rp, 0, 2 * 296 * sizeof(double), h->st));
   for (int q = 0; q < 3; ++q) {
     phys_of<T>(h, fs, fs.F[q], dst, tmp, 0);
-    k_reduce_sq<T><<<296, 256, 0, h->st>>>(g, dst, 1, h->dred + 0);
+    k_reduce_sq<T><<<296, 256, 0, h->st>>>(g, dst, 1, rp);
     for (int op = 1; op <= 3; ++op) {
       phys_of<T>(h, fs, fs.F[q], dst, tmp, op);
-      k_reduce_sq<T><<<296, 256, 0, h->st>>>(g, dst, 1, h->dred + 1);
+      k_reduce_sq<T><<<296, 256, 0, h->st>>>(g, dst, 1, rp + 296);
     }
   }
-  double red[8];
+  double red[2] = {0, 0};
   // maxcalc statistics on the physical fields
   {
     const double dx = h->p.xlen / h->nx, dy = h->p.ylen / h->ny;
@@ -476,10 +483,13 @@ static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
                                               h->dpart + (size_t)q * 296 * 5);
     }
   }
-  std::vector<double> part((size_t)4 * 296 * 5);
+  std::vector<double> part((size_t)4 * 296 * 5 + 2 * 296);
   CK(cudaMemcpyAsync(part.data(), h->dpart, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  CK(cudaMemcpyAsync(red, h->dred, sizeof red, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
+  for (int b = 0; b < 296; ++b) {
+    red[0] += part[(size_t)4 * 296 * 5 + b];
+    red[1] += part[(size_t)4 * 296 * 5 + 296 + b];
+  }
   memset(out, 0, sizeof *out);
   {
     double mm[4][2], cf[4] = {0, 0, 0, 0}, s2 = 0, cnt = 0;
@@ -525,7 +535,7 @@ static int diag_impl(iw_handle* h, FieldSet<T>& fs, iw_diag_out* out) {
   CK(cudaMemcpyAsync(&flag, h->dflag, sizeof flag, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   if (flag) return set_err(IW_ERR_NONFINITE, "non-finite value in the state");
-  return IW_OK;
+  return sync_errors(h);
 }
 
 // CFL numbers of the state for the adaptive rule: maxcalc's cflxmax and

@@ -351,6 +351,10 @@ struct iw_handle {
   double *dwnl = 0, *dwvr = 0, *dred = 0;
   int* dcnt = 0;
   int* dflag = 0;
+  int* derr = 0;  // device error words: [0] non-finite state, [1] a bounded device wait gave up
+  int* herr = 0;  // pinned host copy of derr, written after each eager step or graph run
+  cudaEvent_t err_ev = 0;
+  bool err_ev_live = false;
   FftPlan plx, ply;
   FieldSet<double> f64;
   FieldSet<float> f32;
@@ -383,6 +387,12 @@ struct iw_handle {
   // tasks [0, nrefine) get one FP64 residual sweep: their systems have an
   // estimated condition number above kRefineCond (small kx^2+ky^2 pressure)
   int nrefine[SYS_KINDS] = {0, 0, 0, 0};
+  // system-grouped tasks of k_solve_sys (up to 4 u/v or 8 other columns of
+  // one system each) for the sorted columns after tasks [0, nold) of k_solve_cta
+  Task* dtasks2[SYS_KINDS] = {0, 0, 0, 0};
+  int ntask2[SYS_KINDS] = {0, 0, 0, 0};
+  int nold[SYS_KINDS] = {0, 0, 0, 0};
+  int use_sys = 1;  // 0: k_solve_cta for every task (kept for comparison)
   double bi_bdfv[SYS_KINDS] = {-1, -1, -1, -1};
   bool bi_fold[SYS_KINDS] = {false, false, false, false};  // Legendre filter folded into ainv
   // distinct subdomain blocks: subdomain ks uses block bmap[ks]; brep[b] is a
@@ -598,6 +608,36 @@ static int build_tasks(iw_handle* h, int kind, const std::vector<int>& colsys, i
   return 0;
 }
 
+// tasks of k_solve_sys: after the k_solve_cta prefix (the refined tasks and
+// the columns without a system, which sort first), runs of the sorted column
+// order that share one system, in pieces of at most 4 (u/v) or 8 columns
+static int build_sys_tasks(iw_handle* h, int kind, const std::vector<int>& colsys) {
+  const auto& tk = h->htasks[kind];
+  int nold = h->nrefine[kind];
+  while (nold < (int)tk.size() && tk[nold].sys < 0) ++nold;
+  for (int t = nold; t < (int)tk.size(); ++t)
+    if (tk[t].sys < 0) nold = t + 1;  // a system-less task after the prefix stays with k_solve_cta
+  h->nold[kind] = nold;
+  const int G = kind == SYS_U ? kSysR / 4 : kSysR / 2;
+  std::vector<int> order(h->ncol);
+  for (int c = 0; c < h->ncol; ++c) order[c] = c;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h->col_u[a] < h->col_u[b]; });
+  std::vector<Task> tasks;
+  int i = nold < (int)tk.size() ? tk[nold].first : h->ncol;
+  while (i < h->ncol) {
+    const int s = colsys[order[i]];
+    int jn = i;
+    while (jn < h->ncol && colsys[order[jn]] == s && jn - i < G) ++jn;
+    tasks.push_back(Task{s, i, jn - i});
+    i = jn;
+  }
+  cudaFree(h->dtasks2[kind]);
+  h->dtasks2[kind] = nullptr;
+  h->ntask2[kind] = (int)tasks.size();
+  if (!tasks.empty() && up(h, &h->dtasks2[kind], tasks)) return IW_ERR_NOMEM;
+  return 0;
+}
+
 // (re)build the factors of one kind for the current bdfv/dt
 static int build_factors(iw_handle* h, int kind) {
   const int ns = h->ns, N = h->N, n = h->nz, ldab = 3 * N + 1;
@@ -742,7 +782,8 @@ static int build_blockinv(iw_handle* h, int kind, bool fold) {
     cudaFree(B.colsys);
     B = iw_handle::BI();
     char* ai = nullptr;
-    if (dalloc(h, &ai, (size_t)std::max(nsys, 1) * h->nb * N * N * tib) ||
+    // (+16 bytes: k_solve_sys copies whole 16-byte units)
+    if (dalloc(h, &ai, (size_t)std::max(nsys, 1) * h->nb * N * N * tib + 16) ||
         dalloc(h, &B.cvec, (size_t)std::max(nsys, 1) * ns * N) || dalloc(h, &B.dvec, (size_t)std::max(nsys, 1) * ns * N) ||
         dalloc(h, &B.minv, (size_t)std::max(nsys, 1) * std::max(m * m, 1)) ||
         dalloc(h, &B.pen, (size_t)std::max(nsys, 1) * 6 * ns) || dalloc(h, &B.sys, (size_t)std::max(nsys, 1)) ||
@@ -774,6 +815,7 @@ static int build_blockinv(iw_handle* h, int kind, bool fold) {
     for (int t = 0; t < (int)tk.size(); ++t)
       if (tk[t].sys >= 0 && 1.0 + sys[tk[t].sys].eps * rho > kRefineCond) last = t;
     h->nrefine[kind] = last + 1;
+    if (build_sys_tasks(h, kind, colsys)) return IW_ERR_NOMEM;
     int nraw = 0;
     if (fold)
       for (int t = 0; t <= last; ++t) nraw = std::max(nraw, tk[t].sys + 1);
@@ -905,7 +947,8 @@ template <typename T, int NM>
 static void launch_stageA_r(iw_handle* h, FieldSet<T>& fs, int proj) {
   dim3 grid((unsigned)((h->plane + 127) / 128), (unsigned)h->ns, 4);
   k_stageA_r<T, NM><<<grid, 128, 0, h->st>>>(geo(h), make_zop<T, NM>(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.F1[0],
-                                             fs.F1[1], fs.F1[2], fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj);
+                                             fs.F1[1], fs.F1[2], fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj,
+                                             h->derr);
 }
 
 template <typename T>
@@ -922,7 +965,8 @@ static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
   dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
   size_t smem = (size_t)(h->N * h->N + h->N * kTX) * sizeof(T);
   k_stageA<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.F1[0], fs.F1[1],
-                                                fs.F1[2], fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj);
+                                                fs.F1[2], fs.F1[3], fs.Z4[0], fs.Z4[1], fs.Z4[2], fs.Z4[3], proj,
+                                                h->derr);
 }
 
 template <typename T>
@@ -1319,8 +1363,34 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   // copy and the filter pass; the rest needs no filter pass.
   const int nref = h->nrefine[kind], nt = h->ntask[kind];
   const bool fold = h->bi_fold[kind] && cpen;
+  // system-grouped kernel for the tasks after the prefix, when it applies
+  const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3);
+  const size_t smsys = lay.total * sizeof(double);
+  const bool grouped = h->use_sys && h->nz <= kSysMaxRows && (!cpen || fold) && smsys <= 200 * 1024;
+  const int nend = grouped ? std::max(h->nold[kind], nref) : nt;
+  if (grouped && h->ntask2[kind] > 0) {
+    const int nthr = (h->nz + 31) / 32 * 32;
+    Geo g = geo(h);
+    const double* mg = h->dmeang;
+#define IW_SYS_LAUNCH(RL)                                                                                           \
+  do {                                                                                                            \
+    cudaFuncSetAttribute(k_solve_sys<T, RL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smsys);           \
+    k_solve_sys<T, RL><<<h->ntask2[kind], nthr, smsys, h->st>>>(g, bi, h->dtasks2[kind], h->dcolorder, F0, F1, F2, \
+                                                               rd, meanu, mg, h->dDt, h->dwnl, h->dwvr, kstart,   \
+                                                               h->derr);                                          \
+  } while (0)
+    if (role == 0)
+      IW_SYS_LAUNCH(0);
+    else if (role == 1)
+      IW_SYS_LAUNCH(1);
+    else if (role == 2)
+      IW_SYS_LAUNCH(2);
+    else
+      IW_SYS_LAUNCH(3);
+#undef IW_SYS_LAUNCH
+  }
   for (int part = 0; part < 2; ++part) {
-    const int t0 = part == 0 ? 0 : nref, cnt = part == 0 ? nref : nt - nref;
+    const int t0 = part == 0 ? 0 : nref, cnt = part == 0 ? nref : nend - nref;
     if (cnt <= 0) continue;
     BlockInv b2 = bi;
     int cp = cpen;
@@ -1482,7 +1552,7 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
     cudaEventElapsedTime(&ms, e0, e1);
     return ms;
   };
-  const int save[3] = {h->tune_ytx, h->tune_a, h->tune_e};
+  const int save[4] = {h->tune_ytx, h->tune_a, h->tune_e, h->use_sys};
   // y tiles: the 12-job inverse and the 4-job forward-with-fold launches
   float best = 1e30f;
   int besttx = 8;
@@ -1519,6 +1589,19 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
   }
   h->tune_a = besta;
   h->tune_e = beste;
+  // solves: system-grouped kernel or one task of <= 4 right-hand sides per
+  // CTA (the u/v solve; the tables are built first if no step has run yet)
+  if (ensure_factors(h, (h->p.ispecfilterexp == 1) && ((h->istep + 1) % h->p.nspecfilterexp == 0)) == IW_OK &&
+      h->use_bi) {
+    const int cpen = (h->p.ispecfilterexp == 1) && ((h->istep + 1) % h->p.nspecfilterexp == 0);
+    const int kstart = h->p.bc_variant == IW_BC_NOSLIP ? 1 : 0;
+    float tsolve[2];
+    for (int v = 0; v < 2; ++v) {
+      h->use_sys = v;
+      tsolve[v] = timeit([&] { launch_solve_bi<T>(h, ts, 0, cpen, kstart); });
+    }
+    h->use_sys = tsolve[1] <= tsolve[0] ? 1 : 0;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   const cudaError_t err = cudaGetLastError();
@@ -1526,12 +1609,14 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
     h->tune_ytx = save[0];
     h->tune_a = save[1];
     h->tune_e = save[2];
+    h->use_sys = save[3];
     return set_err(IW_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(err));
   }
   if (choice) {
     choice[0] = h->tune_ytx;
     choice[1] = h->tune_a;
     choice[2] = h->tune_e;
+    choice[3] = h->use_sys;
   }
   return IW_OK;
 }
@@ -1608,6 +1693,42 @@ static int capture_step(iw_handle* const* hs, int n, cudaStream_t s0, cudaGraphE
 // nsteps steps of every handle (all graph_ready, same device) as alternating
 // graph launches on a private stream, ordered after and before the handles'
 // own streams.
+// Device error words -> IW_ERR_*.  Stage A flags a NaN or Inf in the state
+// it reads at the start of every step; a bounded wait of a solve kernel that
+// gave up flags a timeout.  The words stay set until the state is replaced.
+static int err_code(const int* w) {
+  if (w[0]) return set_err(IW_ERR_NONFINITE, "non-finite value in the state (found by a step's stage A)");
+  if (w[1]) return set_err(IW_ERR_TIMEOUT, "a bounded device wait gave up (the solver tables did not arrive)");
+  return IW_OK;
+}
+// the host copy left by the last step whose copy has completed (no wait)
+static int poll_errors(iw_handle* h) {
+  if (!h->err_ev_live || cudaEventQuery(h->err_ev) != cudaSuccess) return IW_OK;
+  return err_code(h->herr);
+}
+// queue the copy of the words behind the work just launched (not while capturing)
+static void post_errors(iw_handle* h) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(h->st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  if (cudaMemcpyAsync(h->herr, h->derr, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->st) == cudaSuccess &&
+      cudaEventRecord(h->err_ev, h->st) == cudaSuccess)
+    h->err_ev_live = true;
+}
+// wait for the handle's stream and check the words
+static int sync_errors(iw_handle* h) {
+  int w[2] = {0, 0};
+  CK(scopy(h, w, h->derr, sizeof w, cudaMemcpyDeviceToHost));
+  return err_code(w);
+}
+// a new state: forget earlier findings
+static int clear_errors(iw_handle* h) {
+  CK(cudaMemsetAsync(h->derr, 0, 2 * sizeof(int), h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->herr[0] = h->herr[1] = 0;
+  h->err_ev_live = false;
+  return IW_OK;
+}
+
 static int run_graphs(iw_handle* const* hs, int n, int nsteps) {
   if (nsteps <= 0) return IW_OK;
   cudaStream_t s0 = nullptr;
@@ -1637,7 +1758,10 @@ static int run_graphs(iw_handle* const* hs, int n, int nsteps) {
         }
     }
     cudaEventRecord(ev, s0);
-    for (int i = 0; i < n; ++i) cudaStreamWaitEvent(hs[i]->st, ev, 0);
+    for (int i = 0; i < n; ++i) {
+      cudaStreamWaitEvent(hs[i]->st, ev, 0);
+      post_errors(hs[i]);
+    }
   }
   for (auto& g : gx)
     if (g) cudaGraphExecDestroy(g);
@@ -1652,6 +1776,7 @@ static int run_graphs(iw_handle* const* hs, int n, int nsteps) {
 extern "C" {
 
 const char* iw_last_error(void) { return g_err.c_str(); }
+int iw_last_status(void) { return g_status; }
 
 int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** out) {
   if (!dims || !prm || !out) return set_err(IW_ERR_CONFIG, "null argument");
@@ -1772,16 +1897,20 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
         const double zm = kg - 1 >= 1 ? zf[kg - 1] : zgl[nz - 1];
         dzi[k] = 1.0 / (zf[kg] - zm);
       }
-    r |= up(h, &h->ddzinv, dzi) || dalloc(h, &h->dpart, (size_t)4 * 296 * 5);
+    r |= up(h, &h->ddzinv, dzi) || dalloc(h, &h->dpart, (size_t)4 * 296 * 5 + 2 * 296);
   }
   r |= up(h, &h->dD, h->tab.D) || up(h, &h->dD2, h->tab.D2) || up(h, &h->dL, h->tab.Lfil) || up(h, &h->dh, hf) ||
        up(h, &h->dxw, xw) || up(h, &h->dyw, yw) || up(h, &h->dcf, cf) || up(h, &h->dzg, zg) || up(h, &h->dzh, zh) ||
        up(h, &h->dwg, h->tab.wg) || up(h, &h->dal, h->tab.alpol) || up(h, &h->dsig, h->tab.sigma) ||
        up(h, &h->dmeang, mg);
   r |= dalloc(h, &h->dwnl, h->plane * 2) || dalloc(h, &h->dwvr, h->plane * 2) || dalloc(h, &h->dred, std::max<size_t>(64, 4 * (size_t)h->nz)) ||
-       dalloc(h, &h->dcnt, 8) || dalloc(h, &h->dflag, 4);
+       dalloc(h, &h->dcnt, 8) || dalloc(h, &h->dflag, 4) || dalloc(h, &h->derr, 2) ||
+       cudaHostAlloc((void**)&h->herr, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->err_ev, cudaEventDisableTiming) != cudaSuccess;
   if (!r) {
     cudaMemset(h->dcnt, 0, 8 * sizeof(int));
+    cudaMemset(h->derr, 0, 2 * sizeof(int));
+    h->herr[0] = h->herr[1] = 0;
     cudaMemset(h->dwnl, 0, h->plane * 2 * sizeof(double));
     cudaMemset(h->dwvr, 0, h->plane * 2 * sizeof(double));
     r = h->mixed ? alloc_fields(h, h->f32) : alloc_fields(h, h->f64);
@@ -1834,9 +1963,13 @@ int iw_destroy(iw_handle* h) {
     cudaFree(p);
   cudaFree(h->dcnt);
   cudaFree(h->dflag);
+  cudaFree(h->derr);
+  if (h->herr) cudaFreeHost(h->herr);
+  if (h->err_ev) cudaEventDestroy(h->err_ev);
   cudaFree(h->dcolorder);
   for (int k = 0; k < SYS_KINDS; ++k) {
     cudaFree(h->dtasks[k]);
+    cudaFree(h->dtasks2[k]);
     cudaFree(h->bi[k].ainv);
     cudaFree(h->bi[k].cvec);
     cudaFree(h->bi[k].dvec);
@@ -1860,29 +1993,32 @@ int iw_destroy(iw_handle* h) {
 }
 
 static int copy_level(iw_handle* h, int level, double* host, bool up_dir) {
-  // level 0 F, 1 Fn, 2 Fnm, 3 Sn, 4 Snm
+  // level 0 F, 1 Fn, 2 Fnm, 3 Sn, 4 Snm.  The host side is always FP64.  For
+  // FP32 fields each half field goes through a scratch field that holds
+  // ntot/2 doubles (the scratch is free between steps): a stream-ordered copy
+  // and a conversion kernel per half, no allocation, one wait at the end.
+  // With pinned host memory the copies run at full link speed.
   const size_t n = h->ntot;
   for (int q = 0; q < 4; ++q) {
-    void* dp;
     if (h->mixed) {
       float* const* L = level == 0 ? h->f32.F : level == 1 ? h->f32.Fn : level == 2 ? h->f32.Fnm : level == 3 ? h->f32.Sn : h->f32.Snm;
-      dp = L[q];
-      // convert through a scratch double buffer (F1 of the FP64 set is absent: use a temp)
-      double* tmp = nullptr;
-      CK(cudaMalloc(&tmp, n * sizeof(double)));
-      if (up_dir) {
-        CK(scopy(h, tmp, host + q * n, n * sizeof(double), cudaMemcpyHostToDevice));
-        k_convert<double, float><<<1024, 256, 0, h->st>>>(tmp, (float*)dp, n);
-      } else {
-        k_convert<float, double><<<1024, 256, 0, h->st>>>((const float*)dp, tmp, n);
-        CK(cudaStreamSynchronize(h->st));
-        CK(scopy(h, host + q * n, tmp, n * sizeof(double), cudaMemcpyDeviceToHost));
+      float* dp = L[q];
+      for (int half = 0; half < 2; ++half) {
+        const size_t o = half ? n / 2 : 0, c = half ? n - n / 2 : n / 2;
+        // c doubles fit in a scratch field of n floats when c <= n/2 + 1 (n is even: nxpp is)
+        double* tmp = (double*)h->f32.Y12[half];
+        if (up_dir) {
+          CK(cudaMemcpyAsync(tmp, host + q * n + o, c * sizeof(double), cudaMemcpyHostToDevice, h->st));
+          k_convert<double, float><<<1184, 256, 0, h->st>>>(tmp, dp + o, c);
+        } else {
+          k_convert<float, double><<<1184, 256, 0, h->st>>>(dp + o, tmp, c);
+          CK(cudaMemcpyAsync(host + q * n + o, tmp, c * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        }
+        CK(cudaGetLastError());
       }
-      CK(cudaStreamSynchronize(h->st));
-      cudaFree(tmp);
     } else {
       double* const* L = level == 0 ? h->f64.F : level == 1 ? h->f64.Fn : level == 2 ? h->f64.Fnm : level == 3 ? h->f64.Sn : h->f64.Snm;
-      dp = L[q];
+      double* dp = L[q];
       if (up_dir)
         CK(cudaMemcpyAsync(dp, host + q * n, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
       else
@@ -1903,6 +2039,7 @@ int iw_upload_state(iw_handle* h, const double* uvwt, const double* uvwt_n, cons
       int r = copy_level(h, l, const_cast<double*>(src[l]), true);
       if (r) return r;
     }
+  if (int r = clear_errors(h)) return r;
   h->t = t;
   h->istep = istep_done;
   h->cdt = 1.;
@@ -1934,16 +2071,24 @@ int iw_download_state(iw_handle* h, double* uvwt, double* uvwt_n, double* uvwt_n
 int iw_step(iw_handle* h) {
   if (!h) return set_err(IW_ERR_STATE, "null handle");
   cudaSetDevice(h->dev);
-  return h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64);
+  int r = poll_errors(h);
+  if (r) return r;
+  r = h->mixed ? full_step<float>(h, h->f32) : full_step<double>(h, h->f64);
+  post_errors(h);
+  return r;
 }
 
 int iw_run(iw_handle* h, int nsteps, int use_graph) {
   if (!h) return set_err(IW_ERR_STATE, "null handle");
   cudaSetDevice(h->dev);
+  int r = poll_errors(h);
+  if (r) return r;
   int s = 0;
   for (; s < nsteps && !(use_graph && graph_ready(h)); ++s) {
-    int r = step_dispatch(h);
+    r = step_dispatch(h);
     if (r) return r;
+    post_errors(h);
+    if ((r = poll_errors(h))) return r;
   }
   return run_graphs(&h, 1, nsteps - s);
 }
@@ -1952,6 +2097,28 @@ int iw_autotune(iw_handle* h, int* choices) {
   if (!h) return set_err(IW_ERR_STATE, "null handle");
   cudaSetDevice(h->dev);
   return h->mixed ? tune_impl<float>(h, h->f32, choices) : tune_impl<double>(h, h->f64, choices);
+}
+
+int iw_set_launch(iw_handle* h, int which, int value) {
+  if (!h) return set_err(IW_ERR_STATE, "null handle");
+  switch (which) {
+    case IW_LAUNCH_YTILE:
+      if (value != 0 && value != 2 && value != 4 && value != 8) return set_err(IW_ERR_CONFIG, "y tile: 0, 2, 4 or 8");
+      h->tune_ytx = value;
+      return IW_OK;
+    case IW_LAUNCH_STAGE_A:
+    case IW_LAUNCH_STAGE_E:
+      if (value < -1 || value > 1) return set_err(IW_ERR_CONFIG, "stage variant: -1, 0 or 1");
+      if (value >= 0 && !zop_bucket(h->N)) return set_err(IW_ERR_CONFIG, "register-column stages need N <= 33");
+      (which == IW_LAUNCH_STAGE_A ? h->tune_a : h->tune_e) = value;
+      return IW_OK;
+    case IW_LAUNCH_SOLVE:
+      if (value < 0 || value > 1) return set_err(IW_ERR_CONFIG, "solve variant: 0 or 1");
+      h->use_sys = value;
+      return IW_OK;
+    default:
+      return set_err(IW_ERR_CONFIG, "unknown launch choice");
+  }
 }
 
 int iw_ensemble_run(iw_handle* const* members, int n, int nsteps) {
@@ -1996,10 +2163,19 @@ int iw_step_coefs(iw_handle* h, const iw_coefs* c) {
   return iw_step(h);
 }
 
+int iw_set_coefs(iw_handle* h, const iw_coefs* c, double t) {
+  if (!h || !c) return set_err(IW_ERR_STATE, "null argument");
+  if (!(c->dt > 0)) return set_err(IW_ERR_CONFIG, "iw_set_coefs: dt must be positive");
+  h->c = Coefs{c->fac1, c->fac2, c->fac3, c->bdf1, c->bdf2, c->bdf3, c->bdfv, c->dt};
+  h->p.dt = c->dt;
+  h->t = t;
+  return IW_OK;
+}
+
 int iw_sync(iw_handle* h) {
   if (!h) return set_err(IW_ERR_STATE, "null handle");
   CK(cudaStreamSynchronize(h->st));
-  return IW_OK;
+  return sync_errors(h);
 }
 
 int iw_field_ptr(iw_handle* h, int f, void** dptr) {

@@ -51,8 +51,10 @@ using namespace iw;
 // errors
 // ---------------------------------------------------------------------------
 static thread_local std::string g_err;
+static thread_local int g_status = 0;
 static int set_err(int code, const std::string& msg) {
   g_err = msg;
+  g_status = code;
   return code;
 }
 #define CK(x)                                                                            \
@@ -106,7 +108,8 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageA(Geo g, const T* __restrict_
                                                      const T* __restrict__ F2_, const T* __restrict__ F3_,
                                                      T* __restrict__ O0, T* __restrict__ O1, T* __restrict__ O2,
                                                      T* __restrict__ O3, T* __restrict__ Z0, T* __restrict__ Z1,
-                                                     T* __restrict__ Z2, T* __restrict__ Z3, int proj) {
+                                                     T* __restrict__ Z2, T* __restrict__ Z3, int proj,
+                                                     int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int N = g.N;
   T* sD = (T*)smraw;             // N*N
@@ -125,6 +128,7 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageA(Geo g, const T* __restrict_
     T x = 0;
     if (act) {
       x = proj ? proj_val<T>(g, F, i, j, kk) : F[fidx<T>(g, i, j, kk)];
+      if (!isfinite(x)) err[0] = 1;  // the state of the last step holds a NaN or Inf
       if (q == 2 && j == 0 && i < 2) x = (T)0;  // wc(1,1,:) = 0, solver.f:66-69
       O[fidx<T>(g, i, j, kk)] = x;
     }
@@ -607,7 +611,8 @@ __global__ void __launch_bounds__(128) k_stageA_r(Geo g, const __grid_constant__
                                                    const T* __restrict__ F2_, const T* __restrict__ F3_,
                                                    T* __restrict__ O0, T* __restrict__ O1, T* __restrict__ O2,
                                                    T* __restrict__ O3, T* __restrict__ Z0, T* __restrict__ Z1,
-                                                   T* __restrict__ Z2, T* __restrict__ Z3, int proj) {
+                                                   T* __restrict__ Z2, T* __restrict__ Z3, int proj,
+                                                   int* __restrict__ err) {
   const int q = blockIdx.z, ks = blockIdx.y, N = g.N;
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.plane) return;
@@ -617,17 +622,20 @@ __global__ void __launch_bounds__(128) k_stageA_r(Geo g, const __grid_constant__
   T* Z = q == 0 ? Z0 : q == 1 ? Z1 : q == 2 ? Z2 : Z3;
   const bool wzero = q == 2 && j == 0 && i < 2;  // wc(1,1,:) = 0, solver.f:66-69
   T col[NM];
+  bool bad = false;
 #pragma unroll
   for (int k = 0; k < NM; ++k) {
     T x = 0;
     if (k < N) {
       const int kk = ks * N + k;
       x = proj ? proj_val<T>(g, F, i, j, kk) : F[(size_t)kk * g.plane + t];
+      bad |= !isfinite(x);
       if (wzero) x = (T)0;
       O[(size_t)kk * g.plane + t] = x;
     }
     col[k] = x;
   }
+  if (bad) err[0] = 1;  // the state of the last step holds a NaN or Inf
   const T fac = (T)g.hfac[ks];
 #pragma unroll
   for (int k1 = 0; k1 < NM; ++k1) {
@@ -1947,6 +1955,346 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
   }
 }
 
+// ===========================================================================
+// System-grouped solve.  One CTA per group of columns that share one system:
+// up to 4 u/v columns (16 right-hand sides) or 8 columns of w, rho or the
+// pressure (16 right-hand sides).  The system's distinct inverse blocks, its
+// left vectors and its interface matrix come into shared memory once per CTA
+// by bulk asynchronous copies (cp.async.bulk, completion counted on an
+// mbarrier) while the CTA gathers its columns, so every product reads both
+// operands from shared memory.  Thread t owns row t for all 16 right-hand
+// sides: one shared load of an inverse entry serves 16 multiply-adds, and the
+// right-hand sides are stored [row][16], so the 16 values of one row come as
+// eight 16-byte broadcasts.  The arithmetic (order of every sum, the RHS and
+// projection formulas) is the one of k_solve_cta, so both give the same bits.
+// Used for n <= 512 rows, filter folded into the inverses (or no filter),
+// no residual sweep and a system present; k_solve_cta takes the rest.
+// ===========================================================================
+constexpr int kSysR = 16;
+constexpr int kSysMaxRows = 512;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// wait for phase `ph` of an mbarrier, for at most `limit_ns`; false if it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t ph, uint64_t limit_ns) {
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(ph)
+        : "memory");
+    if (ok) return true;
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+}
+
+struct SysSmem {  // offsets (doubles) of the shared-memory regions of k_solve_sys
+  size_t a, l, m, b, rz, zz, d, total;
+};
+__host__ __device__ inline SysSmem sys_smem(int n, int N, int ns, int nb, bool dmat) {
+  SysSmem o;
+  const size_t m = 2 * (size_t)(ns - 1), m1 = m > 0 ? m : 1;
+  o.a = 0;
+  o.l = ((size_t)nb * N * N + 3) & ~(size_t)1;  // room for a copy that starts one double early
+  o.m = o.l + m * N;
+  o.b = o.m + m * m;
+  o.rz = o.b + (size_t)n * kSysR;
+  o.zz = o.rz + kSysR * m1;
+  o.d = o.zz + kSysR * m1;
+  o.total = o.d + (dmat ? (((size_t)N * N + 1) & ~(size_t)1) : 0);
+  return o;
+}
+
+// acc[r] = sum_c col[c*N] * b[(base + c)*16 + r]: one row of a block product
+__device__ __forceinline__ void row_product16(const double* col, const double* bb, int N, double* acc) {
+#pragma unroll
+  for (int r = 0; r < kSysR; ++r) acc[r] = 0.0;
+#pragma unroll 2
+  for (int c = 0; c < N; ++c) {
+    const double a = col[(size_t)c * N];
+    const double2* b2 = (const double2*)(bb + (size_t)c * kSysR);
+#pragma unroll
+    for (int q = 0; q < kSysR / 2; ++q) {
+      const double2 v = b2[q];
+      acc[2 * q] += a * v.x;
+      acc[2 * q + 1] += a * v.y;
+    }
+  }
+}
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+  typedef float2 t;
+};
+template <>
+struct Pair<double> {
+  typedef double2 t;
+};
+
+// role 0: u/v (4 RHS per column), 1: w, 2: rho, 3: pressure + projection
+template <typename T, int ROLE>
+__global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
+    Geo g, BlockInv bi, const Task* __restrict__ tasks, const int* __restrict__ col_order, T* __restrict__ F0,
+    T* __restrict__ F1, T* __restrict__ F2, double rdiv, int meanu, const double* __restrict__ meang,
+    const double* __restrict__ Dt, const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart,
+    int* __restrict__ err) {
+  typedef typename Pair<T>::t P2;
+  constexpr int R = kSysR;
+  constexpr int PER = ROLE == 0 ? 4 : 2;  // right-hand sides per column
+  constexpr int NC = R / PER;             // column slots
+  extern __shared__ __align__(16) double sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int cj[NC], cii[NC];
+  const Task tk = tasks[blockIdx.x];
+  const int n = g.nz, N = g.N, ns = g.ns, m = 2 * (ns - 1), nb = bi.nb;
+  const int tid = threadIdx.x;
+  const int s = tk.sys;
+  const SysSmem L = sys_smem(n, N, ns, nb, ROLE == 3);
+  double* sA = sm + L.a;
+  double* sL = sm + L.l;
+  double* sM = sm + L.m;
+  double* sb = sm + L.b;
+  double* srz = sm + L.rz;
+  double* szz = sm + L.zz;
+  double* sD = sm + L.d;
+  // the system's tables: one bulk copy each, all counted on one mbarrier
+  const uintptr_t ga = (uintptr_t)((const double*)bi.ainv + (size_t)s * nb * N * N);
+  const int offA = (int)((ga & 15u) >> 3);  // the copy starts one double early when ga is not 16-byte aligned
+  const uint32_t bytesA = (uint32_t)((((size_t)nb * N * N + offA) * 8 + 15) & ~(size_t)15);
+  const uint32_t bytesL = (uint32_t)((size_t)m * N * 8), bytesM = (uint32_t)((size_t)m * m * 8);
+  if (tid == 0) mbar_init(&bar, 1);
+  if (tid < NC) {
+    const int c = tid < tk.count ? col_order[tk.first + tid] : -1;
+    cj[tid] = c < 0 ? -1 : c / g.nxhp;
+    cii[tid] = c < 0 ? -1 : c % g.nxhp;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&bar, bytesA + bytesL + bytesM);
+    bulk_g2s(sA, (const void*)(ga - (uintptr_t)offA * 8), bytesA, &bar);
+    if (m > 0) {
+      bulk_g2s(sL, bi.lvec + (size_t)s * m * N, bytesL, &bar);
+      bulk_g2s(sM, bi.minv + (size_t)s * m * m, bytesM, &bar);
+    }
+  }
+  if (ROLE == 3)
+    for (int q = tid; q < N * N; q += blockDim.x) sD[q] = Dt[q];
+  const double eps = bi.sys[s].eps;
+  const double dt = g.dt;
+  const int k = tid;
+  const bool live = k < n;
+  const int ks = live ? k / N : 0, kk = k - ks * N;
+  // gather this row of every column: [row][16]
+  if (live) {
+    double v[R];
+#pragma unroll
+    for (int ci = 0; ci < NC; ++ci) {
+      P2 a = {0, 0}, b = {0, 0};
+      if (cj[ci] >= 0) {
+        const size_t p = fidx<T>(g, 2 * cii[ci], cj[ci], k);
+        if (ROLE == 3) {
+          a = *(const P2*)(F2 + p);
+        } else {
+          a = *(const P2*)(F0 + p);
+          if (ROLE == 0) b = *(const P2*)(F1 + p);
+        }
+      }
+      v[PER * ci] = (double)a.x;
+      v[PER * ci + 1] = (double)a.y;
+      if (ROLE == 0) {
+        v[PER * ci + 2] = (double)b.x;
+        v[PER * ci + 3] = (double)b.y;
+      }
+    }
+    if (ROLE != 3) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = -(-(v[r] / rdiv) * eps);
+    }
+    double2* d2 = (double2*)(sb + (size_t)k * R);
+#pragma unroll
+    for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(v[2 * q], v[2 * q + 1]);
+  }
+  const bool ok = mbar_wait(&bar, 0, 2000000000ull);
+  if (__syncthreads_or(!ok)) {  // the tables never arrived: report, let the copies finish, leave
+    if (tid == 0) err[1] = 1;
+    mbar_wait(&bar, 0, 2000000000ull);
+    return;
+  }
+  double acc[R];
+  if (ROLE == 3) {
+    // divergence of u*: i kx u* + i ky v* + (2/h) D w*; RHS = -(div/dt) eps
+    // plus the Neumann data at the walls (calcuvwt.f:87-229)
+    double rhs[R];
+    if (live) {
+      row_product16(sD + kk, sb + (size_t)ks * N * R, N, acc);
+      const double fac = g.hfac[ks];
+      const SysDesc sd = bi.sys[s];
+#pragma unroll
+      for (int ci = 0; ci < NC; ++ci) {
+        double vr = 0.0, vi = 0.0;
+        if (cj[ci] >= 0) {
+          const int j = cj[ci], ii = cii[ci];
+          const size_t pr = fidx<T>(g, 2 * ii, j, k);
+          const P2 u2 = *(const P2*)(F0 + pr), w2 = *(const P2*)(F1 + pr);
+          const double ur = (double)u2.x, ui = (double)u2.y;
+          const double wr = (double)w2.x, wi = (double)w2.y;
+          const double xw = g.xw[ii], yw = g.yw[j];
+          const double dr = -(xw * ui) - (yw * wi) + acc[2 * ci] * fac;
+          const double di = (xw * ur) + (yw * wr) + acc[2 * ci + 1] * fac;
+          vr = -((dr / dt) * eps);
+          vi = -((di / dt) * eps);
+          if (k == 0) {
+            const size_t p1 = (size_t)g.nxpp * j + 2 * ii;
+            vr -= (sd.tau1_bot * (wnl[p1] + wvr[p1])) * eps;
+            vi -= (sd.tau1_bot * (wnl[p1 + 1] + wvr[p1 + 1])) * eps;
+          }
+          if (k == n - 1) {
+            const size_t p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii;
+            vr += (sd.tau2_top * (wnl[p2] + wvr[p2])) * eps;
+            vi += (sd.tau2_top * (wnl[p2 + 1] + wvr[p2 + 1])) * eps;
+          }
+        }
+        rhs[2 * ci] = vr;
+        rhs[2 * ci + 1] = vi;
+      }
+    }
+    __syncthreads();  // every row of w* has been read
+    if (live) {
+      double2* d2 = (double2*)(sb + (size_t)k * R);
+#pragma unroll
+      for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(rhs[2 * q], rhs[2 * q + 1]);
+    }
+    __syncthreads();
+  }
+  // interface system: r_e = <lvec_e, b_blk(e)>, z = M^-1 r
+  if (m > 0) {
+    for (int q = tid; q < m * R; q += blockDim.x) {
+      const int r = q / m, e = q - r * m;
+      const int blk = e < ns - 1 ? e : e - (ns - 1) + 1;
+      const double* lv = sL + (size_t)e * N;
+      const double* sv = sb + (size_t)blk * N * R + r;
+      double a = 0.0;
+      for (int c = 0; c < N; ++c) a += lv[c] * sv[(size_t)c * R];
+      srz[q] = a;
+    }
+    __syncthreads();
+    for (int q = tid; q < m * R; q += blockDim.x) {
+      const int r = q / m, e = q - r * m;
+      const double* mr = sM + (size_t)e * m;
+      const double* rr = srz + r * m;
+      double z = 0.0;
+      for (int c = 0; c < m; ++c) z += mr[c] * rr[c];
+      szz[q] = z;
+    }
+    __syncthreads();
+  }
+  // x = A_ks^-1 b_ks - A_ks^-1 e_0 z_{ks-1} - A_ks^-1 e_{N-1} z_{ns-1+ks}
+  double x[R];
+  if (live) {
+    const double* col = sA + offA + (size_t)bi.bmap[ks] * N * N + kk;
+    row_product16(col, sb + (size_t)ks * N * R, N, acc);
+    const double p = ks >= 1 ? col[0] : 0.0;
+    const double q = ks <= ns - 2 ? col[(size_t)(N - 1) * N] : 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      double xv = acc[r];
+      if (ks >= 1) xv -= p * szz[r * m + ks - 1];
+      if (ks <= ns - 2) xv -= q * szz[r * m + ns - 1 + ks];
+      x[r] = xv;
+    }
+  }
+  if (ROLE != 3) {
+    if (!live) return;
+#pragma unroll
+    for (int ci = 0; ci < NC; ++ci) {
+      if (cj[ci] < 0) continue;
+      const size_t p = fidx<T>(g, 2 * cii[ci], cj[ci], k);
+      double a0 = x[PER * ci], a1 = x[PER * ci + 1];
+      if (ROLE == 0 && meanu && cii[ci] == 0 && cj[ci] == 0) {
+        a0 = meang[k] * a0;
+        a1 = meang[k] * a1;
+      }
+      P2 o;
+      o.x = (T)a0;
+      o.y = (T)a1;
+      *(P2*)(F0 + p) = o;
+      if (ROLE == 0) {
+        P2 o2;
+        o2.x = (T)x[PER * ci + 2];
+        o2.y = (T)x[PER * ci + 3];
+        *(P2*)(F1 + p) = o2;
+      }
+    }
+    return;
+  }
+  // pressure: phi into shared memory, (2/h) D phi, projection (calcuvwt.f:826-901)
+  __syncthreads();  // every row of the RHS has been read
+  if (live) {
+    double2* d2 = (double2*)(sb + (size_t)k * R);
+#pragma unroll
+    for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(x[2 * q], x[2 * q + 1]);
+  }
+  __syncthreads();
+  if (!live) return;
+  row_product16(sD + kk, sb + (size_t)ks * N * R, N, acc);
+  const double fac = g.hfac[ks];
+#pragma unroll
+  for (int ci = 0; ci < NC; ++ci) {
+    if (cj[ci] < 0) continue;
+    const int j = cj[ci], ii = cii[ci];
+    const size_t pr = fidx<T>(g, 2 * ii, j, k);
+    P2 zu, zv, zw;
+    if (k < kstart) {
+      zu.x = zu.y = (T)0;
+      *(P2*)(F0 + pr) = zu;
+      *(P2*)(F1 + pr) = zu;
+      *(P2*)(F2 + pr) = zu;
+      continue;
+    }
+    const double phr = x[2 * ci], phi = x[2 * ci + 1];
+    const P2 w2 = *(const P2*)(F2 + pr);
+    double wbr = 0, wbi = 0;
+    if (!(ii == 0 && j == 0)) {
+      wbr = (double)w2.x - dt * (acc[2 * ci] * fac);
+      wbi = (double)w2.y - dt * (acc[2 * ci + 1] * fac);
+    }
+    const double dtx = dt * g.xw[ii], dty = dt * g.yw[j];
+    const P2 u2 = *(const P2*)(F0 + pr), v2 = *(const P2*)(F1 + pr);
+    const double ur = (double)u2.x, ui = (double)u2.y, vr = (double)v2.x, vi = (double)v2.y;
+    zu.x = (T)(ur + dtx * phi);
+    zu.y = (T)(ui - dtx * phr);
+    zv.x = (T)(vr + dty * phi);
+    zv.y = (T)(vi - dty * phr);
+    zw.x = (T)wbr;
+    zw.y = (T)wbi;
+    *(P2*)(F0 + pr) = zu;
+    *(P2*)(F1 + pr) = zv;
+    *(P2*)(F2 + pr) = zw;
+  }
+}
+
 // Distinct blocks of each system into compact storage: out[s][b] = in[s][rep[b]],
 // with the Legendre filter folded in when L is given (out = L in, per column).
 struct BlockRep {
@@ -2196,8 +2544,12 @@ __global__ void k_filter_field(Geo g, T* F, int ifourier, int ilegen) {
 }
 
 // reductions for diagnostics: physical-space sums over i<nx, k>=1
+// Deterministic: a fixed grid and stride, fixed-order warp and block sums,
+// and each block adds its sum to its own slot part[blockIdx.x]; the host adds
+// the slots in order.  Repeated calls on the same state give the same bits.
 template <typename T>
-__global__ void k_reduce_sq(Geo g, const T* __restrict__ a, int kmin, double* out) {
+__global__ void k_reduce_sq(Geo g, const T* __restrict__ a, int kmin, double* part) {
+  __shared__ double ws[32];
   double s = 0;
   long total = (long)g.nx * g.ny * (g.nz - kmin);
   for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
@@ -2209,7 +2561,13 @@ __global__ void k_reduce_sq(Geo g, const T* __restrict__ a, int kmin, double* ou
     s += x * x;
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += ws[w];
+    part[blockIdx.x] += b;
+  }
 }
 
 // maxcalc statistics of one physical field (various.f:665-987 without the

@@ -88,8 +88,14 @@ class Solver:
         ptrs = [None if a is None else _pd(a) for a in arrs]
         _lib.check(_lib.lib().iw_upload_state(self.h, *ptrs, t, istep))
 
-    def state(self, level: int = 0) -> np.ndarray:
-        out = np.zeros(self.shape)
+    def state(self, level: int = 0, out: np.ndarray = None) -> np.ndarray:
+        """Download one time level (0: n, 1: n-1, 2: n-2, 3/4: NL terms at
+        n-1/n-2) as FP64, into `out` when given (C-contiguous float64 of
+        self.shape, e.g. pinned host memory)."""
+        if out is None:
+            out = np.zeros(self.shape)
+        elif out.dtype != np.float64 or out.shape != self.shape or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be C-contiguous float64 of shape %s" % (self.shape,))
         ptrs = [None] * 5
         ptrs[level] = _pd(out)
         _lib.check(_lib.lib().iw_download_state(self.h, *ptrs))
@@ -146,10 +152,17 @@ class Solver:
     def autotune(self) -> dict:
         """Time this step's launch candidates and keep the fastest (y-tile
         width, stage A / stage E variant); the state is not changed."""
-        ch = (C.c_int * 3)()
+        ch = (C.c_int * 4)()
         _lib.check(_lib.lib().iw_autotune(self.h, ch))
         names = {1: "register", 0: "tiled", -1: "n/a"}
-        return {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]]}
+        return {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]],
+                "solve": "system-grouped" if ch[3] else "per-task"}
+
+    LAUNCH = {"y_tile": 0, "stage_a": 1, "stage_e": 2, "solve": 3}
+
+    def set_launch(self, which: str, value: int):
+        """Set one launch choice directly (iw_set_launch)."""
+        _lib.check(_lib.lib().iw_set_launch(self.h, self.LAUNCH[which], int(value)))
 
     def run(self, n: int, graph: bool = True):
         """n steps; with graph=True the invariant steady-state step is replayed
@@ -159,6 +172,11 @@ class Solver:
     def step_coefs(self, fac, bdf, bdfv, dt):
         c = IwCoefs(fac[0], fac[1], fac[2], bdf[0], bdf[1], bdf[2], bdfv, dt)
         _lib.check(_lib.lib().iw_step_coefs(self.h, C.byref(c)))
+
+    def set_coefs(self, fac, bdf, bdfv, dt, t):
+        """COMMON /ab/ /bdf/ values, dt and t for convec_/calcuvwt_ (iw_set_coefs)."""
+        c = IwCoefs(fac[0], fac[1], fac[2], bdf[0], bdf[1], bdf[2], bdfv, dt)
+        _lib.check(_lib.lib().iw_set_coefs(self.h, C.byref(c), t))
 
     def sync(self):
         _lib.check(_lib.lib().iw_sync(self.h))

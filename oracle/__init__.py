@@ -235,6 +235,12 @@ class Oracle:
         lib().orc_filter3d(self.h, _p(f), ifourier, ilegen)
         return f
 
+    def filter_legenpen(self, fin: np.ndarray) -> np.ndarray:
+        fin = np.ascontiguousarray(fin, dtype=np.float64)
+        out = np.zeros_like(fin)
+        lib().orc_filter_legenpen(self.h, _p(fin), _p(out))
+        return out
+
     def interface_avg3d(self, f: np.ndarray):
         f = np.array(f, dtype=np.float64, order="C")
         ic = lib().orc_interface_avg3d(self.h, _p(f))
