@@ -409,9 +409,10 @@ void bandlu_solve_(const double *ain, double *xr, double *xi,
  *            back; overwritten by the solutions
  *   stream   cudaStream_t to order the work on (NULL: the default stream); the
  *            call returns once the work is enqueued
- * Limits: nz <= 3072 and (3*nzloc+1)*nz <= 131072.  Larger systems are refused
- * with IW_ERR_CONFIG and a message in iw_last_error().  No handle is needed;
- * the current device is used.
+ * Limits: nzloc in [2, 64], nsubd in [1, 64] and (3*nzloc+1)*nzloc*nsubd <=
+ * 131072 (the band storage), which allows at most nz = 1600 (nzloc = 25,
+ * nsubd = 64).  Other systems are refused with IW_ERR_CONFIG and a message in
+ * iw_last_error().  No handle is needed; the current device is used.
  * Band storage, pivots and status sit in one fixed device array of about 1.06 MB
  * that each GPU loading this library holds until the process exits.  Every call
  * on a device uses that same array; each call rewrites all of it that it reads.
@@ -419,7 +420,9 @@ void bandlu_solve_(const double *ain, double *xr, double *xi,
  * corrupt each other: order them, for example on one stream.
  * The first call on each device also does a one-time set-up (it looks up the
  * device address of the array); make that first call before any stream capture
- * begins.  As in bandlu_solve_ and the reference, a zero pivot is not reported. */
+ * begins.  The address is kept for the life of the process: do not call this
+ * after a cudaDeviceReset of that device.  As in bandlu_solve_ and the
+ * reference, a zero pivot is not reported. */
 int iw_bandlu_solve_noalloc(const double *ain_dev, double *x_dev, int nzloc,
                             int nsubd, int nrhs, void *stream);
 

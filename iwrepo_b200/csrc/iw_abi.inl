@@ -628,7 +628,10 @@ int iw_helm_solve_batched(iw_handle* h, const double* lam_dev, int ncol, int ifb
 // ---------------------------------------------------------------------------
 namespace {
 constexpr size_t kNoAllocBand = 131072;  // band storage: (3 nzloc + 1) * nz doubles at most
-constexpr int kNoAllocMaxN = 3072;       // nz at most (two right-hand sides stay within 48 KB of shared memory)
+// nz bound of the pivot storage and of the solve's shared memory (two right-hand
+// sides stay within 48 KB); the band bound above is the tighter one: with
+// nzloc, nsubd <= 64 it allows nz <= 1600
+constexpr int kNoAllocMaxN = 3072;
 constexpr size_t kNoAllocPivot = kNoAllocBand;                  // pivots: kNoAllocMaxN ints
 constexpr size_t kNoAllocInfo = kNoAllocPivot + kNoAllocMaxN / 2;  // status word
 constexpr size_t kNoAllocSys = kNoAllocInfo + 8;               // system descriptor
@@ -672,7 +675,7 @@ int iw_bandlu_solve_noalloc(const double* ain_dev, double* x_dev, int nzloc, int
   if (nrhs != 1 && nrhs != 2) return set_err(IW_ERR_CONFIG, "iw_bandlu_solve_noalloc: nrhs must be 1 or 2");
   const int n = nzloc * nsubd, ldab = 3 * nzloc + 1;
   if (n > kNoAllocMaxN || (size_t)ldab * n > kNoAllocBand)
-    return set_err(IW_ERR_CONFIG, "iw_bandlu_solve_noalloc: system exceeds the fixed scratch: need nzloc*nsubd <= 3072 and "
+    return set_err(IW_ERR_CONFIG, "iw_bandlu_solve_noalloc: system exceeds the fixed scratch: need "
                                   "(3*nzloc+1)*nzloc*nsubd <= 131072, got nz=" +
                                       std::to_string(n) + ", band " + std::to_string((size_t)ldab * n));
   int dev = 0;

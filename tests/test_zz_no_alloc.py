@@ -50,6 +50,40 @@ def test_bandlu_noalloc_matches_bandlu_solve_on_consecutive_calls():
         assert np.linalg.norm(A @ got[:n] - x1) / np.linalg.norm(x1) < 1e-12
 
 
+@pytest.mark.parametrize("nzloc,nsubd,nrhs", [(9, 3, 1), (25, 8, 2), (25, 8, 1), (25, 64, 2)])
+def test_bandlu_noalloc_at_c1_size_and_at_its_limit(nzloc, nsubd, nrhs):
+    """C1's 8 x 25 system, one and two right-hand sides, and the largest
+    system the scratch takes (nzloc = 25, nsubd = 64: nz = 1600, band
+    (3*25+1)*1600 = 121,600 of 131,072 doubles): bit-equal to bandlu_solve_
+    on two consecutive calls, residual below 1e-11."""
+    import torch
+    import iwrepo_b200 as iw
+    from iwrepo_b200 import _lib
+    from oracle import Oracle
+
+    cfg = cf.Config(nx=4, ny=2, nzloc=nzloc, nsubd=nsubd, dt=1e-3).validate()
+    n = cfg.nz
+    s, o = iw.Solver(cfg), Oracle(cfg)
+    L = _lib.lib()
+    rng = np.random.default_rng(nzloc * 100 + nsubd)
+    for eps, bot, top in [(2e-4, 0, 1), (0.3, 1, 1)]:
+        A = o.penalty_matrix(eps, bot, top)
+        x1, x2 = rng.standard_normal(n), rng.standard_normal(n)
+        ref_r, ref_i = s.bandlu_solve(A, x1, x2)
+        a_dev = torch.from_numpy(np.ascontiguousarray(A.T).ravel()).cuda()
+        x_dev = torch.from_numpy(np.concatenate([x1, x2][:nrhs])).cuda()
+        torch.cuda.synchronize()
+        rc = L.iw_bandlu_solve_noalloc(_ptr(a_dev), _ptr(x_dev), nzloc, nsubd, nrhs, None)
+        assert rc == 0, L.iw_last_error()
+        torch.cuda.synchronize()
+        got = x_dev.cpu().numpy()
+        assert np.array_equal(got[:n], ref_r)
+        if nrhs == 2:
+            assert np.array_equal(got[n:], ref_i)
+        assert np.linalg.norm(A @ got[:n] - x1) / np.linalg.norm(x1) < 1e-11
+    s.close()
+
+
 def test_bandlu_noalloc_refuses_systems_beyond_its_scratch():
     import torch
     from iwrepo_b200 import _lib
@@ -57,9 +91,10 @@ def test_bandlu_noalloc_refuses_systems_beyond_its_scratch():
     L = _lib.lib()
     a_dev = torch.zeros(4, dtype=torch.float64, device="cuda")
     x_dev = torch.zeros(4, dtype=torch.float64, device="cuda")
-    # nz = 64*64 = 4096 > 3072: refused before anything is launched
-    rc = L.iw_bandlu_solve_noalloc(_ptr(a_dev), _ptr(x_dev), 64, 64, 2, None)
-    assert rc == IW_ERR_CONFIG
-    assert b"fixed scratch" in L.iw_last_error()
+    # band (3*64+1)*64*64 and (3*26+1)*26*64 exceed 131,072: refused before anything is launched
+    for nzloc, nsubd in ((64, 64), (26, 64)):
+        rc = L.iw_bandlu_solve_noalloc(_ptr(a_dev), _ptr(x_dev), nzloc, nsubd, 2, None)
+        assert rc == IW_ERR_CONFIG
+        assert b"fixed scratch" in L.iw_last_error()
     rc = L.iw_bandlu_solve_noalloc(_ptr(a_dev), _ptr(x_dev), 9, 3, 3, None)
     assert rc == IW_ERR_CONFIG
