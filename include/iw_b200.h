@@ -293,14 +293,15 @@ int iw_run(iw_handle *h, int nsteps, int use_graph);
  * are built if no step has built them yet).  The stage variants differ only
  * in the order of floating-point sums; the solve variants give the same bits.
  * choices (optional, 4 ints): the y-tile width; for stage A and stage E
- * 1 = register-column, 0 = tiled, -1 = not applicable; the solve variant
- * (1 = system-grouped, 0 = per task). */
+ * 1 = register-column, 0 = tiled, -1 = not applicable (stage E also 2 =
+ * register-column split in two kernels, u* and then the filter); the solve
+ * variant (1 = system-grouped, 0 = per task). */
 int iw_autotune(iw_handle *h, int *choices);
 
 /* Not in the reference.  Sets one launch choice of iw_autotune directly. */
 #define IW_LAUNCH_YTILE 0   /* 0 (size heuristic), 2, 4 or 8 */
 #define IW_LAUNCH_STAGE_A 1 /* -1 (size heuristic), 0 tiled, 1 register-column */
-#define IW_LAUNCH_STAGE_E 2 /* as stage A */
+#define IW_LAUNCH_STAGE_E 2 /* as stage A, or 2: register-column split (u*, then the filter) */
 #define IW_LAUNCH_SOLVE 3   /* 1 system-grouped (default), 0 per task */
 int iw_set_launch(iw_handle *h, int which, int value);
 

@@ -438,13 +438,39 @@ int iw_init_mode1(iw_handle* h, double A, double anoise, uint64_t seed) {
         }
   }
   std::vector<double> zero(4 * h->ntot, 0.0);
-  int r = iw_upload_state(h, st.data(), zero.data(), zero.data(), zero.data(), zero.data(), 0.0, 0);
+  int r = iw_upload_state(h, h->mixed ? nullptr : st.data(), zero.data(), zero.data(), zero.data(), zero.data(), 0.0, 0);
   if (r) return r;
-  for (int q = 0; q < 4; ++q) {
-    if (h->mixed)
-      horfft_dev<float>(h, h->f32, h->f32.F[q], -1, nz);
-    else
-      horfft_dev<double>(h, h->f64, h->f64.F[q], -1, nz);
+  if (h->mixed) {
+    // The forward transform of the initial fields runs in FP64 and only the
+    // spectral result is rounded to FP32, coefficient by coefficient.  An FP32
+    // transform would spread its rounding (relative to the wave's amplitude)
+    // over every (kx, ky) mode of u and w, and the first projection would
+    // carry that divergent noise into v, a field about 1000 times smaller.
+    FieldSet<double> tmp;
+    typedef double2 C;
+    const int M = nx / 2;
+    auto wm = twiddles<C>(M, M);
+    auto wn = twiddles<C>(nx, M + 1);
+    auto wy = twiddles<C>(ny, ny);
+    if (up(h, &tmp.Wm, wm) || up(h, &tmp.Wn, wn) || up(h, &tmp.Wy, wy)) return IW_ERR_NOMEM;
+    DBuf d(h->ntot);
+    if (!d.p) return set_err(IW_ERR_NOMEM, "iw_init_mode1: no memory for the FP64 transform");
+    for (int q = 0; q < 4 && r == 0; ++q) {
+      if (cudaMemcpyAsync(d.p, st.data() + (size_t)q * h->ntot, h->ntot * sizeof(double), cudaMemcpyHostToDevice,
+                          h->st) != cudaSuccess) {
+        r = set_err(IW_ERR_CUDA, "iw_init_mode1: copy of the initial field");
+        break;
+      }
+      horfft_dev<double>(h, tmp, d.p, -1, nz);
+      k_convert<double, float><<<1184, 256, 0, h->st>>>(d.p, h->f32.F[q], h->ntot);
+    }
+    cudaStreamSynchronize(h->st);
+    cudaFree(tmp.Wm);
+    cudaFree(tmp.Wn);
+    cudaFree(tmp.Wy);
+    if (r) return r;
+  } else {
+    for (int q = 0; q < 4; ++q) horfft_dev<double>(h, h->f64, h->f64.F[q], -1, nz);
   }
   CK(cudaMemsetAsync(h->dwnl, 0, h->plane * 2 * sizeof(double), h->st));
   CK(cudaMemsetAsync(h->dwvr, 0, h->plane * 2 * sizeof(double), h->st));

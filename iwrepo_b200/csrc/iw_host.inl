@@ -294,6 +294,10 @@ struct FieldSet {
   T* X11[11] = {0};
   T* B8[8] = {0};
   T* G = 0;  // interface planes
+  // FP32 fields: the jump f(k) - f(k-1) across every interface of the final
+  // u, v, w, rho of a step, [field][interface][plane], formed in FP64 by the
+  // solve kernels before their results are rounded (see k_iface_rows)
+  T* J = 0;
   typename cplx_t<T>::type *Wm = 0, *Wn = 0, *Wy = 0;
 };
 
@@ -518,6 +522,10 @@ static int alloc_fields(iw_handle* h, FieldSet<T>& fs) {
   for (int q = 0; q < 8; ++q)
     if (dalloc(h, &fs.B8[q], n)) return IW_ERR_NOMEM;
   if (h->ns > 1 && dalloc(h, &fs.G, h->plane * 16 * (size_t)(h->ns - 1))) return IW_ERR_NOMEM;
+  if (sizeof(T) == 4 && h->ns > 1) {
+    if (dalloc(h, &fs.J, h->plane * 4 * (size_t)(h->ns - 1))) return IW_ERR_NOMEM;
+    cudaMemset(fs.J, 0, h->plane * 4 * (size_t)(h->ns - 1) * sizeof(T));
+  }
   typedef typename cplx_t<T>::type C;
   int M = h->nx / 2;
   auto wm = twiddles<C>(M, M);
@@ -535,6 +543,7 @@ static void free_fields(FieldSet<T>& fs) {
   for (int q = 0; q < 11; ++q) cudaFree(fs.X11[q]);
   for (int q = 0; q < 8; ++q) cudaFree(fs.B8[q]);
   cudaFree(fs.G);
+  cudaFree(fs.J);
   cudaFree(fs.Wm);
   cudaFree(fs.Wn);
   cudaFree(fs.Wy);
@@ -987,12 +996,22 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   const dim3 rgrid((unsigned)((h->plane + 127) / 128), (unsigned)h->ns, 4);
   // The register-column stage E holds two columns per thread; past these sizes
   // its register count costs more occupancy than the tiled kernel loses.
+  // The split variant (tune_e = 2) runs the same work as two register-column
+  // kernels with one column each: u* first, then the filter in place.
   const int emax = sizeof(T) == 4 ? 25 : 17;
-  const bool reg = h->tune_e < 0 ? h->N <= emax : h->tune_e == 1;
+  const bool reg = h->tune_e < 0 ? h->N <= emax : h->tune_e >= 1;
+  const bool split = h->tune_e == 2;
   switch (reg ? zop_bucket(h->N) : 0) {
 #define IW_ECASE(NM)                                                                          \
   case NM:                                                                                    \
-    k_stageE_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, make_zop<T, NM>(h));         \
+    if (split) {                                                                              \
+      const ZOp<T, NM> op = make_zop<T, NM>(h);                                               \
+      k_stageE_r1<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, op);                     \
+      if (a.filter)                                                                           \
+        k_filter_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], op); \
+    } else {                                                                                  \
+      k_stageE_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, make_zop<T, NM>(h));       \
+    }                                                                                         \
     return;
     IW_ECASE(9)
     IW_ECASE(17)
@@ -1367,6 +1386,8 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3);
   const size_t smsys = lay.total * sizeof(double);
   const bool grouped = h->use_sys && h->nz <= kSysMaxRows && (!cpen || fold) && smsys <= 200 * 1024;
+  // FP32 fields: where the final u, v, w, rho leave their interface jumps
+  T* jmp = (fs.J && role != 3) ? fs.J + (size_t)(role == 0 ? 0 : role == 1 ? 2 : 3) * (h->ns - 1) * h->plane : nullptr;
   const int nend = grouped ? std::max(h->nold[kind], nref) : nt;
   if (grouped && h->ntask2[kind] > 0) {
     const int nthr = (h->nz + 31) / 32 * 32;
@@ -1377,7 +1398,7 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
     cudaFuncSetAttribute(k_solve_sys<T, RL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smsys);           \
     k_solve_sys<T, RL><<<h->ntask2[kind], nthr, smsys, h->st>>>(g, bi, h->dtasks2[kind], h->dcolorder, F0, F1, F2, \
                                                                rd, meanu, mg, h->dDt, h->dwnl, h->dwvr, kstart,   \
-                                                               h->derr);                                          \
+                                                               h->derr, jmp);                                     \
   } while (0)
     if (role == 0)
       IW_SYS_LAUNCH(0);
@@ -1402,7 +1423,7 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
     }
     k_solve_cta<T, R><<<cnt, kSolveThreads, sm, h->st>>>(geo(h), b2, solve_tabs(h, kind), h->dtasks[kind] + t0, F0, F1,
                                                           F2, rd, role, cp, meanu, part == 0 ? 1 : 0, h->dDt, h->dD2t,
-                                                          h->dLt, h->dzh, h->dwnl, h->dwvr, kstart);
+                                                          h->dLt, h->dzh, h->dwnl, h->dwvr, kstart, jmp);
   }
 }
 
@@ -1436,12 +1457,16 @@ static int calcuvwt_impl(iw_handle* h, FieldSet<T>& fs, int cpen) {
       mark(h, 7 + role);
     }
   } else {
+    T* J = fs.J;
+    const size_t jf = J ? (size_t)(h->ns - 1) * h->plane : 0;
     k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_U), fs.F[0], fs.F[1], xnudt, 0, cpen,
-                                                  h->p.meanu_damping);
+                                                  h->p.meanu_damping, J);
     mark(h, 7);
-    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_W), fs.F[2], fs.F[2], xnudt, 1, cpen, 0);
+    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_W), fs.F[2], fs.F[2], xnudt, 1, cpen, 0,
+                                                  J ? J + 2 * jf : nullptr);
     mark(h, 8);
-    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_T), fs.F[3], fs.F[3], dtk, 2, cpen, 0);
+    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_T), fs.F[3], fs.F[3], dtk, 2, cpen, 0,
+                                                  J ? J + 3 * jf : nullptr);
     mark(h, 9);
   }
   return 0;
@@ -1458,7 +1483,8 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
   }
   const int ng = nf * (h->ns - 1);  // plane groups (field, interface)
   const long tot = (long)h->plane * ng * 4;  // 4 planes per group
-  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 0);
+  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 0,
+                                                                       fs.J);
   {
     YJobs<T> jb;
     memset(&jb, 0, sizeof jb);
@@ -1481,7 +1507,8 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
   }
   long total = (long)h->ny * h->nz * nf;
   k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
-  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1);
+  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1,
+                                                                       fs.J);
   return 0;
 }
 
@@ -1577,15 +1604,19 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
   // stage A and stage E variants
   int besta = -1, beste = -1;
   if (zop_bucket(h->N)) {
-    float ta[2], te[2];
-    for (int v = 0; v < 2; ++v) {
-      h->tune_a = v;
-      ta[v] = timeit([&] { launch_stageA<T>(h, ts, 1); });
+    float ta[2], te[3];
+    for (int v = 0; v < 3; ++v) {
+      if (v < 2) {
+        h->tune_a = v;
+        ta[v] = timeit([&] { launch_stageA<T>(h, ts, 1); });
+      }
       h->tune_e = v;
       te[v] = timeit([&] { launch_stageE<T>(h, ts); });
     }
     besta = ta[1] <= ta[0] ? 1 : 0;
-    beste = te[1] <= te[0] ? 1 : 0;
+    beste = 0;
+    for (int v = 1; v < 3; ++v)
+      if (te[v] < te[beste]) beste = v;
   }
   h->tune_a = besta;
   h->tune_e = beste;
@@ -2108,7 +2139,8 @@ int iw_set_launch(iw_handle* h, int which, int value) {
       return IW_OK;
     case IW_LAUNCH_STAGE_A:
     case IW_LAUNCH_STAGE_E:
-      if (value < -1 || value > 1) return set_err(IW_ERR_CONFIG, "stage variant: -1, 0 or 1");
+      if (value < -1 || value > (which == IW_LAUNCH_STAGE_E ? 2 : 1))
+        return set_err(IW_ERR_CONFIG, "stage variant: -1, 0, 1 (or 2 for stage E)");
       if (value >= 0 && !zop_bucket(h->N)) return set_err(IW_ERR_CONFIG, "register-column stages need N <= 33");
       (which == IW_LAUNCH_STAGE_A ? h->tune_a : h->tune_e) = value;
       return IW_OK;

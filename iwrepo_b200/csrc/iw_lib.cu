@@ -734,6 +734,103 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
   }
 }
 
+// Split K_E, first half: everything of k_stageE_r but the filter; writes u*.
+template <typename T, int NM>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_stageE_r1(Geo g, EArgs<T> a, Coefs c, const __grid_constant__ ZOp<T, NM> op) {
+  const int q = blockIdx.z, ks = blockIdx.y, N = g.N;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.plane) return;
+  const int i = (int)(t % g.nxpp), j = (int)(t / g.nxpp);
+  T zc[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k) zc[k] = k < N ? a.Z[q][(size_t)(ks * N + k) * g.plane + t] : (T)0;
+  const T fac = (T)g.hfac[ks];
+  const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
+  const T* Bq = a.B[q];
+  const T* Snq = a.Snold[q];
+  const T* F1q = a.F1[q];
+  const T* Fnq = a.Fn[q];
+  T* Snmq = a.Snm_w[q];
+  T* Fnmq = a.Fnm_w[q];
+  // Rolling window: the inputs of row k1+PF are loaded before the stores of
+  // row k1, so the loads of several rows are in flight at once (the pointers
+  // are not known to be distinct, so the compiler would not hoist them).
+  constexpr int PF = 4;
+  T wb[PF], wsn[PF], wsnm[PF], wf2[PF], wfn[PF], wfnm[PF];
+#pragma unroll
+  for (int k1 = 0; k1 < PF; ++k1) {
+    if (k1 < N) {
+      const int kk = ks * N + k1;
+      const size_t p = (size_t)kk * g.plane + t;
+      wb[k1] = Bq[p];
+      wsn[k1] = Snq[p];
+      wsnm[k1] = Snmq[p];
+      wf2[k1] = proj_val<T>(g, F1q, i, j, kk);
+      wfn[k1] = Fnq[p];
+      wfnm[k1] = Fnmq[p];
+    }
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1) {
+    if (k1 < N) {
+      T fsv;
+      const int sl = k1 % PF;
+      const T b = wb[sl], sn = wsn[sl], snm = wsnm[sl], F2 = wf2[sl], fn = wfn[sl], fnm = wfnm[sl];
+      if (k1 + PF < NM && k1 + PF < N) {
+        const int kn = ks * N + k1 + PF;
+        const size_t pn = (size_t)kn * g.plane + t;
+        wb[sl] = Bq[pn];
+        wsn[sl] = Snq[pn];
+        wsnm[sl] = Snmq[pn];
+        wf2[sl] = proj_val<T>(g, F1q, i, j, kn);
+        wfn[sl] = Fnq[pn];
+        wfnm[sl] = Fnmq[pn];
+      }
+      const int kk = ks * N + k1;
+      const size_t p = (size_t)kk * g.plane + t;
+      T s = 0;
+#pragma unroll
+      for (int k2 = 0; k2 < NM; ++k2) s += op.D[k1 * NM + k2] * zc[k2];
+      const T S = b + s * fac;
+      if (q == 2 && ((kk == 0) || (kk == g.nz - 1)))
+        a.wnl[t + (kk == 0 ? 0 : g.plane)] = (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
+      const T se = f1 * S + f2 * sn + f3 * snm;
+      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
+      Snmq[p] = S;
+      Fnmq[p] = F2;
+      a.F[q][p] = fsv;  // u* before the filter (k_filter_r applies it)
+    }
+  }
+}
+
+// Second half of the split K_E: the Fourier x Legendre filter of u*
+// (filter_3dlegenfourier, filtering.f:811-983) in place, one column per
+// thread held in FP64 registers, (L - I) from the constant bank:
+// F <- cf g with g = f + (L - I) f, the same arithmetic as the combined kernel.
+template <typename T, int NM>
+__global__ void __launch_bounds__(128, 5) k_filter_r(Geo g, T* F0, T* F1_, T* F2_, T* F3_,
+                                                  const __grid_constant__ ZOp<T, NM> op) {
+  const int q = blockIdx.z, ks = blockIdx.y, N = g.N;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.plane) return;
+  const int i = (int)(t % g.nxpp), j = (int)(t / g.nxpp);
+  T* F = q == 0 ? F0 : q == 1 ? F1_ : q == 2 ? F2_ : F3_;
+  double f[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k) f[k] = k < N ? (double)F[(size_t)(ks * N + k) * g.plane + t] : 0.0;
+  const double cfm1 = g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0;
+#pragma unroll
+  for (int k1 = 0; k1 < NM; ++k1) {
+    if (k1 < N) {
+      double s = 0;
+#pragma unroll
+      for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * f[k2];
+      const double gv = f[k1] + s;
+      F[(size_t)(ks * N + k1) * g.plane + t] = (T)(gv + cfm1 * gv);
+    }
+  }
+}
+
 // rotational viscous term at the walls (solver.f:318-394, rotvisc 1210-1253):
 // wviscrot = -nu * (fac1 rot(n) + fac2 rot(n-1) + fac3 rot(n-2)),
 // rot = (kx^2+ky^2) w + i kx du/dz + i ky dv/dz at k0.
@@ -1153,7 +1250,7 @@ struct SolveTabs {
 // role 1: w, role 2: rho.  Warp per column.
 template <typename T>
 __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ F1, double rdiv, int role, int cpen,
-                       int meanu) {
+                       int meanu, T* __restrict__ jmp) {
   extern __shared__ __align__(16) double sm[];
   const int warps = blockDim.x / 32;
   const int wid = threadIdx.x / 32, lane = threadIdx.x & 31;
@@ -1173,6 +1270,12 @@ __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ 
       F0[fidx<T>(g, 2 * ii, j, k)] = 0;
       F0[fidx<T>(g, 2 * ii + 1, j, k)] = 0;
     }
+    if (jmp)
+      for (int e = lane; e < g.ns - 1; e += 32) {
+        const size_t pe = (size_t)e * g.plane + 2 * ii + (size_t)g.nxpp * j;
+        jmp[pe] = 0;
+        jmp[pe + 1] = 0;
+      }
     return;
   }
   const SysDesc sd = tb.sys[s];
@@ -1211,6 +1314,17 @@ __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ 
       if (role == 0 && r < 2 && lzero && meanu) x = rmul(tb.meang[k], x);
       F[fidx<T>(g, 2 * ii + part, j, k)] = (T)x;
     }
+    if (jmp)  // FP32 fields: the jumps across the interfaces, from the FP64 results
+      for (int e = lane; e < g.ns - 1; e += 32) {
+        const int k = (e + 1) * N;
+        double x1 = b[(size_t)r * n + k], x0 = b[(size_t)r * n + k - 1];
+        if (role == 0 && r < 2 && lzero && meanu) {
+          x1 = rmul(tb.meang[k], x1);
+          x0 = rmul(tb.meang[k - 1], x0);
+        }
+        jmp[(size_t)e * g.plane + 2 * ii + part + (size_t)g.nxpp * j + (size_t)(r >> 1) * (g.ns - 1) * g.plane] =
+            (T)(x1 - x0);
+      }
   }
 }
 
@@ -1783,7 +1897,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
     Geo g, BlockInv bi, SolveTabs tb, const Task* __restrict__ tasks, T* __restrict__ F0, T* __restrict__ F1,
     T* __restrict__ F2, double rdiv, int role, int cpen, int meanu, int refine, const double* __restrict__ Dt,
     const double* __restrict__ D2t, const double* __restrict__ Lt, const double* __restrict__ zh,
-    const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart) {
+    const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart, T* __restrict__ jmp) {
   extern __shared__ __align__(16) double sm[];
   __shared__ int cj[R], cii[R];
   const Task tk = tasks[blockIdx.x];
@@ -1805,11 +1919,18 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
   }
   __syncthreads();
   if (s < 0 && role != 3) {  // w of the (0,0) mode is zero
-    for (int ci = 0; ci < ncolt; ++ci)
+    for (int ci = 0; ci < ncolt; ++ci) {
       for (int k = tid; k < n; k += kSolveThreads) {
         F0[fidx<T>(g, 2 * cii[ci], cj[ci], k)] = 0;
         F0[fidx<T>(g, 2 * cii[ci] + 1, cj[ci], k)] = 0;
       }
+      if (jmp)
+        for (int e = tid; e < ns - 1; e += kSolveThreads) {
+          const size_t pe = (size_t)e * g.plane + 2 * cii[ci] + (size_t)g.nxpp * cj[ci];
+          jmp[pe] = 0;
+          jmp[pe + 1] = 0;
+        }
+    }
     return;
   }
   const double* res = x;
@@ -1952,6 +2073,20 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
         F[fidx<T>(g, 2 * cii[ci] + (rr & 1), cj[ci], k)] = (T)v;
       }
     }
+    if (jmp)  // FP32 fields: the jumps across the interfaces, from the FP64 results
+      for (int q = tid; q < (ns - 1) * R; q += kSolveThreads) {
+        const int e = q / R, r = q - e * R;
+        const int ci = r / per, rr = r - ci * per;
+        if (cj[ci] < 0) continue;
+        const int k = (e + 1) * N;
+        double v1 = res[(size_t)r * n + k], v0 = res[(size_t)r * n + k - 1];
+        if (role == 0 && rr < 2 && meanu && cii[ci] == 0 && cj[ci] == 0) {
+          v1 = tb.meang[k] * v1;
+          v0 = tb.meang[k - 1] * v0;
+        }
+        const size_t pe = (size_t)e * g.plane + 2 * cii[ci] + (size_t)g.nxpp * cj[ci];
+        jmp[pe + (size_t)(rr >> 1) * (ns - 1) * g.plane + (rr & 1)] = (T)(v1 - v0);
+      }
   }
 }
 
@@ -1971,6 +2106,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
 // no residual sweep and a system present; k_solve_cta takes the rest.
 // ===========================================================================
 constexpr int kSysR = 16;
+// row stride of the right-hand sides in shared memory: 16 values + 2 of padding,
+// so that the 16-byte stores of consecutive rows fall on different banks
+constexpr int kSysRS = kSysR + 2;
 constexpr int kSysMaxRows = 512;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -2018,27 +2156,32 @@ __host__ __device__ inline SysSmem sys_smem(int n, int N, int ns, int nb, bool d
   o.l = ((size_t)nb * N * N + 3) & ~(size_t)1;  // room for a copy that starts one double early
   o.m = o.l + m * N;
   o.b = o.m + m * m;
-  o.rz = o.b + (size_t)n * kSysR;
+  o.rz = o.b + (size_t)n * kSysRS;
   o.zz = o.rz + kSysR * m1;
   o.d = o.zz + kSysR * m1;
   o.total = o.d + (dmat ? (((size_t)N * N + 1) & ~(size_t)1) : 0);
   return o;
 }
 
-// acc[r] = sum_c col[c*N] * b[(base + c)*16 + r]: one row of a block product
+// 8-byte shared load.  The 16 right-hand-side values of a row are the same
+// for every lane of a warp that works in one block (a broadcast): as 8-byte
+// loads each costs one shared-memory wavefront, as 16-byte loads four.
+__device__ __forceinline__ double lds64(const double* p) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+  return v;
+}
+
+// acc[r] = sum_c col[c*N] * b[(base + c)*RS + r]: one row of a block product
 __device__ __forceinline__ void row_product16(const double* col, const double* bb, int N, double* acc) {
 #pragma unroll
   for (int r = 0; r < kSysR; ++r) acc[r] = 0.0;
 #pragma unroll 2
   for (int c = 0; c < N; ++c) {
     const double a = col[(size_t)c * N];
-    const double2* b2 = (const double2*)(bb + (size_t)c * kSysR);
+    const double* br = bb + (size_t)c * kSysRS;
 #pragma unroll
-    for (int q = 0; q < kSysR / 2; ++q) {
-      const double2 v = b2[q];
-      acc[2 * q] += a * v.x;
-      acc[2 * q + 1] += a * v.y;
-    }
+    for (int r = 0; r < kSysR; ++r) acc[r] += a * lds64(br + r);
   }
 }
 
@@ -2059,7 +2202,7 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
     Geo g, BlockInv bi, const Task* __restrict__ tasks, const int* __restrict__ col_order, T* __restrict__ F0,
     T* __restrict__ F1, T* __restrict__ F2, double rdiv, int meanu, const double* __restrict__ meang,
     const double* __restrict__ Dt, const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart,
-    int* __restrict__ err) {
+    int* __restrict__ err, T* __restrict__ jmp) {
   typedef typename Pair<T>::t P2;
   constexpr int R = kSysR;
   constexpr int PER = ROLE == 0 ? 4 : 2;  // right-hand sides per column
@@ -2132,7 +2275,7 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = -(-(v[r] / rdiv) * eps);
     }
-    double2* d2 = (double2*)(sb + (size_t)k * R);
+    double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
 #pragma unroll
     for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(v[2 * q], v[2 * q + 1]);
   }
@@ -2146,9 +2289,8 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
   if (ROLE == 3) {
     // divergence of u*: i kx u* + i ky v* + (2/h) D w*; RHS = -(div/dt) eps
     // plus the Neumann data at the walls (calcuvwt.f:87-229)
-    double rhs[R];
     if (live) {
-      row_product16(sD + kk, sb + (size_t)ks * N * R, N, acc);
+      row_product16(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
       const double fac = g.hfac[ks];
       const SysDesc sd = bi.sys[s];
 #pragma unroll
@@ -2176,66 +2318,92 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
             vi += (sd.tau2_top * (wnl[p2 + 1] + wvr[p2 + 1])) * eps;
           }
         }
-        rhs[2 * ci] = vr;
-        rhs[2 * ci + 1] = vi;
+        acc[2 * ci] = vr;  // column ci's divergence is no longer needed: the RHS takes its place
+        acc[2 * ci + 1] = vi;
       }
     }
     __syncthreads();  // every row of w* has been read
     if (live) {
-      double2* d2 = (double2*)(sb + (size_t)k * R);
+      double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
 #pragma unroll
-      for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(rhs[2 * q], rhs[2 * q + 1]);
+      for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(acc[2 * q], acc[2 * q + 1]);
     }
     __syncthreads();
   }
-  // interface system: r_e = <lvec_e, b_blk(e)>, z = M^-1 r
+  // interface system: r_e = <lvec_e, b_blk(e)>, z = M^-1 r; stored [e][r] and
+  // computed with the right-hand side index fastest across lanes
   if (m > 0) {
     for (int q = tid; q < m * R; q += blockDim.x) {
-      const int r = q / m, e = q - r * m;
+      const int e = q / R, r = q - e * R;
       const int blk = e < ns - 1 ? e : e - (ns - 1) + 1;
       const double* lv = sL + (size_t)e * N;
-      const double* sv = sb + (size_t)blk * N * R + r;
+      const double* sv = sb + (size_t)blk * N * kSysRS + r;
       double a = 0.0;
-      for (int c = 0; c < N; ++c) a += lv[c] * sv[(size_t)c * R];
+      for (int c = 0; c < N; ++c) a += lv[c] * sv[(size_t)c * kSysRS];
       srz[q] = a;
     }
     __syncthreads();
     for (int q = tid; q < m * R; q += blockDim.x) {
-      const int r = q / m, e = q - r * m;
+      const int e = q / R, r = q - e * R;
       const double* mr = sM + (size_t)e * m;
-      const double* rr = srz + r * m;
       double z = 0.0;
-      for (int c = 0; c < m; ++c) z += mr[c] * rr[c];
+      for (int c = 0; c < m; ++c) z += mr[c] * srz[(size_t)c * R + r];
       szz[q] = z;
     }
     __syncthreads();
   }
   // x = A_ks^-1 b_ks - A_ks^-1 e_0 z_{ks-1} - A_ks^-1 e_{N-1} z_{ns-1+ks}
-  double x[R];
+  double* x = acc;  // the solution replaces the product in place
   if (live) {
     const double* col = sA + offA + (size_t)bi.bmap[ks] * N * N + kk;
-    row_product16(col, sb + (size_t)ks * N * R, N, acc);
+    row_product16(col, sb + (size_t)ks * N * kSysRS, N, acc);
     const double p = ks >= 1 ? col[0] : 0.0;
     const double q = ks <= ns - 2 ? col[(size_t)(N - 1) * N] : 0.0;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       double xv = acc[r];
-      if (ks >= 1) xv -= p * szz[r * m + ks - 1];
-      if (ks <= ns - 2) xv -= q * szz[r * m + ns - 1 + ks];
+      if (ks >= 1) xv -= p * szz[(size_t)(ks - 1) * R + r];
+      if (ks <= ns - 2) xv -= q * szz[(size_t)(ns - 1 + ks) * R + r];
       x[r] = xv;
     }
   }
   if (ROLE != 3) {
+    if (ROLE == 0 && meanu && live) {
+#pragma unroll
+      for (int ci = 0; ci < NC; ++ci)
+        if (cii[ci] == 0 && cj[ci] == 0) {
+          x[PER * ci] = meang[k] * x[PER * ci];
+          x[PER * ci + 1] = meang[k] * x[PER * ci + 1];
+        }
+    }
+    if (jmp) {  // FP32 fields: the jumps across the interfaces, from the FP64 results
+      __syncthreads();  // every thread is done with the right-hand sides
+      if (live) {
+        double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(x[2 * q], x[2 * q + 1]);
+      }
+      __syncthreads();
+      if (live && kk == 0 && ks >= 1) {
+#pragma unroll
+        for (int ci = 0; ci < NC; ++ci) {
+          if (cj[ci] < 0) continue;
+          const size_t pe = (size_t)(ks - 1) * g.plane + 2 * cii[ci] + (size_t)g.nxpp * cj[ci];
+#pragma unroll
+          for (int rr = 0; rr < PER; ++rr) {
+            const int r = PER * ci + rr;
+            const double jv = sb[(size_t)k * kSysRS + r] - sb[(size_t)(k - 1) * kSysRS + r];
+            jmp[pe + (size_t)(rr >> 1) * (g.ns - 1) * g.plane + (rr & 1)] = (T)jv;
+          }
+        }
+      }
+    }
     if (!live) return;
 #pragma unroll
     for (int ci = 0; ci < NC; ++ci) {
       if (cj[ci] < 0) continue;
       const size_t p = fidx<T>(g, 2 * cii[ci], cj[ci], k);
-      double a0 = x[PER * ci], a1 = x[PER * ci + 1];
-      if (ROLE == 0 && meanu && cii[ci] == 0 && cj[ci] == 0) {
-        a0 = meang[k] * a0;
-        a1 = meang[k] * a1;
-      }
+      const double a0 = x[PER * ci], a1 = x[PER * ci + 1];
       P2 o;
       o.x = (T)a0;
       o.y = (T)a1;
@@ -2252,13 +2420,13 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
   // pressure: phi into shared memory, (2/h) D phi, projection (calcuvwt.f:826-901)
   __syncthreads();  // every row of the RHS has been read
   if (live) {
-    double2* d2 = (double2*)(sb + (size_t)k * R);
+    double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
 #pragma unroll
     for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(x[2 * q], x[2 * q + 1]);
   }
   __syncthreads();
   if (!live) return;
-  row_product16(sD + kk, sb + (size_t)ks * N * R, N, acc);
+  row_product16(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
   const double fac = g.hfac[ks];
 #pragma unroll
   for (int ci = 0; ci < NC; ++ci) {
@@ -2273,7 +2441,7 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
       *(P2*)(F2 + pr) = zu;
       continue;
     }
-    const double phr = x[2 * ci], phi = x[2 * ci + 1];
+    const double phr = sb[(size_t)k * kSysRS + 2 * ci], phi = sb[(size_t)k * kSysRS + 2 * ci + 1];
     const P2 w2 = *(const P2*)(F2 + pr);
     double wbr = 0, wbi = 0;
     if (!(ii == 0 && j == 0)) {
@@ -2391,7 +2559,8 @@ __global__ void k_project_planes(Geo g, T* F0, T* F1, T* F2, T* F3, int skip_ifa
 // G[(q*(ns-1)+f)*4 + m] plane = F_q level (f+1)*N - 2 + m; back: add the
 // averaging change held in G to the two interface planes.
 template <typename T>
-__global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, const T* F3, T* G, int back) {
+__global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, const T* F3, T* G, int back,
+                               const T* __restrict__ J) {
   long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long per = (long)g.plane;
   long total = per * 4 * (g.ns - 1) * 4;
@@ -2404,7 +2573,9 @@ __global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, con
   int k = (f + 1) * g.N - 2 + m;
   const T* F = q == 0 ? F0 : q == 1 ? F1 : q == 2 ? F2 : F3;
   if (!back) {
-    G[pl * per + e] = F[(size_t)k * per + e];
+    // FP32 fields: plane 2 holds the jump f(k) - f(k-1) across the interface
+    // that the solves formed in FP64 (see k_iface_rows)
+    G[pl * per + e] = (J && m == 2) ? J[((size_t)q * (g.ns - 1) + f) * per + e] : F[(size_t)k * per + e];
   } else if (m == 1 || m == 2) {
     ((T*)F)[(size_t)k * per + e] += G[pl * per + e];  // spectral change made by the averaging
   }
@@ -2434,13 +2605,22 @@ __global__ void k_iface_rows(Geo g, T* G, FftPlan pl, const typename cplx_t<T>::
   // The interface rows become the change made by the averaging (0 where it
   // does not trigger): the spectral planes are then P(F) + transform of the
   // change, so points left alone never take the round trip's rounding.
+  //
+  // FP32 fields: the jump fsp - fsm is tiny next to the field (it is what the
+  // penalty coupling leaves of the continuity of the solution), and the two
+  // interface planes are rounded to FP32 separately, each with an error of
+  // its own magnitude, so the trigger would follow that rounding near the
+  // threshold.  The solves keep the jump formed in FP64 (J, rounded only
+  // relative to itself); plane 2 holds its transform and fsp = fsm + jump.
   for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    T fsp = P[2 * nx + i], fsm = P[1 * nx + i];
+    const T fsm = P[1 * nx + i];
+    const T jump = sizeof(T) == 4 ? P[2 * nx + i] : P[2 * nx + i] - fsm;
+    const T fsp = sizeof(T) == 4 ? fsm + jump : P[2 * nx + i];
     T favg2 = fsp + fsm;
-    T c0 = fabs(fsp - fsm) / fabs(favg2);
+    T c0 = fabs(jump) / fabs(favg2);
     T d1 = 0, d2 = 0;
     if (c0 > (T)0.005) {
-      T ff = P[0 * nx + i] * (T)0.5 + P[1 * nx + i] * (T)0 + P[2 * nx + i] * (T)0 + P[3 * nx + i] * (T)0.5;
+      T ff = P[0 * nx + i] * (T)0.5 + fsm * (T)0 + fsp * (T)0 + P[3 * nx + i] * (T)0.5;
       d1 = ff - fsm;
       d2 = ff - fsp;
       ++cnt;

@@ -154,7 +154,7 @@ class Solver:
         width, stage A / stage E variant); the state is not changed."""
         ch = (C.c_int * 4)()
         _lib.check(_lib.lib().iw_autotune(self.h, ch))
-        names = {1: "register", 0: "tiled", -1: "n/a"}
+        names = {2: "register-split", 1: "register", 0: "tiled", -1: "n/a"}
         return {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]],
                 "solve": "system-grouped" if ch[3] else "per-task"}
 

@@ -55,7 +55,9 @@ def test_bandlu_noalloc_at_c1_size_and_at_its_limit(nzloc, nsubd, nrhs):
     """C1's 8 x 25 system, one and two right-hand sides, and the largest
     system the scratch takes (nzloc = 25, nsubd = 64: nz = 1600, band
     (3*25+1)*1600 = 121,600 of 131,072 doubles): bit-equal to bandlu_solve_
-    on two consecutive calls, residual below 1e-11."""
+    on two consecutive calls, normwise backward error below 1e-14 (the
+    penalty rows reach 3e6 at these sizes, so the residual itself is not
+    small relative to the right-hand side)."""
     import torch
     import iwrepo_b200 as iw
     from iwrepo_b200 import _lib
@@ -80,7 +82,8 @@ def test_bandlu_noalloc_at_c1_size_and_at_its_limit(nzloc, nsubd, nrhs):
         assert np.array_equal(got[:n], ref_r)
         if nrhs == 2:
             assert np.array_equal(got[n:], ref_i)
-        assert np.linalg.norm(A @ got[:n] - x1) / np.linalg.norm(x1) < 1e-11
+        r = A @ got[:n] - x1
+        assert np.max(np.abs(r)) / (np.linalg.norm(A, np.inf) * np.max(np.abs(got[:n]))) < 1e-14
     s.close()
 
 
