@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the C1 and C4 keys of the default line")
     # smaller horizontal grid with the same vertical grid and physics, for
     # profiling the same kernels on a case that fits a profiler's replay
     ap.add_argument("--nx", type=int, default=None)
@@ -53,12 +54,16 @@ def parse():
     # C3 mixed against C3 FP64 over this many steps: field, kinetic-energy and
     # noise growth-rate errors (a report, not a bench line)
     ap.add_argument("--error-report", type=int, default=0)
+    # interface averaging every N steps (the workloads' default is 1; 0 turns it off)
+    ap.add_argument("--navg", type=int, default=None)
     return ap.parse_args()
 
 
-def workload_cfg(name: str, precision: str, nx=None, ny=None):
+def workload_cfg(name: str, precision: str, nx=None, ny=None, navg=None):
     prec = cf.IW_PREC_MIXED if precision == "mixed" else cf.IW_PREC_FP64
     kw = {k: v for k, v in (("nx", nx), ("ny", ny)) if v}
+    if navg is not None:
+        kw["navgintrfc"] = navg
     return cf.baseline(name, precision=prec, **kw)
 
 
@@ -416,13 +421,31 @@ def run_ours(args, rank, world):
             line["fp64_value"] = fp64
             line["mixed_over_fp64"] = value / world / fp64
             line["mixed_rel_l2_vs_fp64"] = err
+        if not args.no_extra and world == 1 and args.config == "C3" and not (args.nx or args.ny):
+            # the other two batched workloads of the metric, reported beside the headline
+            import types
+            try:
+                c1 = run_c1(types.SimpleNamespace(steps=5, warmup=2), emit=False)
+                line["c1_isolated_solves"] = {"solves_per_s": c1["rates_solves_per_s"],
+                                              "ms_per_batch": c1["ms_per_batch"],
+                                              "fp32_refined_vs_fp64_rel_l2": c1["fp32_refined_vs_fp64_rel_l2"]}
+            except Exception as e:  # reported, never required
+                line["c1_isolated_solves"] = {"failed": str(e)}
+            try:
+                c4 = run_c4(types.SimpleNamespace(steps=6, warmup=4), emit=False)
+                line["c4_ensemble"] = {k: c4[k] for k in ("value", "ms_per_step", "steps", "warmup",
+                                                            "fp64_sequential_value",
+                                                            "batched_mixed_over_sequential_fp64")}
+                line["c4_ensemble"]["workload"] = c4["config"]["workload"]
+            except Exception as e:
+                line["c4_ensemble"] = {"failed": str(e)}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def run_c4(args):
+def run_c4(args, emit=True):
     """C4: 48 independent runs of uneven sizes, mixed precision, advanced
     together (one CUDA-graph launch per ensemble step once every member is in
     steady state), against the same members run one by one in plain FP64."""
@@ -482,10 +505,12 @@ def run_c4(args):
         "fp64_sequential_value": seq, "batched_mixed_over_sequential_fp64": value / seq,
         "note": "gpu_launches counts graph launches; each replays every member's step kernels",
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
-def run_c1(args):
+def run_c1(args, emit=True):
     """C1: 256 x 129 isolated penalty-Helmholtz columns over 8 x 25 GLL points,
     lambda = kx^2 + ky^2 + 11/(6 dt), dt = 1e-3, seeded N(0,1) complex RHS.
     FP64 factor + solve (first call), FP64 solve with cached factors, and FP32
@@ -546,8 +571,10 @@ def run_c1(args):
         "note": "relative residuals are checked in tests/test_gpu_parity.py::test_helm_batched_modes "
                 "(<1e-11 FP64, <1e-7 FP32 + refinement)",
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
     s.close()
+    return line
 
 
 def run_error_report(args):
@@ -557,12 +584,19 @@ def run_error_report(args):
     in the bottom 20 % of the depth (the seeded noise) in each precision."""
     import iwrepo_b200 as iw
 
-    base = workload_cfg(args.config, "mixed", args.nx, args.ny)
+    base = workload_cfg(args.config, "mixed", args.nx, args.ny, args.navg)
     amp, noise = cf.BASELINE_IC.get(base.name, (0.05, 1e-4))
     runs = {"mixed": iw.Solver(base, device=0), "fp64": iw.Solver(base.replace(precision=cf.IW_PREC_FP64), device=0)}
-    hist = {k: [] for k in runs}
     for r in runs.values():
         r.init_mode1(amp, noise, 1000)
+    # the flow's own sensitivity: FP64 from the mixed run's initial state, i.e.
+    # the FP64 initial state rounded to FP32 and nothing else changed
+    st0 = runs["mixed"].state(0)
+    runs["fp64_from_rounded_start"] = iw.Solver(base.replace(precision=cf.IW_PREC_FP64), device=0)
+    z = np.zeros_like(st0)
+    runs["fp64_from_rounded_start"].set_state(st0, z, z, z, z, t=0.0, istep=0)
+    del st0, z
+    hist = {k: [] for k in runs}
     every = 10
     for k in range(0, args.error_report, every):
         for name, r in runs.items():
@@ -570,8 +604,12 @@ def run_error_report(args):
             d = r.diag()
             hist[name].append((d["t"], d["ke"], d["wrms_bottom"]))
     a, b = runs["mixed"].state(0), runs["fp64"].state(0)
+    c = runs["fp64_from_rounded_start"].state(0)
     err = {f: float(np.linalg.norm(a[q] - b[q]) / np.linalg.norm(b[q])) for q, f in enumerate("uvwr")}
     err["velocity"] = float(np.linalg.norm(a[:3] - b[:3]) / np.linalg.norm(b[:3]))
+    sens = {f: float(np.linalg.norm(c[q] - b[q]) / np.linalg.norm(b[q])) for q, f in enumerate("uvwr")}
+    sens["velocity"] = float(np.linalg.norm(c[:3] - b[:3]) / np.linalg.norm(b[:3]))
+    del c
     hm, hd = np.array(hist["mixed"]), np.array(hist["fp64"])
     ke_err = float(np.max(np.abs(hm[:, 1] - hd[:, 1]) / np.abs(hd[:, 1])))
 
@@ -581,7 +619,9 @@ def run_error_report(args):
 
     gm, gd = rate(hm), rate(hd)
     line = {"report": "mixed vs fp64", "workload": describe(base, "mixed")["workload"], "steps": args.error_report,
+            "navgintrfc": base.navgintrfc,
             "field_rel_l2": err, "ke_max_rel_diff": ke_err,
+            "fp64_from_fp32_rounded_start_rel_l2": sens,
             "noise_growth_rate": {"mixed": gm, "fp64": gd, "rel_diff": abs(gm - gd) / abs(gd)},
             "samples_every_steps": every}
     print(json.dumps(line), flush=True)

@@ -294,10 +294,6 @@ struct FieldSet {
   T* X11[11] = {0};
   T* B8[8] = {0};
   T* G = 0;  // interface planes
-  // FP32 fields: the jump f(k) - f(k-1) across every interface of the final
-  // u, v, w, rho of a step, [field][interface][plane], formed in FP64 by the
-  // solve kernels before their results are rounded (see k_iface_rows)
-  T* J = 0;
   typename cplx_t<T>::type *Wm = 0, *Wn = 0, *Wy = 0;
 };
 
@@ -522,10 +518,6 @@ static int alloc_fields(iw_handle* h, FieldSet<T>& fs) {
   for (int q = 0; q < 8; ++q)
     if (dalloc(h, &fs.B8[q], n)) return IW_ERR_NOMEM;
   if (h->ns > 1 && dalloc(h, &fs.G, h->plane * 16 * (size_t)(h->ns - 1))) return IW_ERR_NOMEM;
-  if (sizeof(T) == 4 && h->ns > 1) {
-    if (dalloc(h, &fs.J, h->plane * 4 * (size_t)(h->ns - 1))) return IW_ERR_NOMEM;
-    cudaMemset(fs.J, 0, h->plane * 4 * (size_t)(h->ns - 1) * sizeof(T));
-  }
   typedef typename cplx_t<T>::type C;
   int M = h->nx / 2;
   auto wm = twiddles<C>(M, M);
@@ -543,7 +535,6 @@ static void free_fields(FieldSet<T>& fs) {
   for (int q = 0; q < 11; ++q) cudaFree(fs.X11[q]);
   for (int q = 0; q < 8; ++q) cudaFree(fs.B8[q]);
   cudaFree(fs.G);
-  cudaFree(fs.J);
   cudaFree(fs.Wm);
   cudaFree(fs.Wn);
   cudaFree(fs.Wy);
@@ -1386,8 +1377,6 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3);
   const size_t smsys = lay.total * sizeof(double);
   const bool grouped = h->use_sys && h->nz <= kSysMaxRows && (!cpen || fold) && smsys <= 200 * 1024;
-  // FP32 fields: where the final u, v, w, rho leave their interface jumps
-  T* jmp = (fs.J && role != 3) ? fs.J + (size_t)(role == 0 ? 0 : role == 1 ? 2 : 3) * (h->ns - 1) * h->plane : nullptr;
   const int nend = grouped ? std::max(h->nold[kind], nref) : nt;
   if (grouped && h->ntask2[kind] > 0) {
     const int nthr = (h->nz + 31) / 32 * 32;
@@ -1398,7 +1387,7 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
     cudaFuncSetAttribute(k_solve_sys<T, RL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smsys);           \
     k_solve_sys<T, RL><<<h->ntask2[kind], nthr, smsys, h->st>>>(g, bi, h->dtasks2[kind], h->dcolorder, F0, F1, F2, \
                                                                rd, meanu, mg, h->dDt, h->dwnl, h->dwvr, kstart,   \
-                                                               h->derr, jmp);                                     \
+                                                               h->derr);                                          \
   } while (0)
     if (role == 0)
       IW_SYS_LAUNCH(0);
@@ -1423,7 +1412,7 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
     }
     k_solve_cta<T, R><<<cnt, kSolveThreads, sm, h->st>>>(geo(h), b2, solve_tabs(h, kind), h->dtasks[kind] + t0, F0, F1,
                                                           F2, rd, role, cp, meanu, part == 0 ? 1 : 0, h->dDt, h->dD2t,
-                                                          h->dLt, h->dzh, h->dwnl, h->dwvr, kstart, jmp);
+                                                          h->dLt, h->dzh, h->dwnl, h->dwvr, kstart);
   }
 }
 
@@ -1457,16 +1446,12 @@ static int calcuvwt_impl(iw_handle* h, FieldSet<T>& fs, int cpen) {
       mark(h, 7 + role);
     }
   } else {
-    T* J = fs.J;
-    const size_t jf = J ? (size_t)(h->ns - 1) * h->plane : 0;
     k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_U), fs.F[0], fs.F[1], xnudt, 0, cpen,
-                                                  h->p.meanu_damping, J);
+                                                  h->p.meanu_damping);
     mark(h, 7);
-    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_W), fs.F[2], fs.F[2], xnudt, 1, cpen, 0,
-                                                  J ? J + 2 * jf : nullptr);
+    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_W), fs.F[2], fs.F[2], xnudt, 1, cpen, 0);
     mark(h, 8);
-    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_T), fs.F[3], fs.F[3], dtk, 2, cpen, 0,
-                                                  J ? J + 3 * jf : nullptr);
+    k_visc<T><<<nblk, 32 * warps, smem, h->st>>>(g, solve_tabs(h, SYS_T), fs.F[3], fs.F[3], dtk, 2, cpen, 0);
     mark(h, 9);
   }
   return 0;
@@ -1483,8 +1468,7 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
   }
   const int ng = nf * (h->ns - 1);  // plane groups (field, interface)
   const long tot = (long)h->plane * ng * 4;  // 4 planes per group
-  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 0,
-                                                                       fs.J);
+  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 0);
   {
     YJobs<T> jb;
     memset(&jb, 0, sizeof jb);
@@ -1507,8 +1491,7 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
   }
   long total = (long)h->ny * h->nz * nf;
   k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
-  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1,
-                                                                       fs.J);
+  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1);
   return 0;
 }
 

@@ -1250,7 +1250,7 @@ struct SolveTabs {
 // role 1: w, role 2: rho.  Warp per column.
 template <typename T>
 __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ F1, double rdiv, int role, int cpen,
-                       int meanu, T* __restrict__ jmp) {
+                       int meanu) {
   extern __shared__ __align__(16) double sm[];
   const int warps = blockDim.x / 32;
   const int wid = threadIdx.x / 32, lane = threadIdx.x & 31;
@@ -1270,12 +1270,6 @@ __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ 
       F0[fidx<T>(g, 2 * ii, j, k)] = 0;
       F0[fidx<T>(g, 2 * ii + 1, j, k)] = 0;
     }
-    if (jmp)
-      for (int e = lane; e < g.ns - 1; e += 32) {
-        const size_t pe = (size_t)e * g.plane + 2 * ii + (size_t)g.nxpp * j;
-        jmp[pe] = 0;
-        jmp[pe + 1] = 0;
-      }
     return;
   }
   const SysDesc sd = tb.sys[s];
@@ -1314,17 +1308,6 @@ __global__ void k_visc(Geo g, SolveTabs tb, T* __restrict__ F0, T* __restrict__ 
       if (role == 0 && r < 2 && lzero && meanu) x = rmul(tb.meang[k], x);
       F[fidx<T>(g, 2 * ii + part, j, k)] = (T)x;
     }
-    if (jmp)  // FP32 fields: the jumps across the interfaces, from the FP64 results
-      for (int e = lane; e < g.ns - 1; e += 32) {
-        const int k = (e + 1) * N;
-        double x1 = b[(size_t)r * n + k], x0 = b[(size_t)r * n + k - 1];
-        if (role == 0 && r < 2 && lzero && meanu) {
-          x1 = rmul(tb.meang[k], x1);
-          x0 = rmul(tb.meang[k - 1], x0);
-        }
-        jmp[(size_t)e * g.plane + 2 * ii + part + (size_t)g.nxpp * j + (size_t)(r >> 1) * (g.ns - 1) * g.plane] =
-            (T)(x1 - x0);
-      }
   }
 }
 
@@ -1897,7 +1880,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
     Geo g, BlockInv bi, SolveTabs tb, const Task* __restrict__ tasks, T* __restrict__ F0, T* __restrict__ F1,
     T* __restrict__ F2, double rdiv, int role, int cpen, int meanu, int refine, const double* __restrict__ Dt,
     const double* __restrict__ D2t, const double* __restrict__ Lt, const double* __restrict__ zh,
-    const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart, T* __restrict__ jmp) {
+    const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart) {
   extern __shared__ __align__(16) double sm[];
   __shared__ int cj[R], cii[R];
   const Task tk = tasks[blockIdx.x];
@@ -1919,18 +1902,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
   }
   __syncthreads();
   if (s < 0 && role != 3) {  // w of the (0,0) mode is zero
-    for (int ci = 0; ci < ncolt; ++ci) {
+    for (int ci = 0; ci < ncolt; ++ci)
       for (int k = tid; k < n; k += kSolveThreads) {
         F0[fidx<T>(g, 2 * cii[ci], cj[ci], k)] = 0;
         F0[fidx<T>(g, 2 * cii[ci] + 1, cj[ci], k)] = 0;
       }
-      if (jmp)
-        for (int e = tid; e < ns - 1; e += kSolveThreads) {
-          const size_t pe = (size_t)e * g.plane + 2 * cii[ci] + (size_t)g.nxpp * cj[ci];
-          jmp[pe] = 0;
-          jmp[pe + 1] = 0;
-        }
-    }
     return;
   }
   const double* res = x;
@@ -2073,20 +2049,6 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
         F[fidx<T>(g, 2 * cii[ci] + (rr & 1), cj[ci], k)] = (T)v;
       }
     }
-    if (jmp)  // FP32 fields: the jumps across the interfaces, from the FP64 results
-      for (int q = tid; q < (ns - 1) * R; q += kSolveThreads) {
-        const int e = q / R, r = q - e * R;
-        const int ci = r / per, rr = r - ci * per;
-        if (cj[ci] < 0) continue;
-        const int k = (e + 1) * N;
-        double v1 = res[(size_t)r * n + k], v0 = res[(size_t)r * n + k - 1];
-        if (role == 0 && rr < 2 && meanu && cii[ci] == 0 && cj[ci] == 0) {
-          v1 = tb.meang[k] * v1;
-          v0 = tb.meang[k - 1] * v0;
-        }
-        const size_t pe = (size_t)e * g.plane + 2 * cii[ci] + (size_t)g.nxpp * cj[ci];
-        jmp[pe + (size_t)(rr >> 1) * (ns - 1) * g.plane + (rr & 1)] = (T)(v1 - v0);
-      }
   }
 }
 
@@ -2172,7 +2134,9 @@ __device__ __forceinline__ double lds64(const double* p) {
   return v;
 }
 
-// acc[r] = sum_c col[c*N] * b[(base + c)*RS + r]: one row of a block product
+// acc[r] = sum_c col[c*N] * b[(base + c)*RS + r]: one row of a block product;
+// the loads go out in groups of BL
+template <int BL = 8>
 __device__ __forceinline__ void row_product16(const double* col, const double* bb, int N, double* acc) {
 #pragma unroll
   for (int r = 0; r < kSysR; ++r) acc[r] = 0.0;
@@ -2181,7 +2145,13 @@ __device__ __forceinline__ void row_product16(const double* col, const double* b
     const double a = col[(size_t)c * N];
     const double* br = bb + (size_t)c * kSysRS;
 #pragma unroll
-    for (int r = 0; r < kSysR; ++r) acc[r] += a * lds64(br + r);
+    for (int h = 0; h < kSysR; h += BL) {
+      double v[BL];
+#pragma unroll
+      for (int r = 0; r < BL; ++r) v[r] = lds64(br + h + r);
+#pragma unroll
+      for (int r = 0; r < BL; ++r) acc[h + r] += a * v[r];
+    }
   }
 }
 
@@ -2198,11 +2168,11 @@ struct Pair<double> {
 
 // role 0: u/v (4 RHS per column), 1: w, 2: rho, 3: pressure + projection
 template <typename T, int ROLE>
-__global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
+__global__ void __maxnreg__(72) k_solve_sys(
     Geo g, BlockInv bi, const Task* __restrict__ tasks, const int* __restrict__ col_order, T* __restrict__ F0,
     T* __restrict__ F1, T* __restrict__ F2, double rdiv, int meanu, const double* __restrict__ meang,
     const double* __restrict__ Dt, const double* __restrict__ wnl, const double* __restrict__ wvr, int kstart,
-    int* __restrict__ err, T* __restrict__ jmp) {
+    int* __restrict__ err) {
   typedef typename Pair<T>::t P2;
   constexpr int R = kSysR;
   constexpr int PER = ROLE == 0 ? 4 : 2;  // right-hand sides per column
@@ -2290,7 +2260,7 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
     // divergence of u*: i kx u* + i ky v* + (2/h) D w*; RHS = -(div/dt) eps
     // plus the Neumann data at the walls (calcuvwt.f:87-229)
     if (live) {
-      row_product16(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
+      row_product16<ROLE == 3 ? 4 : 8>(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
       const double fac = g.hfac[ks];
       const SysDesc sd = bi.sys[s];
 #pragma unroll
@@ -2356,7 +2326,7 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
   double* x = acc;  // the solution replaces the product in place
   if (live) {
     const double* col = sA + offA + (size_t)bi.bmap[ks] * N * N + kk;
-    row_product16(col, sb + (size_t)ks * N * kSysRS, N, acc);
+    row_product16<ROLE == 3 ? 4 : 8>(col, sb + (size_t)ks * N * kSysRS, N, acc);
     const double p = ks >= 1 ? col[0] : 0.0;
     const double q = ks <= ns - 2 ? col[(size_t)(N - 1) * N] : 0.0;
 #pragma unroll
@@ -2375,28 +2345,6 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
           x[PER * ci] = meang[k] * x[PER * ci];
           x[PER * ci + 1] = meang[k] * x[PER * ci + 1];
         }
-    }
-    if (jmp) {  // FP32 fields: the jumps across the interfaces, from the FP64 results
-      __syncthreads();  // every thread is done with the right-hand sides
-      if (live) {
-        double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
-#pragma unroll
-        for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(x[2 * q], x[2 * q + 1]);
-      }
-      __syncthreads();
-      if (live && kk == 0 && ks >= 1) {
-#pragma unroll
-        for (int ci = 0; ci < NC; ++ci) {
-          if (cj[ci] < 0) continue;
-          const size_t pe = (size_t)(ks - 1) * g.plane + 2 * cii[ci] + (size_t)g.nxpp * cj[ci];
-#pragma unroll
-          for (int rr = 0; rr < PER; ++rr) {
-            const int r = PER * ci + rr;
-            const double jv = sb[(size_t)k * kSysRS + r] - sb[(size_t)(k - 1) * kSysRS + r];
-            jmp[pe + (size_t)(rr >> 1) * (g.ns - 1) * g.plane + (rr & 1)] = (T)jv;
-          }
-        }
-      }
     }
     if (!live) return;
 #pragma unroll
@@ -2426,7 +2374,7 @@ __global__ void __launch_bounds__(kSysMaxRows) k_solve_sys(
   }
   __syncthreads();
   if (!live) return;
-  row_product16(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
+  row_product16<ROLE == 3 ? 4 : 8>(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
   const double fac = g.hfac[ks];
 #pragma unroll
   for (int ci = 0; ci < NC; ++ci) {
@@ -2559,8 +2507,7 @@ __global__ void k_project_planes(Geo g, T* F0, T* F1, T* F2, T* F3, int skip_ifa
 // G[(q*(ns-1)+f)*4 + m] plane = F_q level (f+1)*N - 2 + m; back: add the
 // averaging change held in G to the two interface planes.
 template <typename T>
-__global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, const T* F3, T* G, int back,
-                               const T* __restrict__ J) {
+__global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, const T* F3, T* G, int back) {
   long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long per = (long)g.plane;
   long total = per * 4 * (g.ns - 1) * 4;
@@ -2573,9 +2520,7 @@ __global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, con
   int k = (f + 1) * g.N - 2 + m;
   const T* F = q == 0 ? F0 : q == 1 ? F1 : q == 2 ? F2 : F3;
   if (!back) {
-    // FP32 fields: plane 2 holds the jump f(k) - f(k-1) across the interface
-    // that the solves formed in FP64 (see k_iface_rows)
-    G[pl * per + e] = (J && m == 2) ? J[((size_t)q * (g.ns - 1) + f) * per + e] : F[(size_t)k * per + e];
+    G[pl * per + e] = F[(size_t)k * per + e];
   } else if (m == 1 || m == 2) {
     ((T*)F)[(size_t)k * per + e] += G[pl * per + e];  // spectral change made by the averaging
   }
@@ -2605,22 +2550,13 @@ __global__ void k_iface_rows(Geo g, T* G, FftPlan pl, const typename cplx_t<T>::
   // The interface rows become the change made by the averaging (0 where it
   // does not trigger): the spectral planes are then P(F) + transform of the
   // change, so points left alone never take the round trip's rounding.
-  //
-  // FP32 fields: the jump fsp - fsm is tiny next to the field (it is what the
-  // penalty coupling leaves of the continuity of the solution), and the two
-  // interface planes are rounded to FP32 separately, each with an error of
-  // its own magnitude, so the trigger would follow that rounding near the
-  // threshold.  The solves keep the jump formed in FP64 (J, rounded only
-  // relative to itself); plane 2 holds its transform and fsp = fsm + jump.
   for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    const T fsm = P[1 * nx + i];
-    const T jump = sizeof(T) == 4 ? P[2 * nx + i] : P[2 * nx + i] - fsm;
-    const T fsp = sizeof(T) == 4 ? fsm + jump : P[2 * nx + i];
+    T fsp = P[2 * nx + i], fsm = P[1 * nx + i];
     T favg2 = fsp + fsm;
-    T c0 = fabs(jump) / fabs(favg2);
+    T c0 = fabs(fsp - fsm) / fabs(favg2);
     T d1 = 0, d2 = 0;
     if (c0 > (T)0.005) {
-      T ff = P[0 * nx + i] * (T)0.5 + fsm * (T)0 + fsp * (T)0 + P[3 * nx + i] * (T)0.5;
+      T ff = P[0 * nx + i] * (T)0.5 + P[1 * nx + i] * (T)0 + P[2 * nx + i] * (T)0 + P[3 * nx + i] * (T)0.5;
       d1 = ff - fsm;
       d2 = ff - fsp;
       ++cnt;
