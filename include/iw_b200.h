@@ -288,21 +288,24 @@ int iw_run(iw_handle *h, int nsteps, int use_graph);
  * its device and keeps the fastest for the following steps: y-tile width (2, 4
  * or 8 columns), the stage-A and stage-E variants (register-column or tiled)
  * and the solve variant (system-grouped CTAs with the tables staged in shared
- * memory, or one CTA per task of <= 4 right-hand sides).  Candidates run on
- * the handle's scratch fields; the state is not changed (the solver tables
- * are built if no step has built them yet).  The stage variants differ only
- * in the order of floating-point sums; the solve variants give the same bits.
+ * memory, their block products on the FP64 pipes or on the FP64 tensor cores,
+ * or one CTA per task of <= 4 right-hand sides).  Candidates run on the
+ * handle's scratch fields; the state is not changed (the solver tables are
+ * built if no step has built them yet).  The tiled stage variants give the
+ * same bits; the solve variants 0 and 1 give the same bits, the tensor-core
+ * products round differently (an FP64 rounding per product).
  * choices (optional, 4 ints): the y-tile width; for stage A and stage E
  * 1 = register-column, 0 = tiled, -1 = not applicable (stage E also 2 =
- * register-column split in two kernels, u* and then the filter); the solve
- * variant (1 = system-grouped, 0 = per task). */
+ * tiled with the input tiles staged by bulk copies, N <= 64); the solve variant
+ * (1 = system-grouped, 2 = system-grouped on the tensor cores, N <= 40,
+ * 0 = per task). */
 int iw_autotune(iw_handle *h, int *choices);
 
 /* Not in the reference.  Sets one launch choice of iw_autotune directly. */
 #define IW_LAUNCH_YTILE 0   /* 0 (size heuristic), 2, 4 or 8 */
 #define IW_LAUNCH_STAGE_A 1 /* -1 (size heuristic), 0 tiled, 1 register-column */
-#define IW_LAUNCH_STAGE_E 2 /* as stage A, or 2: register-column split (u*, then the filter) */
-#define IW_LAUNCH_SOLVE 3   /* 1 system-grouped (default), 0 per task */
+#define IW_LAUNCH_STAGE_E 2 /* as stage A, or 2: tiled, bulk-copied input tiles (N <= 64) */
+#define IW_LAUNCH_SOLVE 3   /* 1 system-grouped (default), 2 same on the FP64 tensor cores, 0 per task */
 int iw_set_launch(iw_handle *h, int which, int value);
 
 /* Not in the reference (its main.f advances one run).  Advances n independent

@@ -274,7 +274,6 @@ std::vector<C> twiddles(int n, int count) {  // exp(-2 pi i e / n), e < count
   }
   return w;
 }
-
 // One system kind: 0 pressure, 1 u/v, 2 w, 3 rho.
 enum { SYS_P = 0, SYS_U, SYS_W, SYS_T, SYS_KINDS };
 
@@ -392,7 +391,7 @@ struct iw_handle {
   Task* dtasks2[SYS_KINDS] = {0, 0, 0, 0};
   int ntask2[SYS_KINDS] = {0, 0, 0, 0};
   int nold[SYS_KINDS] = {0, 0, 0, 0};
-  int use_sys = 1;  // 0: k_solve_cta for every task (kept for comparison)
+  int use_sys = 1;  // 0: k_solve_cta for every task, 1: k_solve_sys, 2: k_solve_sys on the FP64 tensor cores
   double bi_bdfv[SYS_KINDS] = {-1, -1, -1, -1};
   bool bi_fold[SYS_KINDS] = {false, false, false, false};  // Legendre filter folded into ainv
   // distinct subdomain blocks: subdomain ks uses block bmap[ks]; brep[b] is a
@@ -402,7 +401,7 @@ struct iw_handle {
   // launch choices set by iw_autotune (0 / -1: built-in heuristic)
   int tune_ytx = 0;  // y-tile width
   int tune_a = -1;   // stage A: 1 register-column, 0 tiled
-  int tune_e = -1;   // stage E: 1 register-column, 0 tiled
+  int tune_e = -1;   // stage E: 1 register-column, 0 tiled, 2 tiled with bulk-copied tiles
   int brep[IW_MAX_SUBD] = {};
   double bi_dt[SYS_KINDS] = {-1, -1, -1, -1};
   double fac_bdfv[SYS_KINDS] = {-1, -1, -1, -1};  // bdfv the factors were built for
@@ -970,6 +969,11 @@ static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
 }
 
 template <typename T>
+static bool stageE_b_fits(const iw_handle* h) {
+  return h->N <= 8 * kTW && eb_smem<T>(h->N) <= 200 * 1024 && (h->plane * sizeof(T)) % 16 == 0;
+}
+
+template <typename T>
 static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   EArgs<T> a;
   for (int q = 0; q < 4; ++q) {
@@ -987,22 +991,21 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   const dim3 rgrid((unsigned)((h->plane + 127) / 128), (unsigned)h->ns, 4);
   // The register-column stage E holds two columns per thread; past these sizes
   // its register count costs more occupancy than the tiled kernel loses.
-  // The split variant (tune_e = 2) runs the same work as two register-column
-  // kernels with one column each: u* first, then the filter in place.
+  // tune_e = 2: the tiled kernel with its input tiles staged by bulk copies
+  // (N <= 64, shared memory permitting)
+  if (h->tune_e == 2 && stageE_b_fits<T>(h)) {
+    dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
+    const size_t smem = eb_smem<T>(h->N);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_stageE_b<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_stageE_b<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c, h->derr);
+    return;
+  }
   const int emax = sizeof(T) == 4 ? 25 : 17;
-  const bool reg = h->tune_e < 0 ? h->N <= emax : h->tune_e >= 1;
-  const bool split = h->tune_e == 2;
+  const bool reg = h->tune_e < 0 ? h->N <= emax : h->tune_e == 1;
   switch (reg ? zop_bucket(h->N) : 0) {
 #define IW_ECASE(NM)                                                                          \
   case NM:                                                                                    \
-    if (split) {                                                                              \
-      const ZOp<T, NM> op = make_zop<T, NM>(h);                                               \
-      k_stageE_r1<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, op);                     \
-      if (a.filter)                                                                           \
-        k_filter_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), fs.F[0], fs.F[1], fs.F[2], fs.F[3], op); \
-    } else {                                                                                  \
-      k_stageE_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, make_zop<T, NM>(h));       \
-    }                                                                                         \
+    k_stageE_r<T, NM><<<rgrid, 128, 0, h->st>>>(geo(h), a, h->c, make_zop<T, NM>(h));         \
     return;
     IW_ECASE(9)
     IW_ECASE(17)
@@ -1374,7 +1377,9 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   const int nref = h->nrefine[kind], nt = h->ntask[kind];
   const bool fold = h->bi_fold[kind] && cpen;
   // system-grouped kernel for the tasks after the prefix, when it applies
-  const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3);
+  // (use_sys 2: the block products on the FP64 tensor cores, N <= 40)
+  const bool tc = h->use_sys == 2 && h->N <= 8 * kTcMT;
+  const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3, tc ? kTcRS : kSysRS);
   const size_t smsys = lay.total * sizeof(double);
   const bool grouped = h->use_sys && h->nz <= kSysMaxRows && (!cpen || fold) && smsys <= 200 * 1024;
   const int nend = grouped ? std::max(h->nold[kind], nref) : nt;
@@ -1382,21 +1387,29 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
     const int nthr = (h->nz + 31) / 32 * 32;
     Geo g = geo(h);
     const double* mg = h->dmeang;
-#define IW_SYS_LAUNCH(RL)                                                                                           \
+#define IW_SYS_LAUNCH(RL, TCV)                                                                                    \
   do {                                                                                                            \
-    cudaFuncSetAttribute(k_solve_sys<T, RL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smsys);           \
-    k_solve_sys<T, RL><<<h->ntask2[kind], nthr, smsys, h->st>>>(g, bi, h->dtasks2[kind], h->dcolorder, F0, F1, F2, \
-                                                               rd, meanu, mg, h->dDt, h->dwnl, h->dwvr, kstart,   \
-                                                               h->derr);                                          \
+    cudaFuncSetAttribute(k_solve_sys<T, RL, TCV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smsys);      \
+    k_solve_sys<T, RL, TCV><<<h->ntask2[kind], nthr, smsys, h->st>>>(g, bi, h->dtasks2[kind], h->dcolorder, F0, F1, \
+                                                                    F2, rd, meanu, mg, h->dDt, h->dwnl, h->dwvr,   \
+                                                                    kstart, h->derr);                              \
   } while (0)
-    if (role == 0)
-      IW_SYS_LAUNCH(0);
-    else if (role == 1)
-      IW_SYS_LAUNCH(1);
-    else if (role == 2)
-      IW_SYS_LAUNCH(2);
+#define IW_SYS_ROLE(TCV)   \
+  do {                     \
+    if (role == 0)         \
+      IW_SYS_LAUNCH(0, TCV); \
+    else if (role == 1)    \
+      IW_SYS_LAUNCH(1, TCV); \
+    else if (role == 2)    \
+      IW_SYS_LAUNCH(2, TCV); \
+    else                   \
+      IW_SYS_LAUNCH(3, TCV); \
+  } while (0)
+    if (tc)
+      IW_SYS_ROLE(true);
     else
-      IW_SYS_LAUNCH(3);
+      IW_SYS_ROLE(false);
+#undef IW_SYS_ROLE
 #undef IW_SYS_LAUNCH
   }
   for (int part = 0; part < 2; ++part) {
@@ -1587,19 +1600,26 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
   // stage A and stage E variants
   int besta = -1, beste = -1;
   if (zop_bucket(h->N)) {
-    float ta[2], te[3];
-    for (int v = 0; v < 3; ++v) {
-      if (v < 2) {
-        h->tune_a = v;
-        ta[v] = timeit([&] { launch_stageA<T>(h, ts, 1); });
-      }
-      h->tune_e = v;
-      te[v] = timeit([&] { launch_stageE<T>(h, ts); });
+    float ta[2];
+    for (int v = 0; v < 2; ++v) {
+      h->tune_a = v;
+      ta[v] = timeit([&] { launch_stageA<T>(h, ts, 1); });
     }
     besta = ta[1] <= ta[0] ? 1 : 0;
-    beste = 0;
-    for (int v = 1; v < 3; ++v)
-      if (te[v] < te[beste]) beste = v;
+  }
+  {
+    // 0 tiled (any N), 1 register-column (N in a register bucket), 2 tiled
+    // with bulk-copied input tiles (N <= 64)
+    float bt = 0;
+    for (int v = 0; v < 3; ++v) {
+      if ((v == 1 && !zop_bucket(h->N)) || (v == 2 && !stageE_b_fits<T>(h))) continue;
+      h->tune_e = v;
+      const float t = timeit([&] { launch_stageE<T>(h, ts); });
+      if (beste < 0 || t < bt) {
+        bt = t;
+        beste = v;
+      }
+    }
   }
   h->tune_a = besta;
   h->tune_e = beste;
@@ -1609,12 +1629,21 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
       h->use_bi) {
     const int cpen = (h->p.ispecfilterexp == 1) && ((h->istep + 1) % h->p.nspecfilterexp == 0);
     const int kstart = h->p.bc_variant == IW_BC_NOSLIP ? 1 : 0;
-    float tsolve[2];
-    for (int v = 0; v < 2; ++v) {
+    // every solve role of a step: pressure, u/v, w, rho
+    float best = 0;
+    int bestv = 1;
+    for (int v = 0; v < 3; ++v) {
+      if (v == 2 && h->N > 8 * kTcMT) continue;
       h->use_sys = v;
-      tsolve[v] = timeit([&] { launch_solve_bi<T>(h, ts, 0, cpen, kstart); });
+      const float t = timeit([&] {
+        for (int role : {3, 0, 1, 2}) launch_solve_bi<T>(h, ts, role, cpen, kstart);
+      });
+      if (v == 0 || t < best) {
+        best = t;
+        bestv = v;
+      }
     }
-    h->use_sys = tsolve[1] <= tsolve[0] ? 1 : 0;
+    h->use_sys = bestv;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2124,11 +2153,14 @@ int iw_set_launch(iw_handle* h, int which, int value) {
     case IW_LAUNCH_STAGE_E:
       if (value < -1 || value > (which == IW_LAUNCH_STAGE_E ? 2 : 1))
         return set_err(IW_ERR_CONFIG, "stage variant: -1, 0, 1 (or 2 for stage E)");
-      if (value >= 0 && !zop_bucket(h->N)) return set_err(IW_ERR_CONFIG, "register-column stages need N <= 33");
+      if (value == 1 && !zop_bucket(h->N)) return set_err(IW_ERR_CONFIG, "register-column stages need N <= 33");
+      if (value == 2 && !(h->mixed ? stageE_b_fits<float>(h) : stageE_b_fits<double>(h)))
+        return set_err(IW_ERR_CONFIG, "bulk-staged stage E needs N <= 64 and its tiles in shared memory");
       (which == IW_LAUNCH_STAGE_A ? h->tune_a : h->tune_e) = value;
       return IW_OK;
     case IW_LAUNCH_SOLVE:
-      if (value < 0 || value > 1) return set_err(IW_ERR_CONFIG, "solve variant: 0 or 1");
+      if (value < 0 || value > 2) return set_err(IW_ERR_CONFIG, "solve variant: 0, 1 or 2");
+      if (value == 2 && h->N > 8 * kTcMT) return set_err(IW_ERR_CONFIG, "tensor-core solve needs N <= 40");
       h->use_sys = value;
       return IW_OK;
     default:

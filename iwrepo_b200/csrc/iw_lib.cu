@@ -97,6 +97,50 @@ __device__ __forceinline__ T proj_val(const Geo& g, const T* __restrict__ f, int
   return f[fidx<T>(g, i, j, k)];
 }
 
+// Roundings written out (no contraction left to the compiler), so that the
+// variants of a stage give the same bits whatever their loop structure.
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_t(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_t(double a, double b) { return __dmul_rn(a, b); }
+
+// Asynchronous bulk copies into shared memory, completed on an mbarrier;
+// every wait is bounded by the global timer.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// wait for phase `ph` of an mbarrier, for at most `limit_ns`; false if it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t ph, uint64_t limit_ns) {
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(ph)
+        : "memory");
+    if (ok) return true;
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+}
+
 // Tiled z-column kernels: a block owns 32 consecutive real x indices of one
 // (y index, subdomain) and keeps the N x 32 tile in shared memory; the N x N
 // operators (D, filter) are applied with compact loops over the tile.
@@ -141,8 +185,8 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageA(Geo g, const T* __restrict_
     const T* dr = sD + k1 * N;
     T s = 0;
 #pragma unroll 4
-    for (int k2 = 0; k2 < N; ++k2) s += dr[k2] * tile[k2 * kTX + lane];
-    Z[fidx<T>(g, i, j, ks * N + k1)] = s * fac;
+    for (int k2 = 0; k2 < N; ++k2) s = fma_t(dr[k2], tile[k2 * kTX + lane], s);
+    Z[fidx<T>(g, i, j, ks * N + k1)] = mul_t(s, fac);
   }
 }
 
@@ -190,17 +234,31 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   const bool fwd = jb.mode >= 2;
   const bool two = jb.mode == 3;
   (void)nplanes;
-  // load: column ii0+b, row j -> A[b*RSY + fpad(j)] (all copies in flight at once)
-  for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
-    const int b = t % TX, j = t / TX;
-    const int ii = ii0 + b;
-    C* d = A + b * RSY + fpad(j);
-    if (ii < g.nxhp) {
-      cp_async_c<C>(d, (const C*)(jb.src + fidx<T>(g, 2 * ii, j, k)));
-      if (two) cp_async_c<C>(d + TX * RSY, (const C*)(jb.src2 + fidx<T>(g, 2 * ii, j, k)));
-    } else {
-      *d = cmk<C>(0, 0);
-      if (two) d[TX * RSY] = cmk<C>(0, 0);
+  // load: column ii0+b, row j -> A[b*RSY + fpad(j)] (all copies in flight at once).
+  // With 256 threads and TX | 256 a thread keeps its column b and steps j by
+  // JS = 256/TX, so both addresses advance by fixed strides.
+  constexpr int JS = 256 / TX;
+  static_assert(JS % 16 == 0, "the padded smem stride of a j step must be a constant");
+  const int tb = threadIdx.x % TX, tj = threadIdx.x / TX;
+  const int iit = ii0 + tb;
+  const bool colok = iit < g.nxhp;
+  const size_t gstep = (size_t)JS * g.nxpp;
+  {
+    const size_t g0 = fidx<T>(g, 2 * iit, tj, k);
+    C* d = A + tb * RSY + fpad(tj);
+    const C* s1 = (const C*)(jb.src + g0);
+    const C* s2 = two ? (const C*)(jb.src2 + g0) : s1;
+    for (int j = tj; j < ny; j += JS) {
+      if (colok) {
+        cp_async_c<C>(d, s1);
+        if (two) cp_async_c<C>(d + TX * RSY, s2);
+      } else {
+        *d = cmk<C>(0, 0);
+        if (two) d[TX * RSY] = cmk<C>(0, 0);
+      }
+      d += JS + JS / 16;
+      s1 = (const C*)((const T*)s1 + gstep);
+      s2 = (const C*)((const T*)s2 + gstep);
     }
   }
   cp_async_wait_all();
@@ -228,19 +286,22 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   }
   __syncthreads();
   const T sc = fwd ? (T)g.scaley : (T)1;
-  for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
-    const int b = t % TX, j = t / TX;
-    const int ii = ii0 + b;
-    if (ii >= g.nxhp) continue;
-    const C v = A[b * RSY + fpad(j)];
-    C o = cmk<C>(v.x * sc, v.y * sc);
-    if (two) {
-      const C v2 = A2[b * RSY + fpad(j)];
-      const C w2 = cmk<C>(v2.x * sc, v2.y * sc);
-      const T ky = (T)g.yw[j];
-      o = cmk<C>(o.x - ky * w2.y, o.y + ky * w2.x);
+  if (colok) {
+    const C* d = A + tb * RSY + fpad(tj);
+    C* o1 = (C*)(jb.dst + fidx<T>(g, 2 * iit, tj, k));
+    for (int j = tj; j < ny; j += JS) {
+      const C v = *d;
+      C o = cmk<C>(v.x * sc, v.y * sc);
+      if (two) {
+        const C v2 = d[TX * RSY];
+        const C w2 = cmk<C>(v2.x * sc, v2.y * sc);
+        const T ky = (T)g.yw[j];
+        o = cmk<C>(o.x - ky * w2.y, o.y + ky * w2.x);
+      }
+      *o1 = o;
+      d += JS + JS / 16;
+      o1 = (C*)((T*)o1 + gstep);
     }
-    *(C*)(jb.dst + fidx<T>(g, 2 * ii, j, k)) = o;
   }
 }
 
@@ -489,7 +550,29 @@ struct Coefs {
 // make bdf1 + bdf2 + bdf3 differ from bdfv and bias every step the same way.
 template <typename T>
 __device__ __forceinline__ T bdf_combine(const Coefs& c, T se, T F2, T fn, T fnm) {
-  return (T)(c.dt * (double)se + c.bdf1 * (double)F2 + c.bdf2 * (double)fn + c.bdf3 * (double)fnm);
+  return (T)__fma_rn(c.bdf3, (double)fnm,
+                     __fma_rn(c.bdf2, (double)fn, __fma_rn(c.bdf1, (double)F2, __dmul_rn(c.dt, (double)se))));
+}
+
+
+// one point of K_E: S = B + fac (D Z), u* from the BDF combination of the
+// extrapolated S
+template <typename T>
+__device__ __forceinline__ void stageE_point(const Coefs& c, T fac, T f1, T f2, T f3, T b, T dz, T sn, T snm, T F2,
+                                             T fn, T fnm, T& S, T& fsv) {
+  S = fma_t(dz, fac, b);
+  const T se = fma_t(f3, snm, fma_t(f2, sn, mul_t(f1, S)));
+  fsv = bdf_combine<T>(c, se, F2, fn, fnm);
+}
+// the extrapolated S in FP64 at the walls (the wall data of w)
+template <typename T>
+__device__ __forceinline__ double stageE_wall(T f1, T f2, T f3, T S, T sn, T snm) {
+  return __fma_rn((double)f3, (double)snm, __fma_rn((double)f2, (double)sn, __dmul_rn((double)f1, (double)S)));
+}
+// the filtered value: cf (L f) = g + (cf - 1) g with g = f + (L - I) f
+__device__ __forceinline__ double stageE_filtered(double f, double lf, double cfm1) {
+  const double gv = __dadd_rn(f, lf);
+  return __fma_rn(cfm1, gv, gv);
 }
 
 template <typename T>
@@ -535,20 +618,18 @@ __device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, con
       const T* dr = sD + k1 * N;
       T s = 0;
 #pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) s += dr[k2] * tz[k2 * kTX + lane];
-      const T S = a.B[q][p] + s * fac;
+      for (int k2 = 0; k2 < N; ++k2) s = fma_t(dr[k2], tz[k2 * kTX + lane], s);
       const T sn = a.Snold[q][p];
       const T snm = a.Snm_w[q][p];
-      if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
-        const int side = kk == 0 ? 0 : 1;
-        a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] =
-            (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
-      }
-      const T se = f1 * S + f2 * sn + f3 * snm;
       const T F2 = proj_val<T>(g, a.F1[q], i, j, kk);
       const T fn = a.Fn[q][p];
       const T fnm = a.Fnm_w[q][p];
-      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
+      T S;
+      stageE_point<T>(c, fac, f1, f2, f3, a.B[q][p], s, sn, snm, F2, fn, fnm, S, fsv);
+      if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
+        const int side = kk == 0 ? 0 : 1;
+        a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] = stageE_wall<T>(f1, f2, f3, S, sn, snm);
+      }
       a.Snm_w[q][p] = S;
       a.Fnm_w[q][p] = F2;
     }
@@ -567,9 +648,155 @@ __device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, con
       const double* lr = sL + k1 * N;
       double s = 0;
 #pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) s += lr[k2] * (double)tf[k2 * kTX + lane];
-      const double gv = (double)tf[k1 * kTX + lane] + s;  // L f = f + (L - I) f
-      o = (T)(gv + cfm1 * gv);                            // cf g = g + (cf - 1) g
+      for (int k2 = 0; k2 < N; ++k2) s = __fma_rn(lr[k2], (double)tf[k2 * kTX + lane], s);
+      o = (T)stageE_filtered((double)tf[k1 * kTX + lane], s, cfm1);
+    } else {
+      o = tf[k1 * kTX + lane];
+    }
+    a.F[q][fidx<T>(g, i, j, ks * N + k1)] = o;
+  }
+}
+
+// Tiled K_E with its input tiles staged by bulk asynchronous copies: the
+// same CTA tiling and the same sums as stageE_tile (so the same bits), but
+// every row of the seven input tiles (Z, B, S_n, S_{n-1}, F1, F_n, F_{n-1})
+// is requested at once, one cp.async.bulk per row completing on an mbarrier
+// (Z on its own, so that D Z starts while the rest lands), instead of a
+// chain of dependent 4-byte loads per output row.  A row of 32 points is
+// copied from the 16-byte boundary at or below its first point (FP32 rows of
+// an nxpp = 2 (mod 4) field start 8 bytes into a unit); the copy may run up to
+// 15 bytes past the field's end, inside the 16 bytes every field buffer is
+// allocated with beyond its end.  The launch requires nxpp*ny*sizeof(T) to be
+// a multiple of 16, so that every row of a CTA has the same offset.
+constexpr int kEBArr = 7;
+template <typename T>
+__host__ __device__ inline int eb_rs() {  // tile row stride (elements): 32 points and room for the offset
+  return kTX + 16 / (int)sizeof(T);
+}
+template <typename T>
+__host__ inline size_t eb_smem(int N) {
+  return 16 + (size_t)kEBArr * N * eb_rs<T>() * sizeof(T) + (size_t)N * N * sizeof(double) +
+         (size_t)N * N * sizeof(T) + (size_t)N * kTX * sizeof(T);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs c, int* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = g.N, RS = eb_rs<T>();
+  uint64_t* bar = (uint64_t*)smraw;  // [0]: Z, [1]: the other six tiles
+  T* tiles = (T*)(smraw + 16);       // [arr][k][RS]
+  double* sL = (double*)(tiles + (size_t)kEBArr * N * RS);
+  T* sD = (T*)(sL + N * N);
+  T* tf = sD + N * N;  // N*kTX: F* tile
+  const int q = blockIdx.z;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int i0 = blockIdx.x * kTX, i = i0 + lane;
+  const int j = blockIdx.y % g.ny, ks = blockIdx.y / g.ny;
+  const int nval = min(kTX, g.nxpp - i0);
+  if (tid == 0) {
+    mbar_init(&bar[0], (uint32_t)N);
+    mbar_init(&bar[1], (uint32_t)((kEBArr - 1) * N));
+  }
+  __syncthreads();
+  for (int t = tid; t < kEBArr * N; t += blockDim.x) {
+    const int arr = t / N, k = t - arr * N;
+    const T* base = arr == 0 ? a.Z[q]
+                    : arr == 1 ? a.B[q]
+                    : arr == 2 ? a.Snold[q]
+                    : arr == 3 ? a.Snm_w[q]
+                    : arr == 4 ? a.F1[q]
+                    : arr == 5 ? a.Fn[q]
+                               : a.Fnm_w[q];
+    const uintptr_t ga = (uintptr_t)(base + fidx<T>(g, i0, j, ks * N + k));
+    const uint32_t off = (uint32_t)(ga & 15u);
+    const uint32_t bytes = (off + (uint32_t)nval * (uint32_t)sizeof(T) + 15u) & ~15u;
+    uint64_t* b = &bar[arr == 0 ? 0 : 1];
+    mbar_expect_tx(b, bytes);
+    bulk_g2s(tiles + (size_t)t * RS, (const void*)(ga - off), bytes, b);
+  }
+  for (int t = tid; t < N * N; t += blockDim.x) {
+    sD[t] = (T)g.D[t];
+    sL[t] = g.Lfil[t] - (t / N == t % N ? 1.0 : 0.0);
+  }
+  // element offset of this CTA's first point inside each copied row (the
+  // same for every row: the planes are whole 16-byte units)
+  const int eo = (int)((((size_t)i0 + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * (size_t)(ks * N))) * sizeof(T)) &
+                       15u) /
+                 (int)sizeof(T);
+  const bool ok0 = mbar_wait(&bar[0], 0, 2000000000ull);
+  __syncthreads();  // the operator tables are in place
+  const bool act = i < g.nxpp;
+  const T fac = (T)g.hfac[ks];
+  const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
+  // D Z for this warp's rows, kept in registers until the other tiles land
+  constexpr int kMaxRows = 8;  // N <= 8 * kTW = 64
+  T dz[kMaxRows];
+  const T* tz = tiles;  // Z tile
+#pragma unroll
+  for (int r = 0; r < kMaxRows; ++r) {
+    const int k1 = w + kTW * r;
+    dz[r] = 0;
+    if (k1 < N && act) {
+      const T* dr = sD + k1 * N;
+      T s = 0;
+#pragma unroll 4
+      for (int k2 = 0; k2 < N; ++k2) s = fma_t(dr[k2], tz[k2 * RS + eo + lane], s);
+      dz[r] = s;
+    }
+  }
+  const bool ok1 = mbar_wait(&bar[1], 0, 2000000000ull);
+  if (__syncthreads_or(!(ok0 && ok1))) {  // a copy never completed: report, let the copies finish, leave
+    if (tid == 0) err[1] = 1;
+    mbar_wait(&bar[0], 0, 2000000000ull);
+    mbar_wait(&bar[1], 0, 2000000000ull);
+    return;
+  }
+#pragma unroll
+  for (int r = 0; r < kMaxRows; ++r) {
+    const int k1 = w + kTW * r;
+    if (k1 >= N) break;
+    T fsv = 0;
+    if (act) {
+      const int kk = ks * N + k1;
+      const size_t p = fidx<T>(g, i, j, kk);
+      const size_t e = (size_t)k1 * RS + eo + lane;
+      const size_t AS = (size_t)N * RS;
+      const T sn = tiles[2 * AS + e];
+      const T snm = tiles[3 * AS + e];
+      T F2;
+      if (i < 2) {
+        const T va = tiles[4 * AS + e];
+        const T vb = a.F1[q][fidx<T>(g, i, (g.ny - j) % g.ny, kk)];
+        F2 = i == 0 ? (T)0.5 * (va + vb) : (T)0.5 * (va - vb);
+      } else if (i >= g.nx) {
+        F2 = i == g.nx ? tiles[4 * AS + e] * (T)g.scaley : (T)0;
+      } else {
+        F2 = tiles[4 * AS + e];
+      }
+      const T fn = tiles[5 * AS + e];
+      const T fnm = tiles[6 * AS + e];
+      T S;
+      stageE_point<T>(c, fac, f1, f2, f3, tiles[1 * AS + e], dz[r], sn, snm, F2, fn, fnm, S, fsv);
+      if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
+        const int side = kk == 0 ? 0 : 1;
+        a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] = stageE_wall<T>(f1, f2, f3, S, sn, snm);
+      }
+      a.Snm_w[q][p] = S;
+      a.Fnm_w[q][p] = F2;
+    }
+    tf[k1 * kTX + lane] = fsv;
+  }
+  __syncthreads();
+  if (!act) return;
+  const double cfm1 = a.filter ? g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0 : 0.0;
+  for (int k1 = w; k1 < N; k1 += kTW) {
+    T o;
+    if (a.filter) {
+      const double* lr = sL + k1 * N;
+      double s = 0;
+#pragma unroll 4
+      for (int k2 = 0; k2 < N; ++k2) s = __fma_rn(lr[k2], (double)tf[k2 * kTX + lane], s);
+      o = (T)stageE_filtered((double)tf[k1 * kTX + lane], s, cfm1);
     } else {
       o = tf[k1 * kTX + lane];
     }
@@ -642,8 +869,8 @@ __global__ void __launch_bounds__(128) k_stageA_r(Geo g, const __grid_constant__
     if (k1 < N) {
       T s = 0;
 #pragma unroll
-      for (int k2 = 0; k2 < NM; ++k2) s += op.D[k1 * NM + k2] * col[k2];
-      Z[(size_t)(ks * N + k1) * g.plane + t] = s * fac;
+      for (int k2 = 0; k2 < NM; ++k2) s = fma_t(op.D[k1 * NM + k2], col[k2], s);
+      Z[(size_t)(ks * N + k1) * g.plane + t] = mul_t(s, fac);
     }
   }
 }
@@ -704,12 +931,11 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
       const size_t p = (size_t)kk * g.plane + t;
       T s = 0;
 #pragma unroll
-      for (int k2 = 0; k2 < NM; ++k2) s += op.D[k1 * NM + k2] * zc[k2];
-      const T S = b + s * fac;
+      for (int k2 = 0; k2 < NM; ++k2) s = fma_t(op.D[k1 * NM + k2], zc[k2], s);
+      T S;
+      stageE_point<T>(c, fac, f1, f2, f3, b, s, sn, snm, F2, fn, fnm, S, fsv);
       if (q == 2 && ((kk == 0) || (kk == g.nz - 1)))
-        a.wnl[t + (kk == 0 ? 0 : g.plane)] = (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
-      const T se = f1 * S + f2 * sn + f3 * snm;
-      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
+        a.wnl[t + (kk == 0 ? 0 : g.plane)] = stageE_wall<T>(f1, f2, f3, S, sn, snm);
       Snmq[p] = S;
       Fnmq[p] = F2;
     }
@@ -723,110 +949,12 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
       if (a.filter) {
         double s = 0;
 #pragma unroll
-        for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * (double)fs[k2];  // (L - I) f in FP64
-        const double gv = (double)fs[k1] + s;
-        o = (T)(gv + cfm1 * gv);
+        for (int k2 = 0; k2 < NM; ++k2) s = __fma_rn(op.L[k1 * NM + k2], (double)fs[k2], s);  // (L - I) f in FP64
+        o = (T)stageE_filtered((double)fs[k1], s, cfm1);
       } else {
         o = fs[k1];
       }
       a.F[q][(size_t)(ks * N + k1) * g.plane + t] = o;
-    }
-  }
-}
-
-// Split K_E, first half: everything of k_stageE_r but the filter; writes u*.
-template <typename T, int NM>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_stageE_r1(Geo g, EArgs<T> a, Coefs c, const __grid_constant__ ZOp<T, NM> op) {
-  const int q = blockIdx.z, ks = blockIdx.y, N = g.N;
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.plane) return;
-  const int i = (int)(t % g.nxpp), j = (int)(t / g.nxpp);
-  T zc[NM];
-#pragma unroll
-  for (int k = 0; k < NM; ++k) zc[k] = k < N ? a.Z[q][(size_t)(ks * N + k) * g.plane + t] : (T)0;
-  const T fac = (T)g.hfac[ks];
-  const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
-  const T* Bq = a.B[q];
-  const T* Snq = a.Snold[q];
-  const T* F1q = a.F1[q];
-  const T* Fnq = a.Fn[q];
-  T* Snmq = a.Snm_w[q];
-  T* Fnmq = a.Fnm_w[q];
-  // Rolling window: the inputs of row k1+PF are loaded before the stores of
-  // row k1, so the loads of several rows are in flight at once (the pointers
-  // are not known to be distinct, so the compiler would not hoist them).
-  constexpr int PF = 4;
-  T wb[PF], wsn[PF], wsnm[PF], wf2[PF], wfn[PF], wfnm[PF];
-#pragma unroll
-  for (int k1 = 0; k1 < PF; ++k1) {
-    if (k1 < N) {
-      const int kk = ks * N + k1;
-      const size_t p = (size_t)kk * g.plane + t;
-      wb[k1] = Bq[p];
-      wsn[k1] = Snq[p];
-      wsnm[k1] = Snmq[p];
-      wf2[k1] = proj_val<T>(g, F1q, i, j, kk);
-      wfn[k1] = Fnq[p];
-      wfnm[k1] = Fnmq[p];
-    }
-  }
-#pragma unroll
-  for (int k1 = 0; k1 < NM; ++k1) {
-    if (k1 < N) {
-      T fsv;
-      const int sl = k1 % PF;
-      const T b = wb[sl], sn = wsn[sl], snm = wsnm[sl], F2 = wf2[sl], fn = wfn[sl], fnm = wfnm[sl];
-      if (k1 + PF < NM && k1 + PF < N) {
-        const int kn = ks * N + k1 + PF;
-        const size_t pn = (size_t)kn * g.plane + t;
-        wb[sl] = Bq[pn];
-        wsn[sl] = Snq[pn];
-        wsnm[sl] = Snmq[pn];
-        wf2[sl] = proj_val<T>(g, F1q, i, j, kn);
-        wfn[sl] = Fnq[pn];
-        wfnm[sl] = Fnmq[pn];
-      }
-      const int kk = ks * N + k1;
-      const size_t p = (size_t)kk * g.plane + t;
-      T s = 0;
-#pragma unroll
-      for (int k2 = 0; k2 < NM; ++k2) s += op.D[k1 * NM + k2] * zc[k2];
-      const T S = b + s * fac;
-      if (q == 2 && ((kk == 0) || (kk == g.nz - 1)))
-        a.wnl[t + (kk == 0 ? 0 : g.plane)] = (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
-      const T se = f1 * S + f2 * sn + f3 * snm;
-      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
-      Snmq[p] = S;
-      Fnmq[p] = F2;
-      a.F[q][p] = fsv;  // u* before the filter (k_filter_r applies it)
-    }
-  }
-}
-
-// Second half of the split K_E: the Fourier x Legendre filter of u*
-// (filter_3dlegenfourier, filtering.f:811-983) in place, one column per
-// thread held in FP64 registers, (L - I) from the constant bank:
-// F <- cf g with g = f + (L - I) f, the same arithmetic as the combined kernel.
-template <typename T, int NM>
-__global__ void __launch_bounds__(128, 5) k_filter_r(Geo g, T* F0, T* F1_, T* F2_, T* F3_,
-                                                  const __grid_constant__ ZOp<T, NM> op) {
-  const int q = blockIdx.z, ks = blockIdx.y, N = g.N;
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.plane) return;
-  const int i = (int)(t % g.nxpp), j = (int)(t / g.nxpp);
-  T* F = q == 0 ? F0 : q == 1 ? F1_ : q == 2 ? F2_ : F3_;
-  double f[NM];
-#pragma unroll
-  for (int k = 0; k < NM; ++k) f[k] = k < N ? (double)F[(size_t)(ks * N + k) * g.plane + t] : 0.0;
-  const double cfm1 = g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0;
-#pragma unroll
-  for (int k1 = 0; k1 < NM; ++k1) {
-    if (k1 < N) {
-      double s = 0;
-#pragma unroll
-      for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * f[k2];
-      const double gv = f[k1] + s;
-      F[(size_t)(ks * N + k1) * g.plane + t] = (T)(gv + cfm1 * gv);
     }
   }
 }
@@ -2073,52 +2201,17 @@ constexpr int kSysR = 16;
 constexpr int kSysRS = kSysR + 2;
 constexpr int kSysMaxRows = 512;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-// wait for phase `ph` of an mbarrier, for at most `limit_ns`; false if it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t ph, uint64_t limit_ns) {
-  const uint64_t t0 = global_ns();
-  for (;;) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(ph)
-        : "memory");
-    if (ok) return true;
-    if (global_ns() - t0 > limit_ns) return false;
-  }
-}
-
 struct SysSmem {  // offsets (doubles) of the shared-memory regions of k_solve_sys
   size_t a, l, m, b, rz, zz, d, total;
 };
-__host__ __device__ inline SysSmem sys_smem(int n, int N, int ns, int nb, bool dmat) {
+__host__ __device__ inline SysSmem sys_smem(int n, int N, int ns, int nb, bool dmat, int rs = kSysRS) {
   SysSmem o;
   const size_t m = 2 * (size_t)(ns - 1), m1 = m > 0 ? m : 1;
   o.a = 0;
   o.l = ((size_t)nb * N * N + 3) & ~(size_t)1;  // room for a copy that starts one double early
   o.m = o.l + m * N;
   o.b = o.m + m * m;
-  o.rz = o.b + (size_t)n * kSysRS;
+  o.rz = o.b + (size_t)n * rs;
   o.zz = o.rz + kSysR * m1;
   o.d = o.zz + kSysR * m1;
   o.total = o.d + (dmat ? (((size_t)N * N + 1) & ~(size_t)1) : 0);
@@ -2155,6 +2248,49 @@ __device__ __forceinline__ void row_product16(const double* col, const double* b
   }
 }
 
+// FP64 tensor-core variant of the block products (mma.sync m8n8k4, the FP64
+// matrix instruction of sm_100a; tcgen05 has no FP64 kind).  A warp owns whole
+// subdomains: X_ks[:, 8 nt .. 8 nt + 7] = Op_ks B_ks[:, 8 nt ..] in row tiles
+// of 8, 4 columns of Op per instruction, the padding of the ragged N read as
+// zeros.  Lane (g, t4) = (lane / 4, lane % 4) ends with
+// X[8 mt + g][8 nt + 2 t4 + {0, 1}]: one complex value of one column.  The
+// right-hand-side rows have a stride of 20 doubles, so that the 4 rows x 8
+// values of a B fragment fall in two shared-memory wavefronts.
+constexpr int kTcRS = 20;
+constexpr int kTcMT = 5;  // row tiles per subdomain: N <= 40
+
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+// acc[mt] = (Op B)[8 mt + g][8 nt + 2 t4 + {0, 1}] for Op(r, c) = op[c N + r] and
+// B(c, :) = bb[c kTcRS + :], c < N
+__device__ __forceinline__ void tc_block_product(const double* op, const double* bb, int N, int nt, int lane,
+                                                 double (&acc)[kTcMT][2]) {
+  const int g = lane >> 2, t4 = lane & 3;
+  const int MT = (N + 7) >> 3, KT = (N + 3) >> 2;
+  __syncwarp();  // mma.sync wants the whole warp converged
+#pragma unroll
+  for (int mt = 0; mt < kTcMT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+  for (int kt = 0; kt < KT; ++kt) {
+    const int c = kt * 4 + t4;
+    const bool cin = c < N;
+    const int cc = cin ? c : N - 1;  // in-range address for the padding
+    const double b = cin ? bb[(size_t)cc * kTcRS + nt * 8 + g] : 0.0;
+#pragma unroll
+    for (int mt = 0; mt < kTcMT; ++mt) {
+      if (mt < MT) {
+        const int r = mt * 8 + g;
+        const bool rin = r < N;
+        const double a = (cin && rin) ? op[(size_t)cc * N + (rin ? r : N - 1)] : 0.0;
+        dmma884(acc[mt][0], acc[mt][1], a, b);
+      }
+    }
+  }
+}
+
 template <typename T>
 struct Pair;
 template <>
@@ -2166,8 +2302,10 @@ struct Pair<double> {
   typedef double2 t;
 };
 
-// role 0: u/v (4 RHS per column), 1: w, 2: rho, 3: pressure + projection
-template <typename T, int ROLE>
+// role 0: u/v (4 RHS per column), 1: w, 2: rho, 3: pressure + projection.
+// TC: block products on the FP64 tensor cores (N <= 40), else one row per
+// thread on the FP64 pipes.
+template <typename T, int ROLE, bool TC = false>
 __global__ void __maxnreg__(72) k_solve_sys(
     Geo g, BlockInv bi, const Task* __restrict__ tasks, const int* __restrict__ col_order, T* __restrict__ F0,
     T* __restrict__ F1, T* __restrict__ F2, double rdiv, int meanu, const double* __restrict__ meang,
@@ -2177,6 +2315,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
   constexpr int R = kSysR;
   constexpr int PER = ROLE == 0 ? 4 : 2;  // right-hand sides per column
   constexpr int NC = R / PER;             // column slots
+  constexpr int RS = TC ? kTcRS : kSysRS;  // right-hand-side row stride
   extern __shared__ __align__(16) double sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int cj[NC], cii[NC];
@@ -2184,7 +2323,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
   const int n = g.nz, N = g.N, ns = g.ns, m = 2 * (ns - 1), nb = bi.nb;
   const int tid = threadIdx.x;
   const int s = tk.sys;
-  const SysSmem L = sys_smem(n, N, ns, nb, ROLE == 3);
+  const SysSmem L = sys_smem(n, N, ns, nb, ROLE == 3, RS);
   double* sA = sm + L.a;
   double* sL = sm + L.l;
   double* sM = sm + L.m;
@@ -2245,7 +2384,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = -(-(v[r] / rdiv) * eps);
     }
-    double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
+    double2* d2 = (double2*)(sb + (size_t)k * RS);
 #pragma unroll
     for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(v[2 * q], v[2 * q + 1]);
   }
@@ -2255,12 +2394,63 @@ __global__ void __maxnreg__(72) k_solve_sys(
     mbar_wait(&bar, 0, 2000000000ull);
     return;
   }
+  const int lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+  if constexpr (TC) {
+    if (ROLE == 3) {
+      // divergence of u* per subdomain on the tensor cores, the RHS written
+      // over w* in place (a warp reads and writes only its own subdomains)
+      const int gq = lane >> 2, t4 = lane & 3, MT = (N + 7) >> 3;
+      const SysDesc sd = bi.sys[s];
+      for (int ks2 = wid; ks2 < ns; ks2 += nwarp) {
+        double* bb = sb + (size_t)ks2 * N * RS;
+        const double fac = g.hfac[ks2];
+        for (int nt = 0; nt < 2; ++nt) {
+          double tacc[kTcMT][2];
+          tc_block_product(sD, bb, N, nt, lane, tacc);
+          __syncwarp();
+          const int c0 = nt * 8 + 2 * t4, ci = c0 >> 1;
+#pragma unroll
+          for (int mt = 0; mt < kTcMT; ++mt) {
+            const int r = mt * 8 + gq;
+            if (mt >= MT || r >= N) continue;
+            const int kq = ks2 * N + r;
+            double vr = 0.0, vi = 0.0;
+            if (cj[ci] >= 0) {
+              const int j = cj[ci], ii = cii[ci];
+              const size_t pr = fidx<T>(g, 2 * ii, j, kq);
+              const P2 u2 = *(const P2*)(F0 + pr), w2 = *(const P2*)(F1 + pr);
+              const double ur = (double)u2.x, ui = (double)u2.y;
+              const double wr = (double)w2.x, wi = (double)w2.y;
+              const double xw = g.xw[ii], yw = g.yw[j];
+              const double dr = -(xw * ui) - (yw * wi) + tacc[mt][0] * fac;
+              const double di = (xw * ur) + (yw * wr) + tacc[mt][1] * fac;
+              vr = -((dr / dt) * eps);
+              vi = -((di / dt) * eps);
+              if (kq == 0) {
+                const size_t p1 = (size_t)g.nxpp * j + 2 * ii;
+                vr -= (sd.tau1_bot * (wnl[p1] + wvr[p1])) * eps;
+                vi -= (sd.tau1_bot * (wnl[p1 + 1] + wvr[p1 + 1])) * eps;
+              }
+              if (kq == n - 1) {
+                const size_t p2 = (size_t)g.nxpp * (j + g.ny) + 2 * ii;
+                vr += (sd.tau2_top * (wnl[p2] + wvr[p2])) * eps;
+                vi += (sd.tau2_top * (wnl[p2 + 1] + wvr[p2 + 1])) * eps;
+              }
+            }
+            *(double2*)(bb + (size_t)r * RS + c0) = make_double2(vr, vi);
+          }
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+    }
+  }
   double acc[R];
-  if (ROLE == 3) {
+  if (!TC && ROLE == 3) {
     // divergence of u*: i kx u* + i ky v* + (2/h) D w*; RHS = -(div/dt) eps
     // plus the Neumann data at the walls (calcuvwt.f:87-229)
     if (live) {
-      row_product16<ROLE == 3 ? 4 : 8>(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
+      row_product16<ROLE == 3 ? 4 : 8>(sD + kk, sb + (size_t)ks * N * RS, N, acc);
       const double fac = g.hfac[ks];
       const SysDesc sd = bi.sys[s];
 #pragma unroll
@@ -2294,7 +2484,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
     }
     __syncthreads();  // every row of w* has been read
     if (live) {
-      double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
+      double2* d2 = (double2*)(sb + (size_t)k * RS);
 #pragma unroll
       for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(acc[2 * q], acc[2 * q + 1]);
     }
@@ -2307,9 +2497,9 @@ __global__ void __maxnreg__(72) k_solve_sys(
       const int e = q / R, r = q - e * R;
       const int blk = e < ns - 1 ? e : e - (ns - 1) + 1;
       const double* lv = sL + (size_t)e * N;
-      const double* sv = sb + (size_t)blk * N * kSysRS + r;
+      const double* sv = sb + (size_t)blk * N * RS + r;
       double a = 0.0;
-      for (int c = 0; c < N; ++c) a += lv[c] * sv[(size_t)c * kSysRS];
+      for (int c = 0; c < N; ++c) a += lv[c] * sv[(size_t)c * RS];
       srz[q] = a;
     }
     __syncthreads();
@@ -2322,11 +2512,108 @@ __global__ void __maxnreg__(72) k_solve_sys(
     }
     __syncthreads();
   }
+  if constexpr (TC) {
+    // x = A_ks^-1 b_ks - A_ks^-1 e_0 z_{ks-1} - A_ks^-1 e_{N-1} z_{ns-1+ks} on
+    // the tensor cores; u/v, w, rho are stored, phi goes over the RHS in place
+    const int gq = lane >> 2, t4 = lane & 3, MT = (N + 7) >> 3;
+    for (int ks2 = wid; ks2 < ns; ks2 += nwarp) {
+      double* bb = sb + (size_t)ks2 * N * RS;
+      const double* blk = sA + offA + (size_t)bi.bmap[ks2] * N * N;
+      for (int nt = 0; nt < 2; ++nt) {
+        double tacc[kTcMT][2];
+        tc_block_product(blk, bb, N, nt, lane, tacc);
+        if (ROLE == 3) __syncwarp();
+        const int c0 = nt * 8 + 2 * t4;
+#pragma unroll
+        for (int mt = 0; mt < kTcMT; ++mt) {
+          const int r = mt * 8 + gq;
+          if (mt >= MT || r >= N) continue;
+          const int kq = ks2 * N + r;
+          const double p = ks2 >= 1 ? blk[r] : 0.0;
+          const double q = ks2 <= ns - 2 ? blk[(size_t)(N - 1) * N + r] : 0.0;
+          double x0 = tacc[mt][0], x1 = tacc[mt][1];
+          if (ks2 >= 1) {
+            x0 -= p * szz[(size_t)(ks2 - 1) * R + c0];
+            x1 -= p * szz[(size_t)(ks2 - 1) * R + c0 + 1];
+          }
+          if (ks2 <= ns - 2) {
+            x0 -= q * szz[(size_t)(ns - 1 + ks2) * R + c0];
+            x1 -= q * szz[(size_t)(ns - 1 + ks2) * R + c0 + 1];
+          }
+          if (ROLE == 3) {
+            *(double2*)(bb + (size_t)r * RS + c0) = make_double2(x0, x1);
+            continue;
+          }
+          const int ci = c0 / PER;
+          if (cj[ci] < 0) continue;
+          const bool second = ROLE == 0 && (c0 % 4) == 2;  // v of a u/v column
+          if (ROLE == 0 && !second && meanu && cii[ci] == 0 && cj[ci] == 0) {
+            x0 = meang[kq] * x0;
+            x1 = meang[kq] * x1;
+          }
+          P2 o;
+          o.x = (T)x0;
+          o.y = (T)x1;
+          *(P2*)((second ? F1 : F0) + fidx<T>(g, 2 * cii[ci], cj[ci], kq)) = o;
+        }
+        if (ROLE == 3) __syncwarp();
+      }
+    }
+    if (ROLE != 3) return;
+    // (2/h) D phi and the projection, per subdomain (phi of this warp's own
+    // subdomains, written above)
+    for (int ks2 = wid; ks2 < ns; ks2 += nwarp) {
+      const double* bb = sb + (size_t)ks2 * N * RS;
+      const double fac = g.hfac[ks2];
+      for (int nt = 0; nt < 2; ++nt) {
+        double tacc[kTcMT][2];
+        tc_block_product(sD, bb, N, nt, lane, tacc);
+        const int c0 = nt * 8 + 2 * t4, ci = c0 >> 1;
+        if (cj[ci] < 0) continue;
+        const int j = cj[ci], ii = cii[ci];
+#pragma unroll
+        for (int mt = 0; mt < kTcMT; ++mt) {
+          const int r = mt * 8 + gq;
+          if (mt >= MT || r >= N) continue;
+          const int kq = ks2 * N + r;
+          const size_t pr = fidx<T>(g, 2 * ii, j, kq);
+          P2 zu, zv, zw;
+          if (kq < kstart) {
+            zu.x = zu.y = (T)0;
+            *(P2*)(F0 + pr) = zu;
+            *(P2*)(F1 + pr) = zu;
+            *(P2*)(F2 + pr) = zu;
+            continue;
+          }
+          const double phr = bb[(size_t)r * RS + c0], phi = bb[(size_t)r * RS + c0 + 1];
+          const P2 w2 = *(const P2*)(F2 + pr);
+          double wbr = 0, wbi = 0;
+          if (!(ii == 0 && j == 0)) {
+            wbr = (double)w2.x - dt * (tacc[mt][0] * fac);
+            wbi = (double)w2.y - dt * (tacc[mt][1] * fac);
+          }
+          const double dtx = dt * g.xw[ii], dty = dt * g.yw[j];
+          const P2 u2 = *(const P2*)(F0 + pr), v2 = *(const P2*)(F1 + pr);
+          const double ur = (double)u2.x, ui = (double)u2.y, vr = (double)v2.x, vi = (double)v2.y;
+          zu.x = (T)(ur + dtx * phi);
+          zu.y = (T)(ui - dtx * phr);
+          zv.x = (T)(vr + dty * phi);
+          zv.y = (T)(vi - dty * phr);
+          zw.x = (T)wbr;
+          zw.y = (T)wbi;
+          *(P2*)(F0 + pr) = zu;
+          *(P2*)(F1 + pr) = zv;
+          *(P2*)(F2 + pr) = zw;
+        }
+      }
+    }
+    return;
+  }
   // x = A_ks^-1 b_ks - A_ks^-1 e_0 z_{ks-1} - A_ks^-1 e_{N-1} z_{ns-1+ks}
   double* x = acc;  // the solution replaces the product in place
   if (live) {
     const double* col = sA + offA + (size_t)bi.bmap[ks] * N * N + kk;
-    row_product16<ROLE == 3 ? 4 : 8>(col, sb + (size_t)ks * N * kSysRS, N, acc);
+    row_product16<ROLE == 3 ? 4 : 8>(col, sb + (size_t)ks * N * RS, N, acc);
     const double p = ks >= 1 ? col[0] : 0.0;
     const double q = ks <= ns - 2 ? col[(size_t)(N - 1) * N] : 0.0;
 #pragma unroll
@@ -2368,13 +2655,13 @@ __global__ void __maxnreg__(72) k_solve_sys(
   // pressure: phi into shared memory, (2/h) D phi, projection (calcuvwt.f:826-901)
   __syncthreads();  // every row of the RHS has been read
   if (live) {
-    double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
+    double2* d2 = (double2*)(sb + (size_t)k * RS);
 #pragma unroll
     for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(x[2 * q], x[2 * q + 1]);
   }
   __syncthreads();
   if (!live) return;
-  row_product16<ROLE == 3 ? 4 : 8>(sD + kk, sb + (size_t)ks * N * kSysRS, N, acc);
+  row_product16<ROLE == 3 ? 4 : 8>(sD + kk, sb + (size_t)ks * N * RS, N, acc);
   const double fac = g.hfac[ks];
 #pragma unroll
   for (int ci = 0; ci < NC; ++ci) {
@@ -2389,7 +2676,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
       *(P2*)(F2 + pr) = zu;
       continue;
     }
-    const double phr = sb[(size_t)k * kSysRS + 2 * ci], phi = sb[(size_t)k * kSysRS + 2 * ci + 1];
+    const double phr = sb[(size_t)k * RS + 2 * ci], phi = sb[(size_t)k * RS + 2 * ci + 1];
     const P2 w2 = *(const P2*)(F2 + pr);
     double wbr = 0, wbi = 0;
     if (!(ii == 0 && j == 0)) {

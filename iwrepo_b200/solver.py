@@ -151,12 +151,14 @@ class Solver:
 
     def autotune(self) -> dict:
         """Time this step's launch candidates and keep the fastest (y-tile
-        width, stage A / stage E variant); the state is not changed."""
+        width, stage A / stage E variant, solve variant); the state is not
+        changed."""
         ch = (C.c_int * 4)()
         _lib.check(_lib.lib().iw_autotune(self.h, ch))
-        names = {2: "register-split", 1: "register", 0: "tiled", -1: "n/a"}
+        names = {2: "tiled-bulk", 1: "register", 0: "tiled", -1: "n/a"}
+        solve = {0: "per-task", 1: "system-grouped", 2: "system-grouped-tensor-core"}
         return {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]],
-                "solve": "system-grouped" if ch[3] else "per-task"}
+                "solve": solve[ch[3]]}
 
     LAUNCH = {"y_tile": 0, "stage_a": 1, "stage_e": 2, "solve": 3}
 

@@ -205,9 +205,27 @@ def test_mixed_precision_vs_fp64():
         assert rel(a[q], b[q]) <= 1e-5, q
     # velocity vector as a whole
     assert rel(a[:3], b[:3]) <= 1e-5
-    # v only holds the seeded noise (1e-4 of the wave); FP32 rounding of the
-    # wave fields reaches it through the pressure projection (i ky phi)
+    # v only holds the seeded noise (1e-4 of the wave): the FP32 rounding of the
+    # wave shifts the advected noise pattern, and FP32-sized differences decide
+    # the interface averaging at points at its threshold
     assert rel(a[1], b[1]) <= 1e-3
+
+
+@pytest.mark.xfail(strict=False, reason="v, the noise-only field, misses the 1e-5 metric gate in mixed precision: "
+                                        "the FP32-stored wave advects it with a phase error and FP32-sized "
+                                        "differences flip interface-averaging decisions (see the precision notes)")
+def test_mixed_precision_v_within_metric_gate():
+    """The metric's gate (<= 1e-5 relative L2 in every field) applied to v:
+    kept as an expected failure so that the miss stays visible."""
+    from iwrepo_b200 import config as cf
+    import iwrepo_b200 as iw
+    c64 = cf.baseline("C0")
+    c32 = c64.replace(precision=cf.IW_PREC_MIXED)
+    a_s, b_s = iw.Solver(c32), iw.Solver(c64)
+    for s in (a_s, b_s):
+        s.init_mode1(0.05, 1e-4, 99)
+        s.step(100)
+    assert rel(a_s.state()[1], b_s.state()[1]) <= 1e-5
 
 
 def test_deterministic():

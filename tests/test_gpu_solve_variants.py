@@ -1,4 +1,4 @@
-"""The two block-inverse solve kernels give the same bits.
+"""The block-inverse solve kernels agree.
 
 k_solve_sys (one CTA per group of columns that share a system, tables staged
 in shared memory by bulk copies) and k_solve_cta (one CTA per task of <= 4
@@ -43,12 +43,64 @@ def test_grouped_solve_equals_per_task_solve(name):
         assert np.array_equal(a, b), name
 
 
+@pytest.mark.parametrize("name", list(CASES))
+def test_tensor_core_solve_matches_grouped_solve(name):
+    """The grouped solve with its block products on the FP64 tensor cores
+    (mma.sync m8n8k4) applies the same operators; only the rounding of each
+    product differs (1e-12 of the field in FP64 after 5 steps, 1e-5 in mixed
+    precision, where the FP32 storage rounds the difference up)."""
+    import iwrepo_b200 as iw
+    cfg = cf.Config(dt=1e-3, **CASES[name]).validate()
+    runs = []
+    for variant in (1, 2):
+        s = iw.Solver(cfg)
+        s.set_launch("solve", variant)
+        s.init_mode1(0.05, 1e-3, 17)
+        s.step(5)
+        runs.append([s.state(lev) for lev in range(5)])
+        s.close()
+    tol = 1e-12 if cfg.precision == cf.IW_PREC_FP64 else 1e-5
+    for a, b in zip(*runs):
+        for q in range(4):
+            n = np.linalg.norm(a[q])
+            assert np.linalg.norm(a[q] - b[q]) <= tol * (n if n > 0 else 1.0), (name, q)
+
+
+@pytest.mark.parametrize("precision", [cf.IW_PREC_FP64, cf.IW_PREC_MIXED])
+@pytest.mark.parametrize("nzloc", [17, 33, 40])
+def test_stage_e_variants_give_the_same_bits(precision, nzloc):
+    """Stage E as a tiled kernel (0), a register-column kernel (1) or the
+    tiled kernel with its input tiles staged by bulk asynchronous copies (2).
+    Variants 0 and 2 run every sum in the same order and give the same bits;
+    the register-column kernel rounds differently (1e-11 of the field in
+    FP64, 1e-5 in mixed precision after 4 steps)."""
+    import iwrepo_b200 as iw
+    cfg = cf.Config(nx=16, ny=16, nzloc=nzloc, nsubd=3, dt=1e-3, precision=precision).validate()
+    runs = {}
+    for variant in (0, 1, 2) if nzloc <= 33 else (0, 2):
+        s = iw.Solver(cfg)
+        s.set_launch("stage_e", variant)
+        s.init_mode1(0.05, 1e-3, 23)
+        s.step(4)
+        runs[variant] = [s.state(lev) for lev in range(5)]
+        s.close()
+    for a, b in zip(runs[0], runs[2]):
+        assert np.array_equal(a, b)
+    if 1 not in runs:
+        return
+    tol = 1e-11 if precision == cf.IW_PREC_FP64 else 1e-5
+    for a, b in zip(runs[0], runs[1]):
+        for q in range(4):
+            n = np.linalg.norm(b[q])
+            assert np.linalg.norm(a[q] - b[q]) <= tol * (n if n > 0 else 1.0), q
+
+
 def test_autotune_reports_the_solve_variant():
     import iwrepo_b200 as iw
     cfg = cf.Config(nx=32, ny=32, nzloc=17, nsubd=4, dt=1e-3, precision=cf.IW_PREC_MIXED).validate()
     s = iw.Solver(cfg)
     s.init_mode1(0.05, 1e-4, 3)
     ch = s.autotune()
-    assert ch["solve"] in ("system-grouped", "per-task")
+    assert ch["solve"] in ("system-grouped", "system-grouped-tensor-core", "per-task")
     s.step(2)
     s.close()
