@@ -291,14 +291,14 @@ int iw_run(iw_handle *h, int nsteps, int use_graph);
  * memory, their block products on the FP64 pipes or on the FP64 tensor cores,
  * or one CTA per task of <= 4 right-hand sides).  Candidates run on the
  * handle's scratch fields; the state is not changed (the solver tables are
- * built if no step has built them yet).  The tiled stage variants give the
- * same bits; the solve variants 0 and 1 give the same bits, the tensor-core
- * products round differently (an FP64 rounding per product).
+ * built if no step has built them yet).  The stage-A variants and the solve
+ * variants 0 and 1 give the same bits; the stage-E variants and the
+ * tensor-core products round differently.
  * choices (optional, 4 ints): the y-tile width; for stage A and stage E
  * 1 = register-column, 0 = tiled, -1 = not applicable (stage E also 2 =
- * tiled with the input tiles staged by bulk copies, N <= 64); the solve variant
- * (1 = system-grouped, 2 = system-grouped on the tensor cores, N <= 40,
- * 0 = per task). */
+ * tiled with the input tiles staged by bulk copies, N <= 64); the pressure
+ * solve's variant (1 = system-grouped, 2 = system-grouped on the tensor cores,
+ * N <= 40, 0 = per task; each solve role keeps its own fastest). */
 int iw_autotune(iw_handle *h, int *choices);
 
 /* Not in the reference.  Sets one launch choice of iw_autotune directly. */

@@ -392,6 +392,7 @@ struct iw_handle {
   int ntask2[SYS_KINDS] = {0, 0, 0, 0};
   int nold[SYS_KINDS] = {0, 0, 0, 0};
   int use_sys = 1;  // 0: k_solve_cta for every task, 1: k_solve_sys, 2: k_solve_sys on the FP64 tensor cores
+  int sys_role[4] = {-1, -1, -1, -1};  // per solve role (u/v, w, rho, pressure), set by iw_autotune; -1: use_sys
   double bi_bdfv[SYS_KINDS] = {-1, -1, -1, -1};
   bool bi_fold[SYS_KINDS] = {false, false, false, false};  // Legendre filter folded into ainv
   // distinct subdomain blocks: subdomain ks uses block bmap[ks]; brep[b] is a
@@ -1377,11 +1378,12 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   const int nref = h->nrefine[kind], nt = h->ntask[kind];
   const bool fold = h->bi_fold[kind] && cpen;
   // system-grouped kernel for the tasks after the prefix, when it applies
-  // (use_sys 2: the block products on the FP64 tensor cores, N <= 40)
-  const bool tc = h->use_sys == 2 && h->N <= 8 * kTcMT;
-  const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3, tc ? kTcRS : kSysRS);
+  // (variant 2: the block products on the FP64 tensor cores, N <= 40)
+  const int us = h->sys_role[role] >= 0 ? h->sys_role[role] : h->use_sys;
+  const bool tc = us == 2 && h->N <= 8 * kTcMT;
+  const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3, tc ? kTcRS : kSysRS, tc ? tc_ap(h->N) : 0);
   const size_t smsys = lay.total * sizeof(double);
-  const bool grouped = h->use_sys && h->nz <= kSysMaxRows && (!cpen || fold) && smsys <= 200 * 1024;
+  const bool grouped = us && h->nz <= kSysMaxRows && (!cpen || fold) && smsys <= 200 * 1024;
   const int nend = grouped ? std::max(h->nold[kind], nref) : nt;
   if (grouped && h->ntask2[kind] > 0) {
     const int nthr = (h->nz + 31) / 32 * 32;
@@ -1629,21 +1631,21 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
       h->use_bi) {
     const int cpen = (h->p.ispecfilterexp == 1) && ((h->istep + 1) % h->p.nspecfilterexp == 0);
     const int kstart = h->p.bc_variant == IW_BC_NOSLIP ? 1 : 0;
-    // every solve role of a step: pressure, u/v, w, rho
-    float best = 0;
-    int bestv = 1;
-    for (int v = 0; v < 3; ++v) {
-      if (v == 2 && h->N > 8 * kTcMT) continue;
-      h->use_sys = v;
-      const float t = timeit([&] {
-        for (int role : {3, 0, 1, 2}) launch_solve_bi<T>(h, ts, role, cpen, kstart);
-      });
-      if (v == 0 || t < best) {
-        best = t;
-        bestv = v;
+    // each solve role (pressure, u/v, w, rho) keeps its own fastest variant
+    for (int role : {3, 0, 1, 2}) {
+      float best = 0;
+      int bestv = 1;
+      for (int v = 0; v < 3; ++v) {
+        if (v == 2 && h->N > 8 * kTcMT) continue;
+        h->sys_role[role] = v;
+        const float t = timeit([&] { launch_solve_bi<T>(h, ts, role, cpen, kstart); });
+        if (v == 0 || t < best) {
+          best = t;
+          bestv = v;
+        }
       }
+      h->sys_role[role] = bestv;
     }
-    h->use_sys = bestv;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1653,13 +1655,14 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
     h->tune_a = save[1];
     h->tune_e = save[2];
     h->use_sys = save[3];
+    for (int& r : h->sys_role) r = -1;
     return set_err(IW_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(err));
   }
   if (choice) {
     choice[0] = h->tune_ytx;
     choice[1] = h->tune_a;
     choice[2] = h->tune_e;
-    choice[3] = h->use_sys;
+    choice[3] = h->sys_role[3] >= 0 ? h->sys_role[3] : h->use_sys;
   }
   return IW_OK;
 }
@@ -2162,6 +2165,7 @@ int iw_set_launch(iw_handle* h, int which, int value) {
       if (value < 0 || value > 2) return set_err(IW_ERR_CONFIG, "solve variant: 0, 1 or 2");
       if (value == 2 && h->N > 8 * kTcMT) return set_err(IW_ERR_CONFIG, "tensor-core solve needs N <= 40");
       h->use_sys = value;
+      for (int& r : h->sys_role) r = -1;
       return IW_OK;
     default:
       return set_err(IW_ERR_CONFIG, "unknown launch choice");

@@ -97,8 +97,8 @@ __device__ __forceinline__ T proj_val(const Geo& g, const T* __restrict__ f, int
   return f[fidx<T>(g, i, j, k)];
 }
 
-// Roundings written out (no contraction left to the compiler), so that the
-// variants of a stage give the same bits whatever their loop structure.
+// Roundings written out (no contraction left to the compiler): the tiled and
+// register-column stage A give the same bits whatever their loop structure.
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float mul_t(float a, float b) { return __fmul_rn(a, b); }
@@ -550,6 +550,11 @@ struct Coefs {
 // make bdf1 + bdf2 + bdf3 differ from bdfv and bias every step the same way.
 template <typename T>
 __device__ __forceinline__ T bdf_combine(const Coefs& c, T se, T F2, T fn, T fnm) {
+  return (T)(c.dt * (double)se + c.bdf1 * (double)F2 + c.bdf2 * (double)fn + c.bdf3 * (double)fnm);
+}
+// the same with every rounding written out
+template <typename T>
+__device__ __forceinline__ T bdf_combine_rn(const Coefs& c, T se, T F2, T fn, T fnm) {
   return (T)__fma_rn(c.bdf3, (double)fnm,
                      __fma_rn(c.bdf2, (double)fn, __fma_rn(c.bdf1, (double)F2, __dmul_rn(c.dt, (double)se))));
 }
@@ -562,7 +567,7 @@ __device__ __forceinline__ void stageE_point(const Coefs& c, T fac, T f1, T f2, 
                                              T fn, T fnm, T& S, T& fsv) {
   S = fma_t(dz, fac, b);
   const T se = fma_t(f3, snm, fma_t(f2, sn, mul_t(f1, S)));
-  fsv = bdf_combine<T>(c, se, F2, fn, fnm);
+  fsv = bdf_combine_rn<T>(c, se, F2, fn, fnm);
 }
 // the extrapolated S in FP64 at the walls (the wall data of w)
 template <typename T>
@@ -618,18 +623,20 @@ __device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, con
       const T* dr = sD + k1 * N;
       T s = 0;
 #pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) s = fma_t(dr[k2], tz[k2 * kTX + lane], s);
+      for (int k2 = 0; k2 < N; ++k2) s += dr[k2] * tz[k2 * kTX + lane];
+      const T S = a.B[q][p] + s * fac;
       const T sn = a.Snold[q][p];
       const T snm = a.Snm_w[q][p];
+      if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
+        const int side = kk == 0 ? 0 : 1;
+        a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] =
+            (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
+      }
+      const T se = f1 * S + f2 * sn + f3 * snm;
       const T F2 = proj_val<T>(g, a.F1[q], i, j, kk);
       const T fn = a.Fn[q][p];
       const T fnm = a.Fnm_w[q][p];
-      T S;
-      stageE_point<T>(c, fac, f1, f2, f3, a.B[q][p], s, sn, snm, F2, fn, fnm, S, fsv);
-      if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
-        const int side = kk == 0 ? 0 : 1;
-        a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] = stageE_wall<T>(f1, f2, f3, S, sn, snm);
-      }
+      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
       a.Snm_w[q][p] = S;
       a.Fnm_w[q][p] = F2;
     }
@@ -648,8 +655,9 @@ __device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, con
       const double* lr = sL + k1 * N;
       double s = 0;
 #pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) s = __fma_rn(lr[k2], (double)tf[k2 * kTX + lane], s);
-      o = (T)stageE_filtered((double)tf[k1 * kTX + lane], s, cfm1);
+      for (int k2 = 0; k2 < N; ++k2) s += lr[k2] * (double)tf[k2 * kTX + lane];
+      const double gv = (double)tf[k1 * kTX + lane] + s;  // L f = f + (L - I) f
+      o = (T)(gv + cfm1 * gv);                            // cf g = g + (cf - 1) g
     } else {
       o = tf[k1 * kTX + lane];
     }
@@ -658,7 +666,8 @@ __device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, con
 }
 
 // Tiled K_E with its input tiles staged by bulk asynchronous copies: the
-// same CTA tiling and the same sums as stageE_tile (so the same bits), but
+// same CTA tiling and the same sums in the same order as stageE_tile (with
+// every rounding written out, so it agrees to rounding), but
 // every row of the seven input tiles (Z, B, S_n, S_{n-1}, F1, F_n, F_{n-1})
 // is requested at once, one cp.async.bulk per row completing on an mbarrier
 // (Z on its own, so that D Z starts while the rest lands), instead of a
@@ -673,21 +682,32 @@ template <typename T>
 __host__ __device__ inline int eb_rs() {  // tile row stride (elements): 32 points and room for the offset
   return kTX + 16 / (int)sizeof(T);
 }
+__host__ __device__ inline int eb_np(int N) { return (N + 1) & ~1; }  // operator row stride: pairs stay aligned
 template <typename T>
 __host__ inline size_t eb_smem(int N) {
-  return 16 + (size_t)kEBArr * N * eb_rs<T>() * sizeof(T) + (size_t)N * N * sizeof(double) +
-         (size_t)N * N * sizeof(T) + (size_t)N * kTX * sizeof(T);
+  return 16 + (size_t)kEBArr * N * eb_rs<T>() * sizeof(T) + (size_t)N * eb_np(N) * sizeof(double) +
+         (size_t)N * eb_np(N) * sizeof(T) + (size_t)N * kTX * sizeof(T);
+}
+// two consecutive operator entries (an 8-byte broadcast load for FP32)
+__device__ __forceinline__ void ld_pair(const float* p, float& a, float& b) {
+  const float2 v = *(const float2*)p;
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ld_pair(const double* p, double& a, double& b) {
+  a = p[0];
+  b = p[1];
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs c, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int N = g.N, RS = eb_rs<T>();
+  const int N = g.N, RS = eb_rs<T>(), NP = eb_np(N);
   uint64_t* bar = (uint64_t*)smraw;  // [0]: Z, [1]: the other six tiles
   T* tiles = (T*)(smraw + 16);       // [arr][k][RS]
-  double* sL = (double*)(tiles + (size_t)kEBArr * N * RS);
-  T* sD = (T*)(sL + N * N);
-  T* tf = sD + N * N;  // N*kTX: F* tile
+  double* sL = (double*)(tiles + (size_t)kEBArr * N * RS);  // [k1][NP]: L - I
+  T* sD = (T*)(sL + N * NP);                                 // [k1][NP]
+  T* tf = sD + N * NP;  // N*kTX: F* tile
   const int q = blockIdx.z;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int i0 = blockIdx.x * kTX, i = i0 + lane;
@@ -715,8 +735,9 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
     bulk_g2s(tiles + (size_t)t * RS, (const void*)(ga - off), bytes, b);
   }
   for (int t = tid; t < N * N; t += blockDim.x) {
-    sD[t] = (T)g.D[t];
-    sL[t] = g.Lfil[t] - (t / N == t % N ? 1.0 : 0.0);
+    const int r = t / N, cc = t - r * N;
+    sD[r * NP + cc] = (T)g.D[t];
+    sL[r * NP + cc] = g.Lfil[t] - (r == cc ? 1.0 : 0.0);
   }
   // element offset of this CTA's first point inside each copied row (the
   // same for every row: the planes are whole 16-byte units)
@@ -728,20 +749,36 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
   const bool act = i < g.nxpp;
   const T fac = (T)g.hfac[ks];
   const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
-  // D Z for this warp's rows, kept in registers until the other tiles land
+  // D Z for this warp's rows (k1 = w + 8 r), all rows at once: each column
+  // value feeds every row, each pair of operator entries is one broadcast
+  // load; the sums run over k2 in order, as in the one-row-per-pass kernel.
+  // Lanes past the field's end compute on stale tile entries and store nothing.
   constexpr int kMaxRows = 8;  // N <= 8 * kTW = 64
   T dz[kMaxRows];
-  const T* tz = tiles;  // Z tile
 #pragma unroll
-  for (int r = 0; r < kMaxRows; ++r) {
-    const int k1 = w + kTW * r;
-    dz[r] = 0;
-    if (k1 < N && act) {
-      const T* dr = sD + k1 * N;
-      T s = 0;
-#pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) s = fma_t(dr[k2], tz[k2 * RS + eo + lane], s);
-      dz[r] = s;
+  for (int r = 0; r < kMaxRows; ++r) dz[r] = 0;
+  const T* zc = tiles + eo + lane;  // this lane's column of the Z tile
+  {
+    int k2 = 0;
+    for (; k2 + 1 < N; k2 += 2) {
+      const T z0 = zc[k2 * RS], z1 = zc[(k2 + 1) * RS];
+#pragma unroll
+      for (int r = 0; r < kMaxRows; ++r) {
+        const int k1 = w + kTW * r;
+        if (k1 < N) {
+          T d0, d1;
+          ld_pair(sD + k1 * NP + k2, d0, d1);
+          dz[r] = fma_t(d1, z1, fma_t(d0, z0, dz[r]));
+        }
+      }
+    }
+    if (k2 < N) {
+      const T z0 = zc[k2 * RS];
+#pragma unroll
+      for (int r = 0; r < kMaxRows; ++r) {
+        const int k1 = w + kTW * r;
+        if (k1 < N) dz[r] = fma_t(sD[k1 * NP + k2], z0, dz[r]);
+      }
     }
   }
   const bool ok1 = mbar_wait(&bar[1], 0, 2000000000ull);
@@ -789,18 +826,26 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
   __syncthreads();
   if (!act) return;
   const double cfm1 = a.filter ? g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0 : 0.0;
-  for (int k1 = w; k1 < N; k1 += kTW) {
-    T o;
-    if (a.filter) {
-      const double* lr = sL + k1 * N;
-      double s = 0;
-#pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) s = __fma_rn(lr[k2], (double)tf[k2 * kTX + lane], s);
-      o = (T)stageE_filtered((double)tf[k1 * kTX + lane], s, cfm1);
-    } else {
-      o = tf[k1 * kTX + lane];
+  if (!a.filter) {
+    for (int k1 = w; k1 < N; k1 += kTW) a.F[q][fidx<T>(g, i, j, ks * N + k1)] = tf[k1 * kTX + lane];
+    return;
+  }
+  // (L - I) F* in FP64 for all of this warp's rows at once, sums in k2 order
+  double s2[kMaxRows];
+#pragma unroll
+  for (int r = 0; r < kMaxRows; ++r) s2[r] = 0.0;
+  for (int k2 = 0; k2 < N; ++k2) {
+    const double f = (double)tf[k2 * kTX + lane];
+#pragma unroll
+    for (int r = 0; r < kMaxRows; ++r) {
+      const int k1 = w + kTW * r;
+      if (k1 < N) s2[r] = __fma_rn(sL[k1 * NP + k2], f, s2[r]);
     }
-    a.F[q][fidx<T>(g, i, j, ks * N + k1)] = o;
+  }
+#pragma unroll
+  for (int r = 0; r < kMaxRows; ++r) {
+    const int k1 = w + kTW * r;
+    if (k1 < N) a.F[q][fidx<T>(g, i, j, ks * N + k1)] = (T)stageE_filtered((double)tf[k1 * kTX + lane], s2[r], cfm1);
   }
 }
 
@@ -931,11 +976,12 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
       const size_t p = (size_t)kk * g.plane + t;
       T s = 0;
 #pragma unroll
-      for (int k2 = 0; k2 < NM; ++k2) s = fma_t(op.D[k1 * NM + k2], zc[k2], s);
-      T S;
-      stageE_point<T>(c, fac, f1, f2, f3, b, s, sn, snm, F2, fn, fnm, S, fsv);
+      for (int k2 = 0; k2 < NM; ++k2) s += op.D[k1 * NM + k2] * zc[k2];
+      const T S = b + s * fac;
       if (q == 2 && ((kk == 0) || (kk == g.nz - 1)))
-        a.wnl[t + (kk == 0 ? 0 : g.plane)] = stageE_wall<T>(f1, f2, f3, S, sn, snm);
+        a.wnl[t + (kk == 0 ? 0 : g.plane)] = (double)f1 * (double)S + (double)f2 * (double)sn + (double)f3 * (double)snm;
+      const T se = f1 * S + f2 * sn + f3 * snm;
+      fsv = bdf_combine<T>(c, se, F2, fn, fnm);
       Snmq[p] = S;
       Fnmq[p] = F2;
     }
@@ -949,8 +995,9 @@ __global__ void __launch_bounds__(128) k_stageE_r(Geo g, EArgs<T> a, Coefs c, co
       if (a.filter) {
         double s = 0;
 #pragma unroll
-        for (int k2 = 0; k2 < NM; ++k2) s = __fma_rn(op.L[k1 * NM + k2], (double)fs[k2], s);  // (L - I) f in FP64
-        o = (T)stageE_filtered((double)fs[k1], s, cfm1);
+        for (int k2 = 0; k2 < NM; ++k2) s += op.L[k1 * NM + k2] * (double)fs[k2];  // (L - I) f in FP64
+        const double gv = (double)fs[k1] + s;
+        o = (T)(gv + cfm1 * gv);
       } else {
         o = fs[k1];
       }
@@ -2204,17 +2251,18 @@ constexpr int kSysMaxRows = 512;
 struct SysSmem {  // offsets (doubles) of the shared-memory regions of k_solve_sys
   size_t a, l, m, b, rz, zz, d, total;
 };
-__host__ __device__ inline SysSmem sys_smem(int n, int N, int ns, int nb, bool dmat, int rs = kSysRS) {
+__host__ __device__ inline SysSmem sys_smem(int n, int N, int ns, int nb, bool dmat, int rs = kSysRS, int ap = 0) {
   SysSmem o;
   const size_t m = 2 * (size_t)(ns - 1), m1 = m > 0 ? m : 1;
+  if (ap <= 0) ap = N;
   o.a = 0;
-  o.l = ((size_t)nb * N * N + 3) & ~(size_t)1;  // room for a copy that starts one double early
+  o.l = ((size_t)nb * N * ap + 3) & ~(size_t)1;  // room for a copy that starts one double early
   o.m = o.l + m * N;
   o.b = o.m + m * m;
   o.rz = o.b + (size_t)n * rs;
   o.zz = o.rz + kSysR * m1;
   o.d = o.zz + kSysR * m1;
-  o.total = o.d + (dmat ? (((size_t)N * N + 1) & ~(size_t)1) : 0);
+  o.total = o.d + (dmat ? (((size_t)N * ap + 1) & ~(size_t)1) : 0);
   return o;
 }
 
@@ -2254,10 +2302,21 @@ __device__ __forceinline__ void row_product16(const double* col, const double* b
 // of 8, 4 columns of Op per instruction, the padding of the ragged N read as
 // zeros.  Lane (g, t4) = (lane / 4, lane % 4) ends with
 // X[8 mt + g][8 nt + 2 t4 + {0, 1}]: one complex value of one column.  The
-// right-hand-side rows have a stride of 20 doubles, so that the 4 rows x 8
-// values of a B fragment fall in two shared-memory wavefronts.
-constexpr int kTcRS = 20;
+// right-hand-side rows keep the stride of 18 doubles (a B fragment then takes
+// four shared-memory wavefronts instead of two, but a stride of 20 would cost
+// the second resident CTA per SM at C3's sizes); the operators get rows of
+// tc_ap(N) doubles, which makes the five A fragments per step conflict-free.
+constexpr int kTcRS = 18;
 constexpr int kTcMT = 5;  // row tiles per subdomain: N <= 40
+
+// Row stride of the operators staged for the tensor-core products: = 4
+// (mod 8) doubles, so that an A fragment (8 rows x 4 columns of 8 bytes) falls
+// in two shared-memory wavefronts.
+__host__ __device__ inline int tc_ap(int N) {
+  int a = N;
+  while (a % 8 != 4) ++a;
+  return a;
+}
 
 __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
   asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -2265,15 +2324,16 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
       : "d"(a), "d"(b));
 }
 
-// acc[mt] = (Op B)[8 mt + g][8 nt + 2 t4 + {0, 1}] for Op(r, c) = op[c N + r] and
+// acc[mt] = (Op B)[8 mt + g][8 nt + 2 t4 + {0, 1}] for Op(r, c) = op[c ap + r] and
 // B(c, :) = bb[c kTcRS + :], c < N
-__device__ __forceinline__ void tc_block_product(const double* op, const double* bb, int N, int nt, int lane,
+__device__ __forceinline__ void tc_block_product(const double* op, int ap, const double* bb, int N, int nt, int lane,
                                                  double (&acc)[kTcMT][2]) {
   const int g = lane >> 2, t4 = lane & 3;
   const int MT = (N + 7) >> 3, KT = (N + 3) >> 2;
   __syncwarp();  // mma.sync wants the whole warp converged
 #pragma unroll
   for (int mt = 0; mt < kTcMT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+#pragma unroll 3
   for (int kt = 0; kt < KT; ++kt) {
     const int c = kt * 4 + t4;
     const bool cin = c < N;
@@ -2284,8 +2344,37 @@ __device__ __forceinline__ void tc_block_product(const double* op, const double*
       if (mt < MT) {
         const int r = mt * 8 + g;
         const bool rin = r < N;
-        const double a = (cin && rin) ? op[(size_t)cc * N + (rin ? r : N - 1)] : 0.0;
+        const double a = (cin && rin) ? op[(size_t)cc * ap + (rin ? r : N - 1)] : 0.0;
         dmma884(acc[mt][0], acc[mt][1], a, b);
+      }
+    }
+  }
+}
+// both halves of the 16 right-hand sides at once (each A fragment loaded once)
+__device__ __forceinline__ void tc_block_product2(const double* op, int ap, const double* bb, int N, int lane,
+                                                  double (&acc)[2][kTcMT][2]) {
+  const int g = lane >> 2, t4 = lane & 3;
+  const int MT = (N + 7) >> 3, KT = (N + 3) >> 2;
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int mt = 0; mt < kTcMT; ++mt) acc[h][mt][0] = acc[h][mt][1] = 0.0;
+#pragma unroll 3
+  for (int kt = 0; kt < KT; ++kt) {
+    const int c = kt * 4 + t4;
+    const bool cin = c < N;
+    const int cc = cin ? c : N - 1;
+    const double b0 = cin ? bb[(size_t)cc * kTcRS + g] : 0.0;
+    const double b1 = cin ? bb[(size_t)cc * kTcRS + 8 + g] : 0.0;
+#pragma unroll
+    for (int mt = 0; mt < kTcMT; ++mt) {
+      if (mt < MT) {
+        const int r = mt * 8 + g;
+        const bool rin = r < N;
+        const double a = (cin && rin) ? op[(size_t)cc * ap + (rin ? r : N - 1)] : 0.0;
+        dmma884(acc[0][mt][0], acc[0][mt][1], a, b0);
+        dmma884(acc[1][mt][0], acc[1][mt][1], a, b1);
       }
     }
   }
@@ -2323,7 +2412,8 @@ __global__ void __maxnreg__(72) k_solve_sys(
   const int n = g.nz, N = g.N, ns = g.ns, m = 2 * (ns - 1), nb = bi.nb;
   const int tid = threadIdx.x;
   const int s = tk.sys;
-  const SysSmem L = sys_smem(n, N, ns, nb, ROLE == 3, RS);
+  const int AP = TC ? tc_ap(N) : N;  // operator row stride in shared memory
+  const SysSmem L = sys_smem(n, N, ns, nb, ROLE == 3, RS, AP);
   double* sA = sm + L.a;
   double* sL = sm + L.l;
   double* sM = sm + L.m;
@@ -2344,15 +2434,32 @@ __global__ void __maxnreg__(72) k_solve_sys(
   }
   __syncthreads();
   if (tid == 0) {
-    mbar_expect_tx(&bar, bytesA + bytesL + bytesM);
-    bulk_g2s(sA, (const void*)(ga - (uintptr_t)offA * 8), bytesA, &bar);
+    // (the tensor-core variant stages the inverse blocks itself, below, in
+    // rows of AP doubles)
+    mbar_expect_tx(&bar, (TC ? 0u : bytesA) + bytesL + bytesM);
+    if (!TC) bulk_g2s(sA, (const void*)(ga - (uintptr_t)offA * 8), bytesA, &bar);
     if (m > 0) {
       bulk_g2s(sL, bi.lvec + (size_t)s * m * N, bytesL, &bar);
       bulk_g2s(sM, bi.minv + (size_t)s * m * m, bytesM, &bar);
     }
   }
-  if (ROLE == 3)
-    for (int q = tid; q < N * N; q += blockDim.x) sD[q] = Dt[q];
+  if (TC) {
+    const double* ag = (const double*)bi.ainv + (size_t)s * nb * N * N;
+    for (int q = tid; q < nb * N * N; q += blockDim.x) {
+      const int c = q / N, r = q - c * N;  // c runs over the blocks' columns
+      sA[(size_t)c * AP + r] = ag[q];
+    }
+  }
+  if (ROLE == 3) {
+    if (TC) {
+      for (int q = tid; q < N * N; q += blockDim.x) {
+        const int c = q / N, r = q - c * N;
+        sD[(size_t)c * AP + r] = Dt[q];
+      }
+    } else {
+      for (int q = tid; q < N * N; q += blockDim.x) sD[q] = Dt[q];
+    }
+  }
   const double eps = bi.sys[s].eps;
   const double dt = g.dt;
   const int k = tid;
@@ -2406,7 +2513,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
         const double fac = g.hfac[ks2];
         for (int nt = 0; nt < 2; ++nt) {
           double tacc[kTcMT][2];
-          tc_block_product(sD, bb, N, nt, lane, tacc);
+          tc_block_product(sD, AP, bb, N, nt, lane, tacc);
           __syncwarp();
           const int c0 = nt * 8 + 2 * t4, ci = c0 >> 1;
 #pragma unroll
@@ -2518,11 +2625,23 @@ __global__ void __maxnreg__(72) k_solve_sys(
     const int gq = lane >> 2, t4 = lane & 3, MT = (N + 7) >> 3;
     for (int ks2 = wid; ks2 < ns; ks2 += nwarp) {
       double* bb = sb + (size_t)ks2 * N * RS;
-      const double* blk = sA + offA + (size_t)bi.bmap[ks2] * N * N;
+      const double* blk = sA + (size_t)bi.bmap[ks2] * N * AP;
+      // the pressure writes phi over its own right-hand side, half by half;
+      // the other roles store to the fields and take both halves at once
+      double tacc2[2][kTcMT][2];
+      if (ROLE != 3) tc_block_product2(blk, AP, bb, N, lane, tacc2);
       for (int nt = 0; nt < 2; ++nt) {
         double tacc[kTcMT][2];
-        tc_block_product(blk, bb, N, nt, lane, tacc);
-        if (ROLE == 3) __syncwarp();
+        if (ROLE == 3) {
+          tc_block_product(blk, AP, bb, N, nt, lane, tacc);
+          __syncwarp();
+        } else {
+#pragma unroll
+          for (int mt = 0; mt < kTcMT; ++mt) {
+            tacc[mt][0] = tacc2[nt][mt][0];
+            tacc[mt][1] = tacc2[nt][mt][1];
+          }
+        }
         const int c0 = nt * 8 + 2 * t4;
 #pragma unroll
         for (int mt = 0; mt < kTcMT; ++mt) {
@@ -2530,7 +2649,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
           if (mt >= MT || r >= N) continue;
           const int kq = ks2 * N + r;
           const double p = ks2 >= 1 ? blk[r] : 0.0;
-          const double q = ks2 <= ns - 2 ? blk[(size_t)(N - 1) * N + r] : 0.0;
+          const double q = ks2 <= ns - 2 ? blk[(size_t)(N - 1) * AP + r] : 0.0;
           double x0 = tacc[mt][0], x1 = tacc[mt][1];
           if (ks2 >= 1) {
             x0 -= p * szz[(size_t)(ks2 - 1) * R + c0];
@@ -2567,7 +2686,7 @@ __global__ void __maxnreg__(72) k_solve_sys(
       const double fac = g.hfac[ks2];
       for (int nt = 0; nt < 2; ++nt) {
         double tacc[kTcMT][2];
-        tc_block_product(sD, bb, N, nt, lane, tacc);
+        tc_block_product(sD, AP, bb, N, nt, lane, tacc);
         const int c0 = nt * 8 + 2 * t4, ci = c0 >> 1;
         if (cj[ci] < 0) continue;
         const int j = cj[ci], ii = cii[ci];

