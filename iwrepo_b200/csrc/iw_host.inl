@@ -971,7 +971,8 @@ static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
 
 template <typename T>
 static bool stageE_b_fits(const iw_handle* h) {
-  return h->N <= 8 * kTW && eb_smem<T>(h->N) <= 200 * 1024 && (h->plane * sizeof(T)) % 16 == 0;
+  const int nm = zop_bucket(h->N);
+  return nm > 0 && eb_smem<T>(h->N, nm) <= 200 * 1024 && (h->plane * sizeof(T)) % 16 == 0;
 }
 
 template <typename T>
@@ -993,13 +994,26 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   // The register-column stage E holds two columns per thread; past these sizes
   // its register count costs more occupancy than the tiled kernel loses.
   // tune_e = 2: the tiled kernel with its input tiles staged by bulk copies
-  // (N <= 64, shared memory permitting)
+  // and its z operators unrolled at the register-column bucket size (N <= 33)
   if (h->tune_e == 2 && stageE_b_fits<T>(h)) {
     dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
-    const size_t smem = eb_smem<T>(h->N);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_stageE_b<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_stageE_b<T><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c, h->derr);
+    const int nm = zop_bucket(h->N);
+    const size_t smem = eb_smem<T>(h->N, nm);
+    switch (nm) {
+#define IW_EBCASE(NM)                                                                                           \
+  case NM:                                                                                                      \
+    cudaFuncSetAttribute(k_stageE_b<T, NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
+    k_stageE_b<T, NM><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c, h->derr);                             \
     return;
+      IW_EBCASE(9)
+      IW_EBCASE(17)
+      IW_EBCASE(21)
+      IW_EBCASE(25)
+      IW_EBCASE(29)
+      IW_EBCASE(33)
+#undef IW_EBCASE
+      default: break;
+    }
   }
   const int emax = sizeof(T) == 4 ? 25 : 17;
   const bool reg = h->tune_e < 0 ? h->N <= emax : h->tune_e == 1;
@@ -1611,7 +1625,7 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
   }
   {
     // 0 tiled (any N), 1 register-column (N in a register bucket), 2 tiled
-    // with bulk-copied input tiles (N <= 64)
+    // with bulk-copied input tiles (N in a register bucket)
     float bt = 0;
     for (int v = 0; v < 3; ++v) {
       if ((v == 1 && !zop_bucket(h->N)) || (v == 2 && !stageE_b_fits<T>(h))) continue;
@@ -2158,7 +2172,7 @@ int iw_set_launch(iw_handle* h, int which, int value) {
         return set_err(IW_ERR_CONFIG, "stage variant: -1, 0, 1 (or 2 for stage E)");
       if (value == 1 && !zop_bucket(h->N)) return set_err(IW_ERR_CONFIG, "register-column stages need N <= 33");
       if (value == 2 && !(h->mixed ? stageE_b_fits<float>(h) : stageE_b_fits<double>(h)))
-        return set_err(IW_ERR_CONFIG, "bulk-staged stage E needs N <= 64 and its tiles in shared memory");
+        return set_err(IW_ERR_CONFIG, "bulk-staged stage E needs N <= 33 and whole 16-byte planes");
       (which == IW_LAUNCH_STAGE_A ? h->tune_a : h->tune_e) = value;
       return IW_OK;
     case IW_LAUNCH_SOLVE:

@@ -665,13 +665,17 @@ __device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, con
   }
 }
 
-// Tiled K_E with its input tiles staged by bulk asynchronous copies: the
-// same CTA tiling and the same sums in the same order as stageE_tile (with
-// every rounding written out, so it agrees to rounding), but
-// every row of the seven input tiles (Z, B, S_n, S_{n-1}, F1, F_n, F_{n-1})
-// is requested at once, one cp.async.bulk per row completing on an mbarrier
-// (Z on its own, so that D Z starts while the rest lands), instead of a
-// chain of dependent 4-byte loads per output row.  A row of 32 points is
+// Tiled K_E with its input tiles staged by bulk asynchronous copies and the
+// z operators unrolled at a compile-time size NM >= N (the zero-padded
+// bucket of the register-column kernels).  The CTA tiling is stageE_tile's
+// (32 x points of one (y, subdomain), 8 warps) and so are the sums, in the
+// same order (every rounding written out, so it agrees to rounding).  The
+// seven input tiles (Z, B, S_n, S_{n-1}, F1, F_n, F_{n-1}) are requested at
+// once, one cp.async.bulk per row completing on an mbarrier (Z on its own,
+// so that D Z starts while the rest lands).  Warp w computes all of its
+// output rows k1 = w + 8 r at once, so each column value feeds every row and
+// each pair of operator entries is one 8-byte broadcast; with NM known every
+// shared-memory address is a base plus an immediate.  A row of 32 points is
 // copied from the 16-byte boundary at or below its first point (FP32 rows of
 // an nxpp = 2 (mod 4) field start 8 bytes into a unit); the copy may run up to
 // 15 bytes past the field's end, inside the 16 bytes every field buffer is
@@ -682,11 +686,11 @@ template <typename T>
 __host__ __device__ inline int eb_rs() {  // tile row stride (elements): 32 points and room for the offset
   return kTX + 16 / (int)sizeof(T);
 }
-__host__ __device__ inline int eb_np(int N) { return (N + 1) & ~1; }  // operator row stride: pairs stay aligned
+__host__ __device__ constexpr int eb_np(int NM) { return (NM + 1) & ~1; }  // operator row stride: pairs stay aligned
 template <typename T>
-__host__ inline size_t eb_smem(int N) {
-  return 16 + (size_t)kEBArr * N * eb_rs<T>() * sizeof(T) + (size_t)N * eb_np(N) * sizeof(double) +
-         (size_t)N * eb_np(N) * sizeof(T) + (size_t)N * kTX * sizeof(T);
+__host__ inline size_t eb_smem(int N, int NM) {
+  return 16 + ((size_t)NM + (size_t)(kEBArr - 1) * N) * eb_rs<T>() * sizeof(T) +
+         (size_t)NM * eb_np(NM) * sizeof(double) + (size_t)NM * eb_np(NM) * sizeof(T) + (size_t)NM * kTX * sizeof(T);
 }
 // two consecutive operator entries (an 8-byte broadcast load for FP32)
 __device__ __forceinline__ void ld_pair(const float* p, float& a, float& b) {
@@ -699,15 +703,16 @@ __device__ __forceinline__ void ld_pair(const double* p, double& a, double& b) {
   b = p[1];
 }
 
-template <typename T>
+template <typename T, int NM>
 __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs c, int* __restrict__ err) {
+  constexpr int NP = eb_np(NM), RB = (NM + kTW - 1) / kTW;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int N = g.N, RS = eb_rs<T>(), NP = eb_np(N);
+  const int N = g.N, RS = eb_rs<T>();
   uint64_t* bar = (uint64_t*)smraw;  // [0]: Z, [1]: the other six tiles
-  T* tiles = (T*)(smraw + 16);       // [arr][k][RS]
-  double* sL = (double*)(tiles + (size_t)kEBArr * N * RS);  // [k1][NP]: L - I
-  T* sD = (T*)(sL + N * NP);                                 // [k1][NP]
-  T* tf = sD + N * NP;  // N*kTX: F* tile
+  T* tiles = (T*)(smraw + 16);       // Z: [NM][RS], then arrays 1..6: [N][RS] each
+  double* sL = (double*)(tiles + ((size_t)NM + (size_t)(kEBArr - 1) * N) * RS);  // [NM][NP]: L - I
+  T* sD = (T*)(sL + NM * NP);                                                     // [NM][NP]
+  T* tf = sD + NM * NP;                                                           // [NM][kTX]: F* tile
   const int q = blockIdx.z;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int i0 = blockIdx.x * kTX, i = i0 + lane;
@@ -731,53 +736,50 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
     const uint32_t off = (uint32_t)(ga & 15u);
     const uint32_t bytes = (off + (uint32_t)nval * (uint32_t)sizeof(T) + 15u) & ~15u;
     uint64_t* b = &bar[arr == 0 ? 0 : 1];
+    T* dst = tiles + (arr == 0 ? (size_t)k : (size_t)NM + (size_t)(arr - 1) * N + k) * RS;
     mbar_expect_tx(b, bytes);
-    bulk_g2s(tiles + (size_t)t * RS, (const void*)(ga - off), bytes, b);
+    bulk_g2s(dst, (const void*)(ga - off), bytes, b);
   }
-  for (int t = tid; t < N * N; t += blockDim.x) {
-    const int r = t / N, cc = t - r * N;
-    sD[r * NP + cc] = (T)g.D[t];
-    sL[r * NP + cc] = g.Lfil[t] - (r == cc ? 1.0 : 0.0);
+  // operators zero-padded to NM x NM, the padding rows of the Z and F* tiles zero
+  for (int t = tid; t < NM * NP; t += blockDim.x) {
+    const int r = t / NP, cc = t - r * NP;
+    const bool in = r < N && cc < N;
+    sD[t] = in ? (T)g.D[r * N + cc] : (T)0;
+    sL[t] = in ? g.Lfil[r * N + cc] - (r == cc ? 1.0 : 0.0) : 0.0;
   }
+  for (int t = N * RS + tid; t < NM * RS; t += blockDim.x) tiles[t] = (T)0;
+  for (int t = N * kTX + tid; t < NM * kTX; t += blockDim.x) tf[t] = (T)0;
   // element offset of this CTA's first point inside each copied row (the
   // same for every row: the planes are whole 16-byte units)
   const int eo = (int)((((size_t)i0 + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * (size_t)(ks * N))) * sizeof(T)) &
                        15u) /
                  (int)sizeof(T);
   const bool ok0 = mbar_wait(&bar[0], 0, 2000000000ull);
-  __syncthreads();  // the operator tables are in place
+  __syncthreads();  // the operator tables and padding are in place
   const bool act = i < g.nxpp;
   const T fac = (T)g.hfac[ks];
   const T f1 = (T)c.fac1, f2 = (T)c.fac2, f3 = (T)c.fac3;
-  // D Z for this warp's rows (k1 = w + 8 r), all rows at once: each column
-  // value feeds every row, each pair of operator entries is one broadcast
-  // load; the sums run over k2 in order, as in the one-row-per-pass kernel.
-  // Lanes past the field's end compute on stale tile entries and store nothing.
-  constexpr int kMaxRows = 8;  // N <= 8 * kTW = 64
-  T dz[kMaxRows];
+  // D Z for this warp's rows; lanes past the field's end compute on stale
+  // tile entries and store nothing
+  T dz[RB];
 #pragma unroll
-  for (int r = 0; r < kMaxRows; ++r) dz[r] = 0;
+  for (int r = 0; r < RB; ++r) dz[r] = 0;
   const T* zc = tiles + eo + lane;  // this lane's column of the Z tile
-  {
-    int k2 = 0;
-    for (; k2 + 1 < N; k2 += 2) {
-      const T z0 = zc[k2 * RS], z1 = zc[(k2 + 1) * RS];
+  const T* dw = sD + w * NP;        // row w of D; row w + 8 r is dw + 8 r NP
 #pragma unroll
-      for (int r = 0; r < kMaxRows; ++r) {
-        const int k1 = w + kTW * r;
-        if (k1 < N) {
-          T d0, d1;
-          ld_pair(sD + k1 * NP + k2, d0, d1);
+  for (int k2 = 0; k2 < NM; k2 += 2) {
+    const T z0 = zc[k2 * RS];
+    const T z1 = k2 + 1 < NM ? zc[(k2 + 1) * RS] : (T)0;
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      if (r < RB - 1 || w + kTW * r < NM) {
+        T d0, d1;
+        if (k2 + 1 < NM) {
+          ld_pair(dw + r * kTW * NP + k2, d0, d1);
           dz[r] = fma_t(d1, z1, fma_t(d0, z0, dz[r]));
+        } else {
+          dz[r] = fma_t(dw[r * kTW * NP + k2], z0, dz[r]);
         }
-      }
-    }
-    if (k2 < N) {
-      const T z0 = zc[k2 * RS];
-#pragma unroll
-      for (int r = 0; r < kMaxRows; ++r) {
-        const int k1 = w + kTW * r;
-        if (k1 < N) dz[r] = fma_t(sD[k1 * NP + k2], z0, dz[r]);
       }
     }
   }
@@ -789,31 +791,31 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
     return;
   }
 #pragma unroll
-  for (int r = 0; r < kMaxRows; ++r) {
+  for (int r = 0; r < RB; ++r) {
     const int k1 = w + kTW * r;
     if (k1 >= N) break;
     T fsv = 0;
     if (act) {
       const int kk = ks * N + k1;
       const size_t p = fidx<T>(g, i, j, kk);
-      const size_t e = (size_t)k1 * RS + eo + lane;
+      const size_t e = (size_t)NM * RS + (size_t)k1 * RS + eo + lane;  // array 1 (B), row k1
       const size_t AS = (size_t)N * RS;
-      const T sn = tiles[2 * AS + e];
-      const T snm = tiles[3 * AS + e];
+      const T sn = tiles[e + 1 * AS];
+      const T snm = tiles[e + 2 * AS];
       T F2;
       if (i < 2) {
-        const T va = tiles[4 * AS + e];
+        const T va = tiles[e + 3 * AS];
         const T vb = a.F1[q][fidx<T>(g, i, (g.ny - j) % g.ny, kk)];
         F2 = i == 0 ? (T)0.5 * (va + vb) : (T)0.5 * (va - vb);
       } else if (i >= g.nx) {
-        F2 = i == g.nx ? tiles[4 * AS + e] * (T)g.scaley : (T)0;
+        F2 = i == g.nx ? tiles[e + 3 * AS] * (T)g.scaley : (T)0;
       } else {
-        F2 = tiles[4 * AS + e];
+        F2 = tiles[e + 3 * AS];
       }
-      const T fn = tiles[5 * AS + e];
-      const T fnm = tiles[6 * AS + e];
+      const T fn = tiles[e + 4 * AS];
+      const T fnm = tiles[e + 5 * AS];
       T S;
-      stageE_point<T>(c, fac, f1, f2, f3, tiles[1 * AS + e], dz[r], sn, snm, F2, fn, fnm, S, fsv);
+      stageE_point<T>(c, fac, f1, f2, f3, tiles[e], dz[r], sn, snm, F2, fn, fnm, S, fsv);
       if (q == 2 && ((kk == 0) || (kk == g.nz - 1))) {
         const int side = kk == 0 ? 0 : 1;
         a.wnl[(size_t)i + (size_t)g.nxpp * ((size_t)j + (size_t)g.ny * side)] = stageE_wall<T>(f1, f2, f3, S, sn, snm);
@@ -825,25 +827,29 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
   }
   __syncthreads();
   if (!act) return;
-  const double cfm1 = a.filter ? g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0 : 0.0;
   if (!a.filter) {
-    for (int k1 = w; k1 < N; k1 += kTW) a.F[q][fidx<T>(g, i, j, ks * N + k1)] = tf[k1 * kTX + lane];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int k1 = w + kTW * r;
+      if (k1 < N) a.F[q][fidx<T>(g, i, j, ks * N + k1)] = tf[k1 * kTX + lane];
+    }
     return;
   }
+  const double cfm1 = g.cfour[(size_t)j * g.nxhp + (i >> 1)] - 1.0;
   // (L - I) F* in FP64 for all of this warp's rows at once, sums in k2 order
-  double s2[kMaxRows];
+  double s2[RB];
 #pragma unroll
-  for (int r = 0; r < kMaxRows; ++r) s2[r] = 0.0;
-  for (int k2 = 0; k2 < N; ++k2) {
+  for (int r = 0; r < RB; ++r) s2[r] = 0.0;
+  const double* lw = sL + w * NP;
+#pragma unroll
+  for (int k2 = 0; k2 < NM; ++k2) {
     const double f = (double)tf[k2 * kTX + lane];
 #pragma unroll
-    for (int r = 0; r < kMaxRows; ++r) {
-      const int k1 = w + kTW * r;
-      if (k1 < N) s2[r] = __fma_rn(sL[k1 * NP + k2], f, s2[r]);
-    }
+    for (int r = 0; r < RB; ++r)
+      if (r < RB - 1 || w + kTW * r < NM) s2[r] = __fma_rn(lw[r * kTW * NP + k2], f, s2[r]);
   }
 #pragma unroll
-  for (int r = 0; r < kMaxRows; ++r) {
+  for (int r = 0; r < RB; ++r) {
     const int k1 = w + kTW * r;
     if (k1 < N) a.F[q][fidx<T>(g, i, j, ks * N + k1)] = (T)stageE_filtered((double)tf[k1 * kTX + lane], s2[r], cfm1);
   }

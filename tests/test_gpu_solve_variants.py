@@ -67,7 +67,7 @@ def test_tensor_core_solve_matches_grouped_solve(name):
 
 
 @pytest.mark.parametrize("precision", [cf.IW_PREC_FP64, cf.IW_PREC_MIXED])
-@pytest.mark.parametrize("nzloc", [17, 33, 40])
+@pytest.mark.parametrize("nzloc", [17, 25, 33])
 def test_stage_e_variants_agree(precision, nzloc):
     """Stage E as a tiled kernel (0), a register-column kernel (1) or the
     tiled kernel with its input tiles staged by bulk asynchronous copies (2).
@@ -77,7 +77,7 @@ def test_stage_e_variants_agree(precision, nzloc):
     import iwrepo_b200 as iw
     cfg = cf.Config(nx=16, ny=16, nzloc=nzloc, nsubd=3, dt=1e-3, precision=precision).validate()
     runs = {}
-    for variant in (0, 1, 2) if nzloc <= 33 else (0, 2):
+    for variant in (0, 1, 2):
         s = iw.Solver(cfg)
         s.set_launch("stage_e", variant)
         s.init_mode1(0.05, 1e-3, 23)
