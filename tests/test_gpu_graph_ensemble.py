@@ -72,7 +72,8 @@ def test_autotune_keeps_results(precision, tol):
     b.step(2)
     before = b.state(0)
     ch = b.autotune()
-    assert ch["y_tile"] in (2, 4, 8) and ch["stage_a"] in ("register", "tiled") and ch["stage_e"] in ("register", "tiled")
+    assert ch["y_tile"] in (2, 4, 8) and ch["stage_a"] in ("register", "tiled")
+    assert ch["stage_e"] in ("register", "tiled", "tiled-bulk")
     assert np.array_equal(before, b.state(0))
     a.step(6)
     b.step(6)
