@@ -305,8 +305,18 @@ int iw_autotune(iw_handle *h, int *choices);
 #define IW_LAUNCH_YTILE 0   /* 0 (size heuristic), 2, 4 or 8 */
 #define IW_LAUNCH_STAGE_A 1 /* -1 (size heuristic), 0 tiled, 1 register-column */
 #define IW_LAUNCH_STAGE_E 2 /* as stage A, or 2: tiled, bulk-copied input tiles (N <= 64) */
-#define IW_LAUNCH_SOLVE 3   /* 1 system-grouped (default), 2 same on the FP64 tensor cores, 0 per task */
+#define IW_LAUNCH_SOLVE 3   /* 1 system-grouped (default), 2 same on the FP64 tensor cores, 0 per task,
+                               3 system-grouped with two rows per thread (u/v, w, rho; the pressure takes 1) */
+/* one solve role's variant (values as IW_LAUNCH_SOLVE; -1 = the IW_LAUNCH_SOLVE choice) */
+#define IW_LAUNCH_SOLVE_UV 4
+#define IW_LAUNCH_SOLVE_W 5
+#define IW_LAUNCH_SOLVE_RHO 6
+#define IW_LAUNCH_SOLVE_PRESSURE 7
 int iw_set_launch(iw_handle *h, int which, int value);
+
+/* Not in the reference.  Reads one launch choice (the IW_LAUNCH_* ids), e.g.
+ * the per-role solve variants iw_autotune kept. */
+int iw_get_launch(iw_handle *h, int which, int *value);
 
 /* Not in the reference (its main.f advances one run).  Advances n independent
  * runs of any sizes (separate handles on one device) by nsteps steps each.

@@ -23,7 +23,7 @@ PI = C.POINTER(C.c_int)
 # every entry point declared in include/iw_b200.h
 EXPORTS = [
     "iw_init", "iw_destroy", "iw_last_error", "iw_last_status", "iw_upload_state", "iw_download_state", "iw_init_mode1",
-    "iw_write_restart", "iw_read_restart", "iw_write_fields", "iw_wait_fields", "iw_set_animation", "iw_set_speclegen", "iw_postp", "iw_set_postp", "iw_step", "iw_run", "iw_ensemble_run", "iw_autotune", "iw_set_launch", "iw_step_coefs", "iw_set_coefs", "iw_diag", "iw_sync", "iw_field_ptr", "iw_stream",
+    "iw_write_restart", "iw_read_restart", "iw_write_fields", "iw_wait_fields", "iw_set_animation", "iw_set_speclegen", "iw_postp", "iw_set_postp", "iw_step", "iw_run", "iw_ensemble_run", "iw_autotune", "iw_set_launch", "iw_get_launch", "iw_step_coefs", "iw_set_coefs", "iw_diag", "iw_sync", "iw_field_ptr", "iw_stream",
     "iw_device_bytes", "iw_helm_solve_batched", "iw_bind", "iw_profile", "iw_profile_read", "iw_mean_profiles",
     "horfft_", "dpdz_", "filter_3dlegenfourier_", "filter_legenpen_", "interface_avg3d_",
     "penalty_main_", "bandlu_solve_", "iw_bandlu_solve_noalloc", "penalty_setup_", "convec_", "calcuvwt_",
@@ -67,6 +67,7 @@ def lib():
     L.iw_ensemble_run.argtypes = [C.POINTER(vp), C.c_int, C.c_int]
     L.iw_autotune.argtypes = [vp, PI]
     L.iw_set_launch.argtypes = [vp, C.c_int, C.c_int]
+    L.iw_get_launch.argtypes = [vp, C.c_int, PI]
     L.iw_step_coefs.argtypes = [vp, C.POINTER(IwCoefs)]
     L.iw_set_coefs.argtypes = [vp, C.POINTER(IwCoefs), C.c_double]
     L.iw_diag.argtypes = [vp, C.POINTER(IwDiagOut)]

@@ -1371,7 +1371,9 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   bi.nb = h->nb;
   memcpy(bi.bmap, h->bmap, sizeof bi.bmap);
   const int mm = std::max(2 * (h->ns - 1), 1);
-  const size_t sm = ((size_t)2 * R * h->nz + 2 * R * mm) * sizeof(double);
+  // the pressure keeps its u*, v*, w* columns in shared memory as well
+  const size_t sm = ((size_t)2 * R * h->nz + 2 * R * mm) * sizeof(double) +
+                    (role == 3 ? (size_t)3 * R * h->nz * sizeof(T) : 0);
   T *F0, *F1 = nullptr, *F2 = nullptr;
   if (role == 3) {
     F0 = fs.F[0];
@@ -1393,7 +1395,11 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
   const bool fold = h->bi_fold[kind] && cpen;
   // system-grouped kernel for the tasks after the prefix, when it applies
   // (variant 2: the block products on the FP64 tensor cores, N <= 40)
-  const int us = h->sys_role[role] >= 0 ? h->sys_role[role] : h->use_sys;
+  int us = h->sys_role[role] >= 0 ? h->sys_role[role] : h->use_sys;
+  // variant 3 (two rows per thread) exists for u/v, w and rho when a subdomain's
+  // row pairs fit one CTA; otherwise the one-row grouped kernel takes its place
+  const int nthr2 = (h->ns * ((h->N + 1) / 2) + 31) / 32 * 32;
+  if (us == 3 && (role == 3 || nthr2 > kSys2MaxThreads)) us = 1;
   const bool tc = us == 2 && h->N <= 8 * kTcMT;
   const SysSmem lay = sys_smem(h->nz, h->N, h->ns, h->nb, role == 3, tc ? kTcRS : kSysRS, tc ? tc_ap(h->N) : 0);
   const size_t smsys = lay.total * sizeof(double);
@@ -1421,10 +1427,25 @@ static void launch_solve_bi(iw_handle* h, FieldSet<T>& fs, int role, int cpen, i
     else                   \
       IW_SYS_LAUNCH(3, TCV); \
   } while (0)
-    if (tc)
+#define IW_SYS2_LAUNCH(RL)                                                                                   \
+  do {                                                                                                       \
+    cudaFuncSetAttribute(k_solve_sys2<T, RL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smsys);      \
+    k_solve_sys2<T, RL><<<h->ntask2[kind], nthr2, smsys, h->st>>>(g, bi, h->dtasks2[kind], h->dcolorder, F0, \
+                                                                  F1, rd, meanu, mg, h->derr);              \
+  } while (0)
+    if (us == 3) {
+      if (role == 0)
+        IW_SYS2_LAUNCH(0);
+      else if (role == 1)
+        IW_SYS2_LAUNCH(1);
+      else
+        IW_SYS2_LAUNCH(2);
+    } else if (tc) {
       IW_SYS_ROLE(true);
-    else
+    } else {
       IW_SYS_ROLE(false);
+    }
+#undef IW_SYS2_LAUNCH
 #undef IW_SYS_ROLE
 #undef IW_SYS_LAUNCH
   }
@@ -1649,8 +1670,9 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
     for (int role : {3, 0, 1, 2}) {
       float best = 0;
       int bestv = 1;
-      for (int v = 0; v < 3; ++v) {
+      for (int v = 0; v < 4; ++v) {
         if (v == 2 && h->N > 8 * kTcMT) continue;
+        if (v == 3 && (role == 3 || (h->ns * ((h->N + 1) / 2) + 31) / 32 * 32 > kSys2MaxThreads)) continue;
         h->sys_role[role] = v;
         const float t = timeit([&] { launch_solve_bi<T>(h, ts, role, cpen, kstart); });
         if (v == 0 || t < best) {
@@ -2176,13 +2198,39 @@ int iw_set_launch(iw_handle* h, int which, int value) {
       (which == IW_LAUNCH_STAGE_A ? h->tune_a : h->tune_e) = value;
       return IW_OK;
     case IW_LAUNCH_SOLVE:
-      if (value < 0 || value > 2) return set_err(IW_ERR_CONFIG, "solve variant: 0, 1 or 2");
+      if (value < 0 || value > 3) return set_err(IW_ERR_CONFIG, "solve variant: 0, 1, 2 or 3");
       if (value == 2 && h->N > 8 * kTcMT) return set_err(IW_ERR_CONFIG, "tensor-core solve needs N <= 40");
       h->use_sys = value;
       for (int& r : h->sys_role) r = -1;
       return IW_OK;
+    case IW_LAUNCH_SOLVE_UV:
+    case IW_LAUNCH_SOLVE_W:
+    case IW_LAUNCH_SOLVE_RHO:
+    case IW_LAUNCH_SOLVE_PRESSURE: {
+      if (value < -1 || value > 3) return set_err(IW_ERR_CONFIG, "solve variant: -1, 0, 1, 2 or 3");
+      if (value == 2 && h->N > 8 * kTcMT) return set_err(IW_ERR_CONFIG, "tensor-core solve needs N <= 40");
+      const int role = which == IW_LAUNCH_SOLVE_UV ? 0 : which == IW_LAUNCH_SOLVE_W ? 1
+                       : which == IW_LAUNCH_SOLVE_RHO ? 2 : 3;
+      h->sys_role[role] = value;
+      return IW_OK;
+    }
     default:
       return set_err(IW_ERR_CONFIG, "unknown launch choice");
+  }
+}
+
+int iw_get_launch(iw_handle* h, int which, int* value) {
+  if (!h || !value) return set_err(IW_ERR_STATE, "iw_get_launch: null argument");
+  switch (which) {
+    case IW_LAUNCH_YTILE: *value = h->tune_ytx; return IW_OK;
+    case IW_LAUNCH_STAGE_A: *value = h->tune_a; return IW_OK;
+    case IW_LAUNCH_STAGE_E: *value = h->tune_e; return IW_OK;
+    case IW_LAUNCH_SOLVE: *value = h->use_sys; return IW_OK;
+    case IW_LAUNCH_SOLVE_UV: *value = h->sys_role[0]; return IW_OK;
+    case IW_LAUNCH_SOLVE_W: *value = h->sys_role[1]; return IW_OK;
+    case IW_LAUNCH_SOLVE_RHO: *value = h->sys_role[2]; return IW_OK;
+    case IW_LAUNCH_SOLVE_PRESSURE: *value = h->sys_role[3]; return IW_OK;
+    default: return set_err(IW_ERR_CONFIG, "unknown launch choice");
   }
 }
 

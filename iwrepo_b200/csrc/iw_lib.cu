@@ -430,13 +430,20 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
   const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
   // rows 0..3 u v w t, 4..7 dx, 8..11 dy, 12..15 dz, 16..19 neighbour u v w t:
   // half-complex rows (M+1 values), all copies in flight at once
-  const int nxhp = M + 1;
-  for (int q = tid; q < nrow * nxhp; q += nthr) {
-    const int r = q / nxhp, kk = q - r * nxhp;
-    const T* src = r < 4 ? a.in[r] : r < 8 ? a.in[r - 4] : r < 16 ? a.in[r - 4] : a.in[r - 16];
-    const int kr = r < 16 ? k : knb;
-    cp_async_c<C>(buf + r * RS + fpad(kk), (const C*)(src + fidx<T>(g, 2 * kk, j, kr)));
+  // Element offsets of this (j, k) row and of the neighbour's, once per CTA.
+  // A thread keeps its kk and walks the rows (fixed strides, no index
+  // arithmetic per copy); kk = M, the last value of a row, goes to thread r.
+  const size_t roff = fidx<T>(g, 0, j, k), roffn = fidx<T>(g, 0, j, knb);
+  auto rsrc = [&](int r) -> const C* {
+    return (const C*)((r < 4 ? a.in[r] : r < 16 ? a.in[r - 4] : a.in[r - 16]) + (r < 16 ? roff : roffn));
+  };
+  for (int kk = tid; kk < M; kk += nthr) {
+    C* d = buf + fpad(kk);
+#pragma unroll
+    for (int r = 0; r < 20; ++r)
+      if (r < nrow) cp_async_c<C>(d + r * RS, rsrc(r) + kk);
   }
+  if (tid < nrow) cp_async_c<C>(buf + tid * RS + fpad(M), rsrc(tid) + M);
   cp_async_wait_all();
   __syncthreads();
   const int nh = M / 2 + 1;
@@ -514,22 +521,24 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
   __syncthreads();
   const T invN = (T)1 / (T)nx;
   // outputs: A_q = X(Q_q) + i kx X(P_uq) for q = u v w t ; then uv vv vw vt uw ww wt
-  const int nout = M + 1;
-  for (int t = tid; t < 11 * nout; t += nthr) {
-    const int o = t / nout, kk = t - o * nout;
-    C val;
+  // a thread keeps its kk and writes it in all 11 output rows; kk = M goes
+  // to thread o
+  auto outv = [&](int o, int kk) -> C {
     if (o < 4) {
       const C x1 = xfwd_post_p<C>(buf + o * RS, kk, M, Wn, invN);
       const C x2 = xfwd_post_p<C>(buf + (4 + o) * RS, kk, M, Wn, invN);
       const T kx = kxs * (T)kk;
-      val = cmk<C>(x1.x - kx * x2.y, x1.y + kx * x2.x);
-    } else {
-      // map: 4->uv(5) 5->vv(8) 6->vw(9) 7->vt(10) 8->uw(6) 9->ww(11) 10->wt(12)
-      const int sr = o == 4 ? 5 : o == 5 ? 8 : o == 6 ? 9 : o == 7 ? 10 : o == 8 ? 6 : o == 9 ? 11 : 12;
-      val = xfwd_post_p<C>(buf + sr * RS, kk, M, Wn, invN);
+      return cmk<C>(x1.x - kx * x2.y, x1.y + kx * x2.x);
     }
-    *(C*)(a.out[o] + fidx<T>(g, 2 * kk, j, k)) = val;
+    // map: 4->uv(5) 5->vv(8) 6->vw(9) 7->vt(10) 8->uw(6) 9->ww(11) 10->wt(12)
+    const int sr = o == 4 ? 5 : o == 5 ? 8 : o == 6 ? 9 : o == 7 ? 10 : o == 8 ? 6 : o == 9 ? 11 : 12;
+    return xfwd_post_p<C>(buf + sr * RS, kk, M, Wn, invN);
+  };
+  for (int kk = tid; kk < M; kk += nthr) {
+#pragma unroll 1
+    for (int o = 0; o < 11; ++o) *((C*)(a.out[o] + roff) + kk) = outv(o, kk);
   }
+  if (tid < 11) *((C*)(a.out[tid] + roff) + M) = outv(tid, M);
 }
 
 // ===========================================================================
@@ -1915,6 +1924,19 @@ __global__ void k_press_g(Geo g, SolveTabs tb, const Task* __restrict__ tasks, i
 // ===========================================================================
 constexpr int kSolveThreads = 128;
 
+// (re, im) pair of one complex value stored as two T
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+  typedef float2 t;
+};
+template <>
+struct Pair<double> {
+  typedef double2 t;
+};
+
+
 // dst = (accum ? dst : 0) + A^-1 src for R right-hand sides of length n.
 // rz, zz: R*m doubles of shared scratch.  Ends synchronised.
 template <int R>
@@ -2071,6 +2093,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
   double* x = b + (size_t)R * n;
   double* rz = x + (size_t)R * n;
   double* zz = rz + (size_t)R * (m > 0 ? m : 1);
+  // role 3: u*, v*, w* of the task's columns, [field][r][k], read from global
+  // memory once for both the divergence and the projection
+  T* fv = (T*)(zz + (size_t)R * (m > 0 ? m : 1));
   const int per = role == 0 ? 4 : 2;
   const int ncols = R / per;  // column slots per task
   const int s = tk.sys;
@@ -2082,6 +2107,29 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
     cii[tid] = c < 0 ? -1 : c % g.nxhp;
   }
   __syncthreads();
+  if (role == 3) {
+    // one 8-byte (re, im) load per field and column, all in flight at once
+    typedef typename Pair<T>::t P2;
+    for (int k = tid; k < n; k += kSolveThreads) {
+#pragma unroll
+      for (int ci = 0; ci < R / 2; ++ci) {
+        P2 u2 = {0, 0}, v2 = {0, 0}, w2 = {0, 0};
+        if (cj[ci] >= 0) {
+          const size_t p = fidx<T>(g, 2 * cii[ci], cj[ci], k);
+          u2 = *(const P2*)(F0 + p);
+          v2 = *(const P2*)(F1 + p);
+          w2 = *(const P2*)(F2 + p);
+        }
+        fv[(size_t)(2 * ci) * n + k] = u2.x;
+        fv[(size_t)(2 * ci + 1) * n + k] = u2.y;
+        fv[(size_t)(R + 2 * ci) * n + k] = v2.x;
+        fv[(size_t)(R + 2 * ci + 1) * n + k] = v2.y;
+        fv[(size_t)(2 * R + 2 * ci) * n + k] = w2.x;
+        fv[(size_t)(2 * R + 2 * ci + 1) * n + k] = w2.y;
+      }
+    }
+    __syncthreads();
+  }
   if (s < 0 && role != 3) {  // w of the (0,0) mode is zero
     for (int ci = 0; ci < ncolt; ++ci)
       for (int k = tid; k < n; k += kSolveThreads) {
@@ -2099,14 +2147,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
     const double eps = sd.eps;
     if (role == 3) {
       for (int k = tid; k < n; k += kSolveThreads) {  // w* columns into x (scratch)
-        double v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int ci = r >> 1;
-          v[r] = cj[ci] >= 0 ? (double)F2[fidx<T>(g, 2 * cii[ci] + (r & 1), cj[ci], k)] : 0.0;
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r) x[(size_t)r * n + k] = v[r];
+        for (int r = 0; r < R; ++r) x[(size_t)r * n + k] = (double)fv[(size_t)(2 * R + r) * n + k];
       }
       __syncthreads();
       for (int k = tid; k < n; k += kSolveThreads) {
@@ -2125,9 +2167,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
           double vr = 0.0, vi = 0.0;
           if (cj[ci] >= 0) {
             const int j = cj[ci], ii = cii[ci];
-            const size_t pr = fidx<T>(g, 2 * ii, j, k);
-            const double ur = (double)F0[pr], ui = (double)F0[pr + 1];
-            const double wr = (double)F1[pr], wi = (double)F1[pr + 1];
+            const double ur = (double)fv[(size_t)(2 * ci) * n + k], ui = (double)fv[(size_t)(2 * ci + 1) * n + k];
+            const double wr = (double)fv[(size_t)(R + 2 * ci) * n + k];
+            const double wi = (double)fv[(size_t)(R + 2 * ci + 1) * n + k];
             const double xw = g.xw[ii], yw = g.yw[j];
             const double dr = -(xw * ui) - (yw * wi) + dw[2 * ci] * fac;
             const double di = (xw * ur) + (yw * wr) + dw[2 * ci + 1] * fac;
@@ -2205,11 +2247,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_cta(
         const double phr = res[(size_t)(2 * ci) * n + k], phi = res[(size_t)(2 * ci + 1) * n + k];
         double wbr = 0, wbi = 0;
         if (!(ii == 0 && j == 0)) {
-          wbr = (double)F2[pr] - dt * (dz[2 * ci] * fac);
-          wbi = (double)F2[pi] - dt * (dz[2 * ci + 1] * fac);
+          wbr = (double)fv[(size_t)(2 * R + 2 * ci) * n + k] - dt * (dz[2 * ci] * fac);
+          wbi = (double)fv[(size_t)(2 * R + 2 * ci + 1) * n + k] - dt * (dz[2 * ci + 1] * fac);
         }
         const double dtx = dt * g.xw[ii], dty = dt * g.yw[j];
-        const double ur = (double)F0[pr], ui = (double)F0[pi], vr = (double)F1[pr], vi = (double)F1[pi];
+        const double ur = (double)fv[(size_t)(2 * ci) * n + k], ui = (double)fv[(size_t)(2 * ci + 1) * n + k];
+        const double vr = (double)fv[(size_t)(R + 2 * ci) * n + k], vi = (double)fv[(size_t)(R + 2 * ci + 1) * n + k];
         F0[pr] = (T)(ur + dtx * phi);
         F0[pi] = (T)(ui - dtx * phr);
         F1[pr] = (T)(vr + dty * phi);
@@ -2385,17 +2428,6 @@ __device__ __forceinline__ void tc_block_product2(const double* op, int ap, cons
     }
   }
 }
-
-template <typename T>
-struct Pair;
-template <>
-struct Pair<float> {
-  typedef float2 t;
-};
-template <>
-struct Pair<double> {
-  typedef double2 t;
-};
 
 // role 0: u/v (4 RHS per column), 1: w, 2: rho, 3: pressure + projection.
 // TC: block products on the FP64 tensor cores (N <= 40), else one row per
@@ -2820,6 +2852,190 @@ __global__ void __maxnreg__(72) k_solve_sys(
     *(P2*)(F0 + pr) = zu;
     *(P2*)(F1 + pr) = zv;
     *(P2*)(F2 + pr) = zw;
+  }
+}
+
+// ===========================================================================
+// System-grouped solve with two rows per thread (u/v, w and rho).  The
+// grouped solve above spends most of its time in the shared-memory pipe: each
+// multiply-add of its block product takes one broadcast load of a
+// right-hand-side value.  Here thread (ks, q) owns rows q and q + H of
+// subdomain ks (H = ceil(N/2)), both of one inverse block, so every broadcast
+// feeds two multiply-adds and the loads per multiply-add fall from 18/16 to
+// 20/32.  The tables, the gather, the interface system and the order of every
+// sum are those of k_solve_sys, so both give the same bits.
+// ===========================================================================
+constexpr int kSys2MaxThreads = 256;
+
+// acc0/acc1[r] = sum_c col[c N (+ H)] * b[c RS + r] for two rows of one block
+__device__ __forceinline__ void row_product16x2(const double* col, int H, bool has1, const double* bb, int N,
+                                                double* acc0, double* acc1) {
+#pragma unroll
+  for (int r = 0; r < kSysR; ++r) acc0[r] = acc1[r] = 0.0;
+#pragma unroll 1
+  for (int c = 0; c < N; ++c) {
+    const double a0 = col[(size_t)c * N];
+    const double a1 = has1 ? col[(size_t)c * N + H] : 0.0;
+    const double* br = bb + (size_t)c * kSysRS;
+#pragma unroll
+    for (int h = 0; h < kSysR; h += 8) {
+      double v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = lds64(br + h + r);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        acc0[h + r] += a0 * v[r];
+        acc1[h + r] += a1 * v[r];
+      }
+    }
+  }
+}
+
+template <typename T, int ROLE>
+__global__ void __launch_bounds__(kSys2MaxThreads, 2) k_solve_sys2(
+    Geo g, BlockInv bi, const Task* __restrict__ tasks, const int* __restrict__ col_order, T* __restrict__ F0,
+    T* __restrict__ F1, double rdiv, int meanu, const double* __restrict__ meang, int* __restrict__ err) {
+  static_assert(ROLE >= 0 && ROLE <= 2, "u/v, w and rho only");
+  typedef typename Pair<T>::t P2;
+  constexpr int R = kSysR;
+  constexpr int PER = ROLE == 0 ? 4 : 2;  // right-hand sides per column
+  constexpr int NC = R / PER;             // column slots
+  extern __shared__ __align__(16) double sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int cj[NC], cii[NC];
+  const Task tk = tasks[blockIdx.x];
+  const int n = g.nz, N = g.N, ns = g.ns, m = 2 * (ns - 1), nb = bi.nb;
+  const int H = (N + 1) >> 1;
+  const int tid = threadIdx.x;
+  const int s = tk.sys;
+  const SysSmem L = sys_smem(n, N, ns, nb, false);
+  double* sA = sm + L.a;
+  double* sL = sm + L.l;
+  double* sM = sm + L.m;
+  double* sb = sm + L.b;
+  double* srz = sm + L.rz;
+  double* szz = sm + L.zz;
+  const uintptr_t ga = (uintptr_t)((const double*)bi.ainv + (size_t)s * nb * N * N);
+  const int offA = (int)((ga & 15u) >> 3);
+  const uint32_t bytesA = (uint32_t)((((size_t)nb * N * N + offA) * 8 + 15) & ~(size_t)15);
+  const uint32_t bytesL = (uint32_t)((size_t)m * N * 8), bytesM = (uint32_t)((size_t)m * m * 8);
+  if (tid == 0) mbar_init(&bar, 1);
+  if (tid < NC) {
+    const int c = tid < tk.count ? col_order[tk.first + tid] : -1;
+    cj[tid] = c < 0 ? -1 : c / g.nxhp;
+    cii[tid] = c < 0 ? -1 : c % g.nxhp;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&bar, bytesA + bytesL + bytesM);
+    bulk_g2s(sA, (const void*)(ga - (uintptr_t)offA * 8), bytesA, &bar);
+    if (m > 0) {
+      bulk_g2s(sL, bi.lvec + (size_t)s * m * N, bytesL, &bar);
+      bulk_g2s(sM, bi.minv + (size_t)s * m * m, bytesM, &bar);
+    }
+  }
+  const double eps = bi.sys[s].eps;
+  const int ks = tid / H, q0 = tid - ks * H;
+  const bool live = ks < ns;
+  const bool has1 = live && q0 + H < N;
+  const int k0 = ks * N + q0, k1 = k0 + H;
+  // gather rows k0 and k1 of every column: [row][16]
+#pragma unroll 1
+  for (int hr = 0; hr < 2; ++hr) {
+    if (!(hr == 0 ? live : has1)) continue;
+    const int k = hr == 0 ? k0 : k1;
+    double v[R];
+#pragma unroll
+    for (int ci = 0; ci < NC; ++ci) {
+      P2 a = {0, 0}, b = {0, 0};
+      if (cj[ci] >= 0) {
+        const size_t p = fidx<T>(g, 2 * cii[ci], cj[ci], k);
+        a = *(const P2*)(F0 + p);
+        if (ROLE == 0) b = *(const P2*)(F1 + p);
+      }
+      v[PER * ci] = (double)a.x;
+      v[PER * ci + 1] = (double)a.y;
+      if (ROLE == 0) {
+        v[PER * ci + 2] = (double)b.x;
+        v[PER * ci + 3] = (double)b.y;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = -(-(v[r] / rdiv) * eps);
+    double2* d2 = (double2*)(sb + (size_t)k * kSysRS);
+#pragma unroll
+    for (int q = 0; q < R / 2; ++q) d2[q] = make_double2(v[2 * q], v[2 * q + 1]);
+  }
+  const bool ok = mbar_wait(&bar, 0, 2000000000ull);
+  if (__syncthreads_or(!ok)) {  // the tables never arrived: report, let the copies finish, leave
+    if (tid == 0) err[1] = 1;
+    mbar_wait(&bar, 0, 2000000000ull);
+    return;
+  }
+  // interface system (the loops and sums of k_solve_sys)
+  if (m > 0) {
+    for (int q = tid; q < m * R; q += blockDim.x) {
+      const int e = q / R, r = q - e * R;
+      const int blk = e < ns - 1 ? e : e - (ns - 1) + 1;
+      const double* lv = sL + (size_t)e * N;
+      const double* sv = sb + (size_t)blk * N * kSysRS + r;
+      double a = 0.0;
+      for (int c = 0; c < N; ++c) a += lv[c] * sv[(size_t)c * kSysRS];
+      srz[q] = a;
+    }
+    __syncthreads();
+    for (int q = tid; q < m * R; q += blockDim.x) {
+      const int e = q / R, r = q - e * R;
+      const double* mr = sM + (size_t)e * m;
+      double z = 0.0;
+      for (int c = 0; c < m; ++c) z += mr[c] * srz[(size_t)c * R + r];
+      szz[q] = z;
+    }
+    __syncthreads();
+  }
+  if (!live) return;
+  // x = A_ks^-1 b_ks - A_ks^-1 e_0 z_{ks-1} - A_ks^-1 e_{N-1} z_{ns-1+ks}, two rows
+  const double* col = sA + offA + (size_t)bi.bmap[ks] * N * N + q0;
+  double acc0[R], acc1[R];
+  row_product16x2(col, H, has1, sb + (size_t)ks * N * kSysRS, N, acc0, acc1);
+#pragma unroll 1
+  for (int hr = 0; hr < 2; ++hr) {
+    if (hr == 1 && !has1) break;
+    const int k = hr == 0 ? k0 : k1;
+    const double* cr = col + (hr == 0 ? 0 : H);
+    const double p = ks >= 1 ? cr[0] : 0.0;
+    const double qv = ks <= ns - 2 ? cr[(size_t)(N - 1) * N] : 0.0;
+    double x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      double xv = hr == 0 ? acc0[r] : acc1[r];
+      if (ks >= 1) xv -= p * szz[(size_t)(ks - 1) * R + r];
+      if (ks <= ns - 2) xv -= qv * szz[(size_t)(ns - 1 + ks) * R + r];
+      x[r] = xv;
+    }
+    if (ROLE == 0 && meanu) {
+#pragma unroll
+      for (int ci = 0; ci < NC; ++ci)
+        if (cii[ci] == 0 && cj[ci] == 0) {
+          x[PER * ci] = meang[k] * x[PER * ci];
+          x[PER * ci + 1] = meang[k] * x[PER * ci + 1];
+        }
+    }
+#pragma unroll
+    for (int ci = 0; ci < NC; ++ci) {
+      if (cj[ci] < 0) continue;
+      const size_t p2 = fidx<T>(g, 2 * cii[ci], cj[ci], k);
+      P2 o;
+      o.x = (T)x[PER * ci];
+      o.y = (T)x[PER * ci + 1];
+      *(P2*)(F0 + p2) = o;
+      if (ROLE == 0) {
+        P2 o2;
+        o2.x = (T)x[PER * ci + 2];
+        o2.y = (T)x[PER * ci + 3];
+        *(P2*)(F1 + p2) = o2;
+      }
+    }
   }
 }
 

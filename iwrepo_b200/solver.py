@@ -156,15 +156,25 @@ class Solver:
         ch = (C.c_int * 4)()
         _lib.check(_lib.lib().iw_autotune(self.h, ch))
         names = {2: "tiled-bulk", 1: "register", 0: "tiled", -1: "n/a"}
-        solve = {0: "per-task", 1: "system-grouped", 2: "system-grouped-tensor-core"}
-        return {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]],
-                "solve": solve[ch[3]]}
+        solve = {0: "per-task", 1: "system-grouped", 2: "system-grouped-tensor-core",
+                 3: "system-grouped-two-rows"}
+        out = {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]], "solve": solve[ch[3]]}
+        out["solve_roles"] = {role: solve.get(self.get_launch("solve_" + role), "n/a")
+                              for role in ("uv", "w", "rho", "pressure")}
+        return out
 
-    LAUNCH = {"y_tile": 0, "stage_a": 1, "stage_e": 2, "solve": 3}
+    LAUNCH = {"y_tile": 0, "stage_a": 1, "stage_e": 2, "solve": 3, "solve_uv": 4, "solve_w": 5, "solve_rho": 6,
+              "solve_pressure": 7}
 
     def set_launch(self, which: str, value: int):
         """Set one launch choice directly (iw_set_launch)."""
         _lib.check(_lib.lib().iw_set_launch(self.h, self.LAUNCH[which], int(value)))
+
+    def get_launch(self, which: str) -> int:
+        """Read one launch choice (iw_get_launch)."""
+        v = C.c_int(0)
+        _lib.check(_lib.lib().iw_get_launch(self.h, self.LAUNCH[which], C.byref(v)))
+        return v.value
 
     def run(self, n: int, graph: bool = True):
         """n steps; with graph=True the invariant steady-state step is replayed

@@ -66,6 +66,47 @@ def test_tensor_core_solve_matches_grouped_solve(name):
             assert np.linalg.norm(a[q] - b[q]) <= tol * (n if n > 0 else 1.0), (name, q)
 
 
+@pytest.mark.parametrize("name", list(CASES))
+def test_two_row_solve_equals_grouped_solve(name):
+    """The grouped solve with two rows per thread (variant 3: u/v, w and rho;
+    the pressure keeps variant 1) runs every sum of the one-row grouped kernel
+    in the same order: identical states after 5 steps.  At 512 rows (16
+    subdomains of 32) the row pairs do not fit one CTA and the one-row kernel
+    runs, which the test covers too."""
+    import iwrepo_b200 as iw
+    cfg = cf.Config(dt=1e-3, **CASES[name]).validate()
+    runs = []
+    for variant in (1, 3):
+        s = iw.Solver(cfg)
+        s.set_launch("solve", variant)
+        s.init_mode1(0.05, 1e-3, 17)
+        s.step(5)
+        runs.append([s.state(lev) for lev in range(5)])
+        s.close()
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b), name
+
+
+def test_per_role_solve_choices():
+    """iw_set_launch / iw_get_launch per solve role; a role given variant 3
+    matches the run with every role on the one-row grouped kernel."""
+    import iwrepo_b200 as iw
+    cfg = cf.Config(dt=1e-3, **CASES["c3-vertical-mixed"]).validate()
+    a, b = iw.Solver(cfg), iw.Solver(cfg)
+    a.set_launch("solve", 1)
+    b.set_launch("solve", 1)
+    for role in ("uv", "w", "rho"):
+        b.set_launch("solve_" + role, 3)
+        assert b.get_launch("solve_" + role) == 3
+    assert b.get_launch("solve_pressure") == -1
+    for s in (a, b):
+        s.init_mode1(0.05, 1e-3, 5)
+        s.step(4)
+    assert np.array_equal(a.state(0), b.state(0))
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("precision", [cf.IW_PREC_FP64, cf.IW_PREC_MIXED])
 @pytest.mark.parametrize("nzloc", [17, 25, 33])
 def test_stage_e_variants_agree(precision, nzloc):
@@ -116,6 +157,10 @@ def test_autotune_reports_the_solve_variant():
     s = iw.Solver(cfg)
     s.init_mode1(0.05, 1e-4, 3)
     ch = s.autotune()
-    assert ch["solve"] in ("system-grouped", "system-grouped-tensor-core", "per-task")
+    kinds = ("system-grouped", "system-grouped-tensor-core", "per-task", "system-grouped-two-rows")
+    assert ch["solve"] in kinds
+    assert set(ch["solve_roles"]) == {"uv", "w", "rho", "pressure"}
+    assert all(v in kinds for v in ch["solve_roles"].values())
+    assert ch["solve_roles"]["pressure"] != "system-grouped-two-rows"
     s.step(2)
     s.close()
