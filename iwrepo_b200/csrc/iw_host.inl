@@ -348,6 +348,8 @@ struct iw_handle {
   double *dD = 0, *dD2 = 0, *dL = 0, *dh = 0, *dxw = 0, *dyw = 0, *dcf = 0, *dzg = 0, *dzh = 0;
   double *dwg = 0, *dal = 0, *dsig = 0, *dmeang = 0;
   double *dwnl = 0, *dwvr = 0, *dred = 0;
+  unsigned char* deops = 0;  // stage E's padded operators for k_stageE_b (EArgs::ops), built at init
+  unsigned eops_bytes = 0;
   int* dcnt = 0;
   int* dflag = 0;
   int* derr = 0;  // device error words: [0] non-finite state, [1] a bounded device wait gave up
@@ -975,6 +977,31 @@ static bool stageE_b_fits(const iw_handle* h) {
   return nm > 0 && eb_smem<T>(h->N, nm) <= 200 * 1024 && (h->plane * sizeof(T)) % 16 == 0;
 }
 
+// Stage E's operators zero-padded to the register bucket NM, in the layout of
+// k_stageE_b's shared memory: [NM][NP] doubles of L - I, then [NM][NP] values
+// of D in the storage type, rounded up to 16 bytes (one bulk copy per CTA).
+template <typename T>
+static std::vector<unsigned char> stageE_ops(const iw_handle* h, int NM) {
+  const int N = h->N, NP = eb_np(NM);
+  const size_t nl = (size_t)NM * NP * sizeof(double), nd = (size_t)NM * NP * sizeof(T);
+  std::vector<unsigned char> out((nl + nd + 15) & ~(size_t)15, 0);
+  double* L = (double*)out.data();
+  T* D = (T*)(out.data() + nl);
+  for (int r = 0; r < N; ++r)
+    for (int c = 0; c < N; ++c) {
+      L[(size_t)r * NP + c] = h->tab.Lfil[(size_t)r * N + c] - (r == c ? 1.0 : 0.0);
+      D[(size_t)r * NP + c] = (T)h->tab.D[(size_t)r * N + c];
+    }
+  return out;
+}
+static int build_stageE_ops(iw_handle* h) {
+  const int nm = zop_bucket(h->N);
+  if (nm <= 0) return 0;  // no bulk-staged stage E at this N
+  const std::vector<unsigned char> t = h->mixed ? stageE_ops<float>(h, nm) : stageE_ops<double>(h, nm);
+  h->eops_bytes = (unsigned)t.size();
+  return up(h, &h->deops, t);
+}
+
 template <typename T>
 static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   EArgs<T> a;
@@ -990,6 +1017,10 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   }
   a.wnl = h->dwnl;
   a.filter = h->p.ispecfilternl == 1;
+  // the prebuilt operator table holds the handle's storage type
+  const bool own = h->deops && (h->mixed ? sizeof(T) == 4 : sizeof(T) == 8);
+  a.ops = own ? h->deops : nullptr;
+  a.ops_bytes = own ? h->eops_bytes : 0u;
   const dim3 rgrid((unsigned)((h->plane + 127) / 128), (unsigned)h->ns, 4);
   // The register-column stage E holds two columns per thread; past these sizes
   // its register count costs more occupancy than the tiled kernel loses.
@@ -1511,14 +1542,14 @@ template <typename T>
 static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
   typedef typename cplx_t<T>::type C;
   Geo g = geo(h);
+  const dim3 pgrid((unsigned)((h->ny + 127) / 128), (unsigned)h->nz, (unsigned)(h->ns < 2 ? 4 : nf));
   if (h->ns < 2) {
-    long total = (long)h->ny * h->nz * 4;
-    k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
+    k_project_planes<T><<<pgrid, 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
     return 0;
   }
   const int ng = nf * (h->ns - 1);  // plane groups (field, interface)
-  const long tot = (long)h->plane * ng * 4;  // 4 planes per group
-  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 0);
+  const dim3 ggrid((unsigned)((h->plane + 255) / 256), (unsigned)(ng * 4));  // 4 planes per group
+  k_iface_gather<T><<<ggrid, 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 0);
   {
     YJobs<T> jb;
     memset(&jb, 0, sizeof jb);
@@ -1539,9 +1570,8 @@ static int iface_avg(iw_handle* h, FieldSet<T>& fs, bool count, int nf = 4) {
     jb.j[0] = YJob<T>{fs.G, nullptr, fs.G, 2};
     launch_y<T>(h, fs, jb, 1, ng * 4, false);
   }
-  long total = (long)h->ny * h->nz * nf;
-  k_project_planes<T><<<(unsigned)((total + 127) / 128), 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
-  k_iface_gather<T><<<(unsigned)((tot + 255) / 256), 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1);
+  k_project_planes<T><<<pgrid, 128, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], 0);
+  k_iface_gather<T><<<ggrid, 256, 0, h->st>>>(g, fs.F[0], fs.F[1], fs.F[2], fs.F[3], fs.G, 1);
   return 0;
 }
 
@@ -1985,6 +2015,7 @@ int iw_init(const iw_dims* dims, const iw_params* prm, int device, iw_handle** o
        up(h, &h->dxw, xw) || up(h, &h->dyw, yw) || up(h, &h->dcf, cf) || up(h, &h->dzg, zg) || up(h, &h->dzh, zh) ||
        up(h, &h->dwg, h->tab.wg) || up(h, &h->dal, h->tab.alpol) || up(h, &h->dsig, h->tab.sigma) ||
        up(h, &h->dmeang, mg);
+  if (!r) r = build_stageE_ops(h);
   r |= dalloc(h, &h->dwnl, h->plane * 2) || dalloc(h, &h->dwvr, h->plane * 2) || dalloc(h, &h->dred, std::max<size_t>(64, 4 * (size_t)h->nz)) ||
        dalloc(h, &h->dcnt, 8) || dalloc(h, &h->dflag, 4) || dalloc(h, &h->derr, 2) ||
        cudaHostAlloc((void**)&h->herr, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
@@ -2043,6 +2074,7 @@ int iw_destroy(iw_handle* h) {
   for (double* p : {h->ddzinv, h->dpart, h->dDt, h->dD2t, h->dLt, h->dD, h->dD2, h->dL, h->dh, h->dxw, h->dyw, h->dcf, h->dzg, h->dzh, h->dwg, h->dal, h->dsig,
                     h->dmeang, h->dwnl, h->dwvr, h->dred})
     cudaFree(p);
+  cudaFree(h->deops);
   cudaFree(h->dcnt);
   cudaFree(h->dflag);
   cudaFree(h->derr);

@@ -243,7 +243,25 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   const int iit = ii0 + tb;
   const bool colok = iit < g.nxhp;
   const size_t gstep = (size_t)JS * g.nxpp;
-  {
+  // mode 1 with a compile-time length: the i ky factor is applied as the
+  // values arrive (plain loads, all in flight), not in a second pass over the
+  // shared tile
+  constexpr bool kyload = MC > 0 && MC % JS == 0;
+  const bool mulky = kyload && jb.mode == 1;
+  if (mulky) {
+    const size_t g0 = fidx<T>(g, 2 * iit, tj, k);
+    C* d = A + tb * RSY + fpad(tj);
+    const C* s1 = (const C*)(jb.src + g0);
+    C v[kyload ? MC / JS : 1];
+#pragma unroll
+    for (int it = 0; it < (kyload ? MC / JS : 1); ++it)
+      v[it] = colok ? s1[(size_t)it * (gstep / 2)] : cmk<C>(0, 0);
+#pragma unroll
+    for (int it = 0; it < (kyload ? MC / JS : 1); ++it) {
+      const T ky = (T)g.yw[tj + it * JS];
+      d[it * (JS + JS / 16)] = cmk<C>(-(ky * v[it].y), ky * v[it].x);
+    }
+  } else {
     const size_t g0 = fidx<T>(g, 2 * iit, tj, k);
     C* d = A + tb * RSY + fpad(tj);
     const C* s1 = (const C*)(jb.src + g0);
@@ -263,7 +281,7 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   }
   cp_async_wait_all();
   __syncthreads();
-  if (jb.mode == 1) {
+  if (jb.mode == 1 && !mulky) {
     for (int t = threadIdx.x; t < TX * ny; t += blockDim.x) {
       const int b = t % TX, j = t / TX;
       const T ky = (T)g.yw[j];
@@ -447,9 +465,18 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_xrow_nl(Geo g, NLA
   cp_async_wait_all();
   __syncthreads();
   const int nh = M / 2 + 1;
-  for (int q = tid; q < nrow * nh; q += nthr) {
-    const int r = q / nh, kk = q - r * nh;
-    xprep_pair<C, T>(buf + r * RS, kk, M, Wn, r >= 4 && r < 8, kxs);
+  const int H2 = M / 2;
+  if (MC > 0 && nthr % H2 == 0) {
+    // a thread keeps its pair kk < M/2 and steps over rows by nthr/(M/2);
+    // the middle pair kk = M/2 goes to thread r
+    const int kk = tid % H2, rs = nthr / H2;
+    for (int r = tid / H2; r < nrow; r += rs) xprep_pair<C, T>(buf + r * RS, kk, M, Wn, r >= 4 && r < 8, kxs);
+    if (tid < nrow) xprep_pair<C, T>(buf + tid * RS, H2, M, Wn, tid >= 4 && tid < 8, kxs);
+  } else {
+    for (int q = tid; q < nrow * nh; q += nthr) {
+      const int r = q / nh, kk = q - r * nh;
+      xprep_pair<C, T>(buf + r * RS, kk, M, Wn, r >= 4 && r < 8, kxs);
+    }
   }
   __syncthreads();
   for (int r = wid; r < nrow; r += nw) {
@@ -601,6 +628,11 @@ struct EArgs {
   T* F[4];      // out: filtered u*
   double* wnl;  // (nxpp,ny,2)
   int filter;
+  // k_stageE_b: its zero-padded operators as one table built once on the
+  // host ([NM][NP] doubles of L - I, then [NM][NP] T of D, the size rounded
+  // up to 16 bytes); null: every CTA builds them from D and the filter
+  const void* ops;
+  unsigned ops_bytes;
 };
 
 template <typename T>
@@ -727,11 +759,16 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
   const int i0 = blockIdx.x * kTX, i = i0 + lane;
   const int j = blockIdx.y % g.ny, ks = blockIdx.y / g.ny;
   const int nval = min(kTX, g.nxpp - i0);
+  const bool pre = a.ops != nullptr;
   if (tid == 0) {
-    mbar_init(&bar[0], (uint32_t)N);
+    mbar_init(&bar[0], (uint32_t)N + (pre ? 1u : 0u));
     mbar_init(&bar[1], (uint32_t)((kEBArr - 1) * N));
   }
   __syncthreads();
+  if (pre && tid == (int)blockDim.x - 1) {  // the operators, with the Z tile (the copy may run 15 bytes into tf)
+    mbar_expect_tx(&bar[0], a.ops_bytes);
+    bulk_g2s(sL, a.ops, a.ops_bytes, &bar[0]);
+  }
   for (int t = tid; t < kEBArr * N; t += blockDim.x) {
     const int arr = t / N, k = t - arr * N;
     const T* base = arr == 0 ? a.Z[q]
@@ -749,12 +786,15 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
     mbar_expect_tx(b, bytes);
     bulk_g2s(dst, (const void*)(ga - off), bytes, b);
   }
-  // operators zero-padded to NM x NM, the padding rows of the Z and F* tiles zero
-  for (int t = tid; t < NM * NP; t += blockDim.x) {
-    const int r = t / NP, cc = t - r * NP;
-    const bool in = r < N && cc < N;
-    sD[t] = in ? (T)g.D[r * N + cc] : (T)0;
-    sL[t] = in ? g.Lfil[r * N + cc] - (r == cc ? 1.0 : 0.0) : 0.0;
+  // operators zero-padded to NM x NM (unless copied above), the padding rows of
+  // the Z and F* tiles zero
+  if (!pre) {
+    for (int t = tid; t < NM * NP; t += blockDim.x) {
+      const int r = t / NP, cc = t - r * NP;
+      const bool in = r < N && cc < N;
+      sD[t] = in ? (T)g.D[r * N + cc] : (T)0;
+      sL[t] = in ? g.Lfil[r * N + cc] - (r == cc ? 1.0 : 0.0) : 0.0;
+    }
   }
   for (int t = N * RS + tid; t < NM * RS; t += blockDim.x) tiles[t] = (T)0;
   for (int t = N * kTX + tid; t < NM * kTX; t += blockDim.x) tf[t] = (T)0;
@@ -908,19 +948,36 @@ __global__ void __launch_bounds__(128) k_stageA_r(Geo g, const __grid_constant__
   T* O = q == 0 ? O0 : q == 1 ? O1 : q == 2 ? O2 : O3;
   T* Z = q == 0 ? Z0 : q == 1 ? Z1 : q == 2 ? Z2 : Z3;
   const bool wzero = q == 2 && j == 0 && i < 2;  // wc(1,1,:) = 0, solver.f:66-69
+  // the projection changes only the kx = 0 and Nyquist columns: every other
+  // point is a plain copy, read and written with fixed plane strides
+  const bool special = proj && (i < 2 || i >= g.nx);
+  const size_t pl = g.plane, o0 = (size_t)(ks * N) * pl + t;
   T col[NM];
   bool bad = false;
+  if (!special) {
 #pragma unroll
-  for (int k = 0; k < NM; ++k) {
-    T x = 0;
-    if (k < N) {
-      const int kk = ks * N + k;
-      x = proj ? proj_val<T>(g, F, i, j, kk) : F[(size_t)kk * g.plane + t];
-      bad |= !isfinite(x);
-      if (wzero) x = (T)0;
-      O[(size_t)kk * g.plane + t] = x;
+    for (int k = 0; k < NM; ++k) {
+      T x = 0;
+      if (k < N) {
+        x = F[o0 + (size_t)k * pl];
+        bad |= !isfinite(x);
+        if (wzero) x = (T)0;
+        O[o0 + (size_t)k * pl] = x;
+      }
+      col[k] = x;
     }
-    col[k] = x;
+  } else {
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+      T x = 0;
+      if (k < N) {
+        x = proj_val<T>(g, F, i, j, ks * N + k);
+        bad |= !isfinite(x);
+        if (wzero) x = (T)0;
+        O[o0 + (size_t)k * pl] = x;
+      }
+      col[k] = x;
+    }
   }
   if (bad) err[0] = 1;  // the state of the last step holds a NaN or Inf
   const T fac = (T)g.hfac[ks];
@@ -930,7 +987,7 @@ __global__ void __launch_bounds__(128) k_stageA_r(Geo g, const __grid_constant__
       T s = 0;
 #pragma unroll
       for (int k2 = 0; k2 < NM; ++k2) s = fma_t(op.D[k1 * NM + k2], col[k2], s);
-      Z[(size_t)(ks * N + k1) * g.plane + t] = mul_t(s, fac);
+      Z[o0 + (size_t)k1 * pl] = mul_t(s, fac);
     }
   }
 }
@@ -3101,13 +3158,10 @@ __global__ void k_left_vecs(Geo g, int nsys, const double* __restrict__ ainv, co
 // Nyquist column.
 template <typename T>
 __global__ void k_project_planes(Geo g, T* F0, T* F1, T* F2, T* F3, int skip_iface) {
-  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long total = (long)g.ny * g.nz * 4;
-  if (gid >= total) return;
-  int j = gid % g.ny;
-  long r = gid / g.ny;
-  int k = r % g.nz;
-  int q = r / g.nz;
+  // grid: x over y rows, y over z levels, z over the 4 fields (32-bit indices)
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= g.ny) return;
+  const int k = blockIdx.y, q = blockIdx.z;
   if (skip_iface) {
     int kl = k % g.N;
     if ((kl == 0 && k > 0) || (kl == g.N - 1 && k < g.nz - 1)) return;
@@ -3134,23 +3188,23 @@ __global__ void k_project_planes(Geo g, T* F0, T* F1, T* F2, T* F3, int skip_ifa
 // gather the 4 planes around each interface into a compact buffer:
 // G[(q*(ns-1)+f)*4 + m] plane = F_q level (f+1)*N - 2 + m; back: add the
 // averaging change held in G to the two interface planes.
+// Grid: x over the points of a plane, y over the 16 (ns - 1) planes (no
+// 64-bit division per element).
 template <typename T>
 __global__ void k_iface_gather(Geo g, const T* F0, const T* F1, const T* F2, const T* F3, T* G, int back) {
-  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long per = (long)g.plane;
-  long total = per * 4 * (g.ns - 1) * 4;
-  if (gid >= total) return;
-  long e = gid % per;
-  long pl = gid / per;
+  const size_t per = g.plane;
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= per) return;
+  const int pl = blockIdx.y;
   int m = pl % 4;
   int f = (pl / 4) % (g.ns - 1);
   int q = pl / (4 * (g.ns - 1));
   int k = (f + 1) * g.N - 2 + m;
   const T* F = q == 0 ? F0 : q == 1 ? F1 : q == 2 ? F2 : F3;
   if (!back) {
-    G[pl * per + e] = F[(size_t)k * per + e];
+    G[(size_t)pl * per + e] = F[(size_t)k * per + e];
   } else if (m == 1 || m == 2) {
-    ((T*)F)[(size_t)k * per + e] += G[pl * per + e];  // spectral change made by the averaging
+    ((T*)F)[(size_t)k * per + e] += G[(size_t)pl * per + e];  // spectral change made by the averaging
   }
 }
 
