@@ -248,7 +248,50 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   // shared tile
   constexpr bool kyload = MC > 0 && MC % JS == 0;
   const bool mulky = kyload && jb.mode == 1;
-  if (mulky) {
+  // With a compile-time plan whose first pass has nb0 = MC / R0 butterflies, a
+  // multiple of JS, a thread's loaded values (rows tj + JS it) hold every input
+  // of its first-pass butterflies (rows j + nb0 r, j = tj + JS m).  The first
+  // Stockham pass (Ns = 1, no twiddles) then runs in registers as the values
+  // arrive, and the warps start at the second pass: one shared-memory write and
+  // one read less per value.  The x-Nyquist column keeps its raw values.
+  constexpr int R0 = MC > 0 ? 1 << CtPlan<(MC > 0 ? MC : 2)>::bits(0) : 1;
+  constexpr int NB0 = MC > 0 ? MC / R0 : 1;
+  constexpr bool fuse1 = MC > 0 && R0 <= 8 && NB0 % JS == 0 && CtPlan<(MC > 0 ? MC : 2)>::np > 1;
+  if constexpr (fuse1) {
+    constexpr int NIT = MC / JS, NBT = NB0 / JS;
+    const bool tr = iit < g.nxh;
+    const size_t g0 = fidx<T>(g, 2 * iit, tj, k);
+#pragma unroll 1
+    for (int hh = 0; hh < (two ? 2 : 1); ++hh) {
+      const C* s1 = (const C*)((hh ? jb.src2 : jb.src) + g0);
+      C* row = (hh ? A2 : A) + tb * RSY;
+      C v[NIT];
+#pragma unroll
+      for (int it = 0; it < NIT; ++it) v[it] = colok ? s1[(size_t)it * (gstep / 2)] : cmk<C>(0, 0);
+      if (jb.mode == 1) {
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) {
+          const T ky = (T)g.yw[tj + it * JS];
+          v[it] = cmk<C>(-(ky * v[it].y), ky * v[it].x);
+        }
+      }
+      if (tr) {
+#pragma unroll
+        for (int mb = 0; mb < NBT; ++mb) {
+          C w[R0];
+#pragma unroll
+          for (int r = 0; r < R0; ++r) w[r] = v[mb + r * NBT];  // row tj + JS mb + NB0 r
+          dft_reg<C, R0>(w, !fwd);
+          const int b0 = (tj + JS * mb) * R0;
+#pragma unroll
+          for (int r = 0; r < R0; ++r) row[fpad(b0 + r)] = w[r];
+        }
+      } else {
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) row[fpad(tj) + it * (JS + JS / 16)] = v[it];
+      }
+    }
+  } else if (mulky) {
     const size_t g0 = fidx<T>(g, 2 * iit, tj, k);
     C* d = A + tb * RSY + fpad(tj);
     const C* s1 = (const C*)(jb.src + g0);
@@ -297,7 +340,9 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int r = threadIdx.x >> 5; r < nrow; r += nw) {
     C* row = r < nb ? A + r * RSY : A2 + (r - nb) * RSY;
-    if constexpr (MC > 0)
+    if constexpr (fuse1)
+      fft_passes_ct<C, (MC > 0 ? MC : 2), 1, R0>(row, Wy, !fwd, lane);  // the first pass ran at load
+    else if constexpr (MC > 0)
       fft_warp_ct<C, MC>(row, Wy, !fwd, lane);
     else
       fft_warp<C, DPT, POW2>(row, pl, Wy, !fwd, lane);
