@@ -304,7 +304,8 @@ int iw_autotune(iw_handle *h, int *choices);
 /* Not in the reference.  Sets one launch choice of iw_autotune directly. */
 #define IW_LAUNCH_YTILE 0   /* 0 (size heuristic), 2, 4 or 8 */
 #define IW_LAUNCH_STAGE_A 1 /* -1 (size heuristic), 0 tiled, 1 register-column */
-#define IW_LAUNCH_STAGE_E 2 /* as stage A, or 2: tiled, bulk-copied input tiles (N <= 64) */
+#define IW_LAUNCH_STAGE_E 2 /* as stage A, or 2: tiled, bulk-copied input tiles (N <= 33); 3: the same with
+                               its z operators in the constant bank */
 #define IW_LAUNCH_SOLVE 3   /* 1 system-grouped (default), 2 same on the FP64 tensor cores, 0 per task,
                                3 system-grouped with two rows per thread (u/v, w, rho; the pressure takes 1) */
 /* one solve role's variant (values as IW_LAUNCH_SOLVE; -1 = the IW_LAUNCH_SOLVE choice) */

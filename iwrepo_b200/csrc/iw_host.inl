@@ -972,9 +972,9 @@ static void launch_stageA(iw_handle* h, FieldSet<T>& fs, int proj) {
 }
 
 template <typename T>
-static bool stageE_b_fits(const iw_handle* h) {
+static bool stageE_b_fits(const iw_handle* h, bool cb = false) {
   const int nm = zop_bucket(h->N);
-  return nm > 0 && eb_smem<T>(h->N, nm) <= 200 * 1024 && (h->plane * sizeof(T)) % 16 == 0;
+  return nm > 0 && eb_smem<T>(h->N, nm, cb) <= 200 * 1024 && (h->plane * sizeof(T)) % 16 == 0;
 }
 
 // Stage E's operators zero-padded to the register bucket NM, in the layout of
@@ -1026,15 +1026,22 @@ static void launch_stageE(iw_handle* h, FieldSet<T>& fs) {
   // its register count costs more occupancy than the tiled kernel loses.
   // tune_e = 2: the tiled kernel with its input tiles staged by bulk copies
   // and its z operators unrolled at the register-column bucket size (N <= 33)
-  if (h->tune_e == 2 && stageE_b_fits<T>(h)) {
+  // tune_e = 3: the same kernel with its operators in the constant bank
+  const bool cb = h->tune_e == 3;
+  if ((h->tune_e == 2 || cb) && stageE_b_fits<T>(h, cb)) {
     dim3 grid((unsigned)((h->nxpp + kTX - 1) / kTX), (unsigned)(h->ny * h->ns), 4);
     const int nm = zop_bucket(h->N);
-    const size_t smem = eb_smem<T>(h->N, nm);
+    const size_t smem = eb_smem<T>(h->N, nm, cb);
     switch (nm) {
-#define IW_EBCASE(NM)                                                                                           \
-  case NM:                                                                                                      \
-    cudaFuncSetAttribute(k_stageE_b<T, NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
-    k_stageE_b<T, NM><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c, h->derr);                             \
+#define IW_EBCASE(NM)                                                                                              \
+  case NM:                                                                                                         \
+    if (cb) {                                                                                                      \
+      cudaFuncSetAttribute(k_stageE_b<T, NM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+      k_stageE_b<T, NM, true><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c, h->derr, make_zop<T, NM>(h));    \
+    } else {                                                                                                       \
+      cudaFuncSetAttribute(k_stageE_b<T, NM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+      k_stageE_b<T, NM, false><<<grid, kTX * kTW, smem, h->st>>>(geo(h), a, h->c, h->derr, make_zop<T, NM>(h));   \
+    }                                                                                                              \
     return;
       IW_EBCASE(9)
       IW_EBCASE(17)
@@ -1678,8 +1685,9 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
     // 0 tiled (any N), 1 register-column (N in a register bucket), 2 tiled
     // with bulk-copied input tiles (N in a register bucket)
     float bt = 0;
-    for (int v = 0; v < 3; ++v) {
-      if ((v == 1 && !zop_bucket(h->N)) || (v == 2 && !stageE_b_fits<T>(h))) continue;
+    for (int v = 0; v < 4; ++v) {
+      if ((v == 1 && !zop_bucket(h->N)) || (v == 2 && !stageE_b_fits<T>(h)) || (v == 3 && !stageE_b_fits<T>(h, true)))
+        continue;
       h->tune_e = v;
       const float t = timeit([&] { launch_stageE<T>(h, ts); });
       if (beste < 0 || t < bt) {
@@ -2222,10 +2230,10 @@ int iw_set_launch(iw_handle* h, int which, int value) {
       return IW_OK;
     case IW_LAUNCH_STAGE_A:
     case IW_LAUNCH_STAGE_E:
-      if (value < -1 || value > (which == IW_LAUNCH_STAGE_E ? 2 : 1))
-        return set_err(IW_ERR_CONFIG, "stage variant: -1, 0, 1 (or 2 for stage E)");
+      if (value < -1 || value > (which == IW_LAUNCH_STAGE_E ? 3 : 1))
+        return set_err(IW_ERR_CONFIG, "stage variant: -1, 0, 1 (or 2, 3 for stage E)");
       if (value == 1 && !zop_bucket(h->N)) return set_err(IW_ERR_CONFIG, "register-column stages need N <= 33");
-      if (value == 2 && !(h->mixed ? stageE_b_fits<float>(h) : stageE_b_fits<double>(h)))
+      if (value >= 2 && !(h->mixed ? stageE_b_fits<float>(h, value == 3) : stageE_b_fits<double>(h, value == 3)))
         return set_err(IW_ERR_CONFIG, "bulk-staged stage E needs N <= 33 and whole 16-byte planes");
       (which == IW_LAUNCH_STAGE_A ? h->tune_a : h->tune_e) = value;
       return IW_OK;

@@ -767,6 +767,13 @@ __device__ __forceinline__ void stageE_tile(const Geo& g, const EArgs<T>& a, con
 // 15 bytes past the field's end, inside the 16 bytes every field buffer is
 // allocated with beyond its end.  The launch requires nxpp*ny*sizeof(T) to be
 // a multiple of 16, so that every row of a CTA has the same offset.
+// z operators of the register-column kernels and of k_stageE_b<.., true>: kernel
+// parameters, i.e. served from the constant bank
+template <typename T, int NM>
+struct ZOp {
+  T D[NM * NM];       // D[k1*NM + k2], zero outside N x N
+  double L[NM * NM];  // precombined Legendre filter minus the identity, same layout (FP64, see k_stageE)
+};
 constexpr int kEBArr = 7;
 template <typename T>
 __host__ __device__ inline int eb_rs() {  // tile row stride (elements): 32 points and room for the offset
@@ -774,9 +781,10 @@ __host__ __device__ inline int eb_rs() {  // tile row stride (elements): 32 poin
 }
 __host__ __device__ constexpr int eb_np(int NM) { return (NM + 1) & ~1; }  // operator row stride: pairs stay aligned
 template <typename T>
-__host__ inline size_t eb_smem(int N, int NM) {
+__host__ inline size_t eb_smem(int N, int NM, bool cb = false) {
   return 16 + ((size_t)NM + (size_t)(kEBArr - 1) * N) * eb_rs<T>() * sizeof(T) +
-         (size_t)NM * eb_np(NM) * sizeof(double) + (size_t)NM * eb_np(NM) * sizeof(T) + (size_t)NM * kTX * sizeof(T);
+         (cb ? 0 : (size_t)NM * eb_np(NM) * sizeof(double) + (size_t)NM * eb_np(NM) * sizeof(T)) +
+         (size_t)NM * kTX * sizeof(T);
 }
 // two consecutive operator entries (an 8-byte broadcast load for FP32)
 __device__ __forceinline__ void ld_pair(const float* p, float& a, float& b) {
@@ -789,22 +797,26 @@ __device__ __forceinline__ void ld_pair(const double* p, double& a, double& b) {
   b = p[1];
 }
 
-template <typename T, int NM>
-__global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs c, int* __restrict__ err) {
+// CB: D and L - I from the kernel parameter op (the constant bank; a warp's
+// rows are warp-uniform, so every operator entry is a uniform load) instead of
+// shared memory; the same sums in the same order.
+template <typename T, int NM, bool CB = false>
+__global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs c, int* __restrict__ err,
+                                                       const __grid_constant__ ZOp<T, NM> op) {
   constexpr int NP = eb_np(NM), RB = (NM + kTW - 1) / kTW;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int N = g.N, RS = eb_rs<T>();
   uint64_t* bar = (uint64_t*)smraw;  // [0]: Z, [1]: the other six tiles
   T* tiles = (T*)(smraw + 16);       // Z: [NM][RS], then arrays 1..6: [N][RS] each
-  double* sL = (double*)(tiles + ((size_t)NM + (size_t)(kEBArr - 1) * N) * RS);  // [NM][NP]: L - I
-  T* sD = (T*)(sL + NM * NP);                                                     // [NM][NP]
-  T* tf = sD + NM * NP;                                                           // [NM][kTX]: F* tile
+  double* sL = (double*)(tiles + ((size_t)NM + (size_t)(kEBArr - 1) * N) * RS);  // [NM][NP]: L - I (not CB)
+  T* sD = (T*)(sL + (CB ? 0 : NM * NP));                                          // [NM][NP] (not CB)
+  T* tf = sD + (CB ? 0 : NM * NP);                                                // [NM][kTX]: F* tile
   const int q = blockIdx.z;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int i0 = blockIdx.x * kTX, i = i0 + lane;
   const int j = blockIdx.y % g.ny, ks = blockIdx.y / g.ny;
   const int nval = min(kTX, g.nxpp - i0);
-  const bool pre = a.ops != nullptr;
+  const bool pre = !CB && a.ops != nullptr;
   if (tid == 0) {
     mbar_init(&bar[0], (uint32_t)N + (pre ? 1u : 0u));
     mbar_init(&bar[1], (uint32_t)((kEBArr - 1) * N));
@@ -833,7 +845,7 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
   }
   // operators zero-padded to NM x NM (unless copied above), the padding rows of
   // the Z and F* tiles zero
-  if (!pre) {
+  if (!pre && !CB) {
     for (int t = tid; t < NM * NP; t += blockDim.x) {
       const int r = t / NP, cc = t - r * NP;
       const bool in = r < N && cc < N;
@@ -868,7 +880,16 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
     for (int r = 0; r < RB; ++r) {
       if (r < RB - 1 || w + kTW * r < NM) {
         T d0, d1;
-        if (k2 + 1 < NM) {
+        if constexpr (CB) {
+          const T* od = op.D + (w + kTW * r) * NM + k2;
+          if (k2 + 1 < NM) {
+            d0 = od[0];
+            d1 = od[1];
+            dz[r] = fma_t(d1, z1, fma_t(d0, z0, dz[r]));
+          } else {
+            dz[r] = fma_t(od[0], z0, dz[r]);
+          }
+        } else if (k2 + 1 < NM) {
           ld_pair(dw + r * kTW * NP + k2, d0, d1);
           dz[r] = fma_t(d1, z1, fma_t(d0, z0, dz[r]));
         } else {
@@ -940,7 +961,8 @@ __global__ void __launch_bounds__(kTX* kTW) k_stageE_b(Geo g, EArgs<T> a, Coefs 
     const double f = (double)tf[k2 * kTX + lane];
 #pragma unroll
     for (int r = 0; r < RB; ++r)
-      if (r < RB - 1 || w + kTW * r < NM) s2[r] = __fma_rn(lw[r * kTW * NP + k2], f, s2[r]);
+      if (r < RB - 1 || w + kTW * r < NM)
+        s2[r] = __fma_rn(CB ? op.L[(w + kTW * r) * NM + k2] : lw[r * kTW * NP + k2], f, s2[r]);
   }
 #pragma unroll
   for (int r = 0; r < RB; ++r) {
@@ -971,11 +993,6 @@ __global__ void __launch_bounds__(kTX* kTW, 8) k_stageE_f32(Geo g, EArgs<float> 
 // sit in the constant bank, and the fully unrolled products take them as
 // immediate operands: about one instruction per multiply-add.
 // ---------------------------------------------------------------------------
-template <typename T, int NM>
-struct ZOp {
-  T D[NM * NM];       // D[k1*NM + k2], zero outside N x N
-  double L[NM * NM];  // precombined Legendre filter minus the identity, same layout (FP64, see k_stageE)
-};
 
 template <typename T, int NM>
 __global__ void __launch_bounds__(128) k_stageA_r(Geo g, const __grid_constant__ ZOp<T, NM> op,

@@ -155,7 +155,7 @@ class Solver:
         changed."""
         ch = (C.c_int * 4)()
         _lib.check(_lib.lib().iw_autotune(self.h, ch))
-        names = {2: "tiled-bulk", 1: "register", 0: "tiled", -1: "n/a"}
+        names = {3: "tiled-bulk-constant-operators", 2: "tiled-bulk", 1: "register", 0: "tiled", -1: "n/a"}
         solve = {0: "per-task", 1: "system-grouped", 2: "system-grouped-tensor-core",
                  3: "system-grouped-two-rows"}
         out = {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]], "solve": solve[ch[3]]}

@@ -110,15 +110,16 @@ def test_per_role_solve_choices():
 @pytest.mark.parametrize("precision", [cf.IW_PREC_FP64, cf.IW_PREC_MIXED])
 @pytest.mark.parametrize("nzloc", [17, 25, 33])
 def test_stage_e_variants_agree(precision, nzloc):
-    """Stage E as a tiled kernel (0), a register-column kernel (1) or the
-    tiled kernel with its input tiles staged by bulk asynchronous copies (2).
+    """Stage E as a tiled kernel (0), a register-column kernel (1), the
+    tiled kernel with its input tiles staged by bulk asynchronous copies (2),
+    or that kernel with its operators in the constant bank (3).
     They run the same sums in the same order and differ in how the compiler
     contracts the products (1e-11 of the field in FP64, 1e-5 in mixed
     precision after 4 steps)."""
     import iwrepo_b200 as iw
     cfg = cf.Config(nx=16, ny=16, nzloc=nzloc, nsubd=3, dt=1e-3, precision=precision).validate()
     runs = {}
-    for variant in (0, 1, 2):
+    for variant in (0, 1, 2, 3):
         s = iw.Solver(cfg)
         s.set_launch("stage_e", variant)
         s.init_mode1(0.05, 1e-3, 23)
@@ -126,6 +127,8 @@ def test_stage_e_variants_agree(precision, nzloc):
         runs[variant] = [s.state(lev) for lev in range(5)]
         s.close()
     tol = 1e-11 if precision == cf.IW_PREC_FP64 else 1e-5
+    for a, b in zip(runs[2], runs[3]):  # the same sums from the same operator values
+        assert np.array_equal(a, b)
     for v in runs:
         for a, b in zip(runs[0], runs[v]):
             for q in range(4):
