@@ -81,6 +81,37 @@ def test_gll_tables_katp():
     assert abs(wg @ zp ** 30 - 2.0 / 31) < 1e-13
 
 
+@pytest.mark.parametrize("N", [9, 17, 25, 33])
+def test_gll_tables_independent_derivation(N):
+    """The GLL nodes, weights and differentiation matrix (setup.f:395-479,
+    636-798) against a derivation that shares no code with the restatement:
+    numpy's Legendre series, interior nodes = roots of P'_{N-1} (refined by
+    Newton), w_j = 2 / (N (N-1) P_{N-1}(x_j)^2),
+    D_kj = P_{N-1}(x_k) / (P_{N-1}(x_j) (x_k - x_j)), D_00 = -D_{N-1,N-1} =
+    -N (N-1) / 4; D2 = D D, the exact second derivative on the GLL space."""
+    from numpy.polynomial import legendre as leg
+    t = Oracle(cf.Config(nx=16, ny=8, nzloc=N, nsubd=2, dt=1e-3).validate()).tables()
+    c = np.zeros(N)
+    c[-1] = 1.0
+    r = np.sort(leg.legroots(leg.legder(c)))
+    for _ in range(3):
+        r -= leg.legval(r, leg.legder(c)) / leg.legval(r, leg.legder(c, 2))
+    x = np.concatenate(([-1.0], r, [1.0]))
+    p = leg.legval(x, c)
+    w = 2.0 / (N * (N - 1) * p ** 2)
+    d = np.zeros((N, N))
+    for k in range(N):
+        for j in range(N):
+            if k != j:
+                d[k, j] = p[k] / (p[j] * (x[k] - x[j]))
+    d[0, 0], d[-1, -1] = -N * (N - 1) / 4.0, N * (N - 1) / 4.0
+    assert np.abs(t["zpts"] - x).max() < 1e-15
+    assert np.abs(t["wg"] - w).max() < 1e-15
+    assert np.abs(t["d"] - d).max() < 5e-14 * np.abs(d).max()
+    d2 = d @ d
+    assert np.abs(t["d2"] - d2).max() < 1e-11 * np.abs(d2).max()
+
+
 def test_wave_parameters_run_log():
     """output:53-67 of the 128x250 run: omega = 4.850712500726660E-002."""
     pi2 = 8 * math.atan(1.0)
