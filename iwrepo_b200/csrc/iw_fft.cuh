@@ -363,6 +363,16 @@ __device__ __forceinline__ void fft_passes_ct(C* row, const C* __restrict__ W, b
   }
 }
 
+// Passes P .. PEND-1 only (the first or last pass run elsewhere).
+template <typename C, int M, int P, int PEND, int NS>
+__device__ __forceinline__ void fft_passes_ct_to(C* row, const C* __restrict__ W, bool inv, int lane) {
+  if constexpr (P < PEND) {
+    constexpr int R = 1 << CtPlan<M>::bits(P);
+    fft_pass_ct<C, M, R, NS>(row, W, inv, lane);
+    fft_passes_ct_to<C, M, P + 1, PEND, NS * R>(row, W, inv, lane);
+  }
+}
+
 // In-place transform of one padded row of power-of-two length M by one warp.
 template <typename C, int M>
 __device__ __forceinline__ void fft_warp_ct(C* row, const C* __restrict__ W, bool inv, int lane) {

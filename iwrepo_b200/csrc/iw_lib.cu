@@ -257,6 +257,13 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   constexpr int R0 = MC > 0 ? 1 << CtPlan<(MC > 0 ? MC : 2)>::bits(0) : 1;
   constexpr int NB0 = MC > 0 ? MC / R0 : 1;
   constexpr bool fuse1 = MC > 0 && R0 <= 8 && NB0 % JS == 0 && CtPlan<(MC > 0 ? MC : 2)>::np > 1;
+  // Likewise the last pass (Ns = MC / RL, as many butterflies): butterfly j
+  // writes rows j + Ns r, all of them rows of the thread with tj = j mod JS
+  // when Ns is a multiple of JS, so it runs as the values are stored.
+  constexpr int NPS = CtPlan<(MC > 0 ? MC : 2)>::np;
+  constexpr int RL = MC > 0 ? 1 << CtPlan<(MC > 0 ? MC : 2)>::bits(NPS - 1) : 1;
+  constexpr int NSL = MC > 0 ? MC / RL : 1;
+  constexpr bool fuseL = fuse1 && NPS >= 2 && RL <= 8 && NSL % JS == 0;
   if constexpr (fuse1) {
     constexpr int NIT = MC / JS, NBT = NB0 / JS;
     const bool tr = iit < g.nxh;
@@ -340,7 +347,9 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int r = threadIdx.x >> 5; r < nrow; r += nw) {
     C* row = r < nb ? A + r * RSY : A2 + (r - nb) * RSY;
-    if constexpr (fuse1)
+    if constexpr (fuseL)  // the first pass ran at load, the last runs at the store
+      fft_passes_ct_to<C, (MC > 0 ? MC : 2), 1, NPS - 1, R0>(row, Wy, !fwd, lane);
+    else if constexpr (fuse1)
       fft_passes_ct<C, (MC > 0 ? MC : 2), 1, R0>(row, Wy, !fwd, lane);  // the first pass ran at load
     else if constexpr (MC > 0)
       fft_warp_ct<C, MC>(row, Wy, !fwd, lane);
@@ -349,6 +358,47 @@ __global__ void __launch_bounds__(256, (FftOcc<T, DPT>::v)) k_yfft(Geo g, YJobs<
   }
   __syncthreads();
   const T sc = fwd ? (T)g.scaley : (T)1;
+  if constexpr (fuseL) {
+    if (!colok) return;
+    const bool tr = iit < g.nxh;  // the x-Nyquist column holds raw values
+    const C* ra = A + tb * RSY;
+    const C* rb = A2 + tb * RSY;
+    C* o0 = (C*)(jb.dst + fidx<T>(g, 2 * iit, 0, k));
+    const size_t ys = (size_t)g.nxpp / 2;  // one y row, in complex values
+#pragma unroll 1
+    for (int mb = 0; mb < NSL / JS; ++mb) {
+      const int j = tj + JS * mb;  // butterfly of the last pass (Ns = NSL, step 1)
+      C va[RL], vb[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        va[r] = ra[fpad(j + r * NSL)];
+        if (two) vb[r] = rb[fpad(j + r * NSL)];
+      }
+      if (tr) {
+#pragma unroll
+        for (int r = 1; r < RL; ++r) {
+          C tw = Wy[r * j];
+          if (!fwd) tw.y = -tw.y;
+          va[r] = cmul(va[r], tw);
+          if (two) vb[r] = cmul(vb[r], tw);
+        }
+        dft_reg<C, RL>(va, !fwd);
+        if (two) dft_reg<C, RL>(vb, !fwd);
+      }
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int y = j + r * NSL;
+        C o = cmk<C>(va[r].x * sc, va[r].y * sc);
+        if (two) {
+          const C w2 = cmk<C>(vb[r].x * sc, vb[r].y * sc);
+          const T ky = (T)g.yw[y];
+          o = cmk<C>(o.x - ky * w2.y, o.y + ky * w2.x);
+        }
+        o0[(size_t)y * ys] = o;
+      }
+    }
+    return;
+  }
   if (colok) {
     const C* d = A + tb * RSY + fpad(tj);
     C* o1 = (C*)(jb.dst + fidx<T>(g, 2 * iit, tj, k));
