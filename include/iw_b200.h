@@ -313,6 +313,7 @@ int iw_autotune(iw_handle *h, int *choices);
 #define IW_LAUNCH_SOLVE_W 5
 #define IW_LAUNCH_SOLVE_RHO 6
 #define IW_LAUNCH_SOLVE_PRESSURE 7
+#define IW_LAUNCH_XROW_THREADS 8 /* threads per x-row CTA: 256 (0 = default) or 128 */
 int iw_set_launch(iw_handle *h, int which, int value);
 
 /* Not in the reference.  Reads one launch choice (the IW_LAUNCH_* ids), e.g.

@@ -403,6 +403,7 @@ struct iw_handle {
   int bmap[IW_MAX_SUBD] = {};
   // launch choices set by iw_autotune (0 / -1: built-in heuristic)
   int tune_ytx = 0;  // y-tile width
+  int tune_xthr = 0;  // threads per x-row CTA: 0 or 256, or 128
   int tune_a = -1;   // stage A: 1 register-column, 0 tiled
   int tune_e = -1;   // stage E: 1 register-column, 0 tiled, 2 tiled with bulk-copied tiles
   int brep[IW_MAX_SUBD] = {};
@@ -1176,33 +1177,14 @@ static int legspec_dump(iw_handle* h, FieldSet<T>& fs);
 template <typename T>
 static int postp_step(iw_handle* h, FieldSet<T>& fs);
 
+// K_C: x rows (k_xrow_nl), one CTA per (y, z) row with 256 threads, or 128
+// when the autotuner measured that faster (tune_xthr)
 template <typename T>
-static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
+static void launch_xrow(iw_handle* h, FieldSet<T>& fs) {
   typedef typename cplx_t<T>::type C;
   Geo g = geo(h);
   const int M = h->nx / 2;
-  mark(h, -1);
-  // K_A
-  launch_stageA<T>(h, fs, proj);
-  mark(h, 0);
-  if (h->anim_pending) {  // the dump sees the fields convec sees: projected, mean w removed
-    h->anim_pending = false;
-    int r = anim_dump<T>(h, fs);
-    if (r) return r;
-  }
-  // K_B: y-inverse of 12 arrays
-  {
-    YJobs<T> jb;
-    memset(&jb, 0, sizeof jb);
-    for (int q = 0; q < 4; ++q) {
-      jb.j[q] = YJob<T>{fs.F1[q], nullptr, fs.Y12[q], 0};
-      jb.j[4 + q] = YJob<T>{fs.F1[q], nullptr, fs.Y12[4 + q], 1};
-      jb.j[8 + q] = YJob<T>{fs.Z4[q], nullptr, fs.Y12[8 + q], 0};
-    }
-    launch_y<T>(h, fs, jb, 12, h->nz, false);
-  }
-  mark(h, 1);
-  // K_C
+  const int xthr = h->tune_xthr == 128 ? 128 : 256;
   {
     NLArgs<T> a;
     memset(&a, 0, sizeof a);
@@ -1241,7 +1223,7 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
 #define IW_XCT(MC, D)                                                                                       \
   case MC:                                                                                                  \
     cudaFuncSetAttribute(k_xrow_nl<T, D, true, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-    k_xrow_nl<T, D, true, MC><<<grid, 256, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);                     \
+    k_xrow_nl<T, D, true, MC><<<grid, xthr, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);                     \
     goto xrow_done;
       IW_XCT(32, 4)
       IW_XCT(64, 4)
@@ -1255,7 +1237,7 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
 #define IW_XCASE(D, P)                                                                                   \
   case (P ? D : -D):                                                                                     \
     cudaFuncSetAttribute(k_xrow_nl<T, D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
-    k_xrow_nl<T, D, P><<<grid, 256, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);                        \
+    k_xrow_nl<T, D, P><<<grid, xthr, smem, h->st>>>(g, a, h->plx, fs.Wm, fs.Wn);                        \
     break;
       IW_XCASE(4, true)
       IW_XCASE(8, true)
@@ -1269,6 +1251,36 @@ static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
     }
   xrow_done:;
   }
+}
+
+template <typename T>
+static int convec_impl(iw_handle* h, FieldSet<T>& fs, int proj) {
+  typedef typename cplx_t<T>::type C;
+  Geo g = geo(h);
+  const int M = h->nx / 2;
+  mark(h, -1);
+  // K_A
+  launch_stageA<T>(h, fs, proj);
+  mark(h, 0);
+  if (h->anim_pending) {  // the dump sees the fields convec sees: projected, mean w removed
+    h->anim_pending = false;
+    int r = anim_dump<T>(h, fs);
+    if (r) return r;
+  }
+  // K_B: y-inverse of 12 arrays
+  {
+    YJobs<T> jb;
+    memset(&jb, 0, sizeof jb);
+    for (int q = 0; q < 4; ++q) {
+      jb.j[q] = YJob<T>{fs.F1[q], nullptr, fs.Y12[q], 0};
+      jb.j[4 + q] = YJob<T>{fs.F1[q], nullptr, fs.Y12[4 + q], 1};
+      jb.j[8 + q] = YJob<T>{fs.Z4[q], nullptr, fs.Y12[8 + q], 0};
+    }
+    launch_y<T>(h, fs, jb, 12, h->nz, false);
+  }
+  mark(h, 1);
+  // K_C
+  launch_xrow<T>(h, fs);
   mark(h, 2);
   // K_D: y-forward; B_q = Y(A_q) + i ky Y(P_q), Z_q = Y(P_zq)
   {
@@ -1671,6 +1683,20 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
     }
   }
   h->tune_ytx = besttx;
+  // threads per x-row CTA (scratch rows in, scratch rows out)
+  {
+    float bx = 0.f;
+    int bestx = 256;
+    for (int xt : {256, 128}) {
+      h->tune_xthr = xt;
+      const float t = timeit([&] { launch_xrow<T>(h, ts); });
+      if (xt == 256 || t < bx) {
+        bx = t;
+        bestx = xt;
+      }
+    }
+    h->tune_xthr = bestx;
+  }
   // stage A and stage E variants
   int besta = -1, beste = -1;
   if (zop_bucket(h->N)) {
@@ -1726,6 +1752,7 @@ static int tune_impl(iw_handle* h, FieldSet<T>& fs, int* choice) {
   const cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     h->tune_ytx = save[0];
+    h->tune_xthr = 0;
     h->tune_a = save[1];
     h->tune_e = save[2];
     h->use_sys = save[3];
@@ -2243,6 +2270,10 @@ int iw_set_launch(iw_handle* h, int which, int value) {
       h->use_sys = value;
       for (int& r : h->sys_role) r = -1;
       return IW_OK;
+    case IW_LAUNCH_XROW_THREADS:
+      if (value != 0 && value != 128 && value != 256) return set_err(IW_ERR_CONFIG, "x-row threads: 0, 128 or 256");
+      h->tune_xthr = value;
+      return IW_OK;
     case IW_LAUNCH_SOLVE_UV:
     case IW_LAUNCH_SOLVE_W:
     case IW_LAUNCH_SOLVE_RHO:
@@ -2270,6 +2301,7 @@ int iw_get_launch(iw_handle* h, int which, int* value) {
     case IW_LAUNCH_SOLVE_W: *value = h->sys_role[1]; return IW_OK;
     case IW_LAUNCH_SOLVE_RHO: *value = h->sys_role[2]; return IW_OK;
     case IW_LAUNCH_SOLVE_PRESSURE: *value = h->sys_role[3]; return IW_OK;
+    case IW_LAUNCH_XROW_THREADS: *value = h->tune_xthr == 128 ? 128 : 256; return IW_OK;
     default: return set_err(IW_ERR_CONFIG, "unknown launch choice");
   }
 }

@@ -161,10 +161,11 @@ class Solver:
         out = {"y_tile": ch[0], "stage_a": names[ch[1]], "stage_e": names[ch[2]], "solve": solve[ch[3]]}
         out["solve_roles"] = {role: solve.get(self.get_launch("solve_" + role), "n/a")
                               for role in ("uv", "w", "rho", "pressure")}
+        out["x_row_threads"] = self.get_launch("x_row_threads")
         return out
 
     LAUNCH = {"y_tile": 0, "stage_a": 1, "stage_e": 2, "solve": 3, "solve_uv": 4, "solve_w": 5, "solve_rho": 6,
-              "solve_pressure": 7}
+              "solve_pressure": 7, "x_row_threads": 8}
 
     def set_launch(self, which: str, value: int):
         """Set one launch choice directly (iw_set_launch)."""

@@ -74,6 +74,7 @@ def test_autotune_keeps_results(precision, tol):
     ch = b.autotune()
     assert ch["y_tile"] in (2, 4, 8) and ch["stage_a"] in ("register", "tiled")
     assert ch["stage_e"] in ("register", "tiled", "tiled-bulk", "tiled-bulk-constant-operators")
+    assert ch["x_row_threads"] in (128, 256)
     assert np.array_equal(before, b.state(0))
     a.step(6)
     b.step(6)

@@ -167,3 +167,23 @@ def test_autotune_reports_the_solve_variant():
     assert ch["solve_roles"]["pressure"] != "system-grouped-two-rows"
     s.step(2)
     s.close()
+
+
+@pytest.mark.parametrize("precision", [cf.IW_PREC_FP64, cf.IW_PREC_MIXED])
+@pytest.mark.parametrize("nx", [32, 48, 256])
+def test_x_row_threads_give_the_same_bits(precision, nx):
+    """k_xrow_nl with 256 or 128 threads per CTA: every loop strides by the
+    block size and every element sees the same arithmetic, so the same bits
+    (power-of-two lengths with compile-time plans and a mixed-radix length)."""
+    import iwrepo_b200 as iw
+    cfg = cf.Config(nx=nx, ny=16, nzloc=9, nsubd=3, dt=1e-3, precision=precision).validate()
+    runs = []
+    for xt in (256, 128):
+        s = iw.Solver(cfg)
+        s.set_launch("x_row_threads", xt)
+        assert s.get_launch("x_row_threads") == xt
+        s.init_mode1(0.05, 1e-3, 41)
+        s.step(3)
+        runs.append(s.state(0))
+        s.close()
+    assert np.array_equal(runs[0], runs[1])
